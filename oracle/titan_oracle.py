@@ -1,0 +1,482 @@
+"""CPU oracle for the k-mesh x complex-energy Green-function path.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker: only the tests, the
+smoke check and the CPU-baseline leg of the benchmark may import it.  The
+product path (titan_b200) never calls it.
+
+It restates the reference's FP64 algorithm with numpy/LAPACK:
+
+* ``hk``                 -- calchk, source/mod_hamiltonian.F90:183-243
+* ``green``              -- green + invers, source/mod_greenfunction.F90:19-75,
+                            source/mod_tools.F90:796-829 (LAPACK inverse)
+* ``eintshechi``         -- source/eintshechi.F90:2-178; the 16 spin-block
+                            products are taken verbatim from the index tables
+                            of lines 86-104 (imaginary axis) and 146-164 (real
+                            axis), NOT from the GEMM re-formulation the GPU
+                            path uses, so the two are independent
+* ``umatrix`` / ``dyson`` -- source/mod_susceptibilities.F90:106-159,
+                            source/calculate_chi.F90:85-89
+* ``site_reduce``        -- source/calculate_chi.F90:91-107
+* ``expectation``        -- source/mod_expectation.F90:28-149
+* ``jacobian``           -- source/mod_self_consistency.F90:795-1205
+* ``self_consistency``   -- Newton iteration on sc_eqs
+                            (source/mod_self_consistency.F90:1516-1833); the
+                            root is the one SLATEC dnsqe converges to
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+PI = 4.0 * math.atan(1.0)
+TPI = 2.0 * PI
+
+# ---------------------------------------------------------------------------
+# Index tables of eintshechi.F90:86-104 (imaginary axis).  For chi element
+# (s1, s2): TERM1 gives the spin blocks of  gf?? (nu,gama,i,j,1) * gf?? (xi,mu,j,i,2)
+# and TERM2 those of conjg( gf?? (mu,xi,i,j,2) * gf?? (gama,nu,j,i,1) ).
+# ---------------------------------------------------------------------------
+TERM1 = {(1, 1): ("dd", "uu"), (1, 2): ("du", "uu"), (1, 3): ("dd", "du"), (1, 4): ("du", "du"),
+         (2, 1): ("ud", "uu"), (2, 2): ("uu", "uu"), (2, 3): ("ud", "du"), (2, 4): ("uu", "du"),
+         (3, 1): ("dd", "ud"), (3, 2): ("du", "ud"), (3, 3): ("dd", "dd"), (3, 4): ("du", "dd"),
+         (4, 1): ("ud", "ud"), (4, 2): ("uu", "ud"), (4, 3): ("ud", "dd"), (4, 4): ("uu", "dd")}
+TERM2 = {(1, 1): ("uu", "dd"), (1, 2): ("uu", "ud"), (1, 3): ("ud", "dd"), (1, 4): ("ud", "ud"),
+         (2, 1): ("uu", "du"), (2, 2): ("uu", "uu"), (2, 3): ("ud", "du"), (2, 4): ("ud", "uu"),
+         (3, 1): ("du", "dd"), (3, 2): ("du", "ud"), (3, 3): ("dd", "dd"), (3, 4): ("dd", "ud"),
+         (4, 1): ("du", "du"), (4, 2): ("du", "uu"), (4, 3): ("dd", "du"), (4, 4): ("dd", "uu")}
+# eintshechi.F90:146-164 (real axis): (gf??(nu,gama,i,j,1) - conjg(gf??(gama,nu,j,i,1))) * conjg(gf??(mu,xi,i,j,2))
+REAL = {(1, 1): ("dd", "dd", "uu"), (1, 2): ("du", "ud", "uu"), (1, 3): ("dd", "dd", "ud"), (1, 4): ("du", "ud", "ud"),
+        (2, 1): ("ud", "du", "uu"), (2, 2): ("uu", "uu", "uu"), (2, 3): ("ud", "du", "ud"), (2, 4): ("uu", "uu", "ud"),
+        (3, 1): ("dd", "dd", "du"), (3, 2): ("du", "ud", "du"), (3, 3): ("dd", "dd", "dd"), (3, 4): ("du", "ud", "dd"),
+        (4, 1): ("ud", "du", "du"), (4, 2): ("uu", "uu", "du"), (4, 3): ("ud", "du", "dd"), (4, 4): ("uu", "uu", "dd")}
+_SPIN = {"u": 0, "d": 1}
+
+
+class Model:
+    """Dense hopping matrices T_k (one per neighbour) and h0 for numpy evaluation."""
+
+    def __init__(self, system, h0):
+        self.system = system
+        self.h0 = np.asarray(h0, dtype=complex)
+        cv, bi, ish, t = system.neighbor_table()
+        n = system.dimH
+        ia = system.ia()
+        norbs = system.norbs
+        nn = cv.shape[0]
+        T = np.zeros((nn, n, n), dtype=complex)
+        for k in range(nn):
+            j = int(bi[k])
+            for i in range(system.n_atoms):
+                if not ish[k, i]:
+                    continue
+                blk = t[k, i, :norbs[j], :norbs[i]]
+                # calchk: rows of atom j (neighbour), columns of atom i; both spins
+                T[k, ia[j][0]:ia[j][1], ia[i][0]:ia[i][1]] += blk
+                T[k, ia[j][2]:ia[j][3], ia[i][2]:ia[i][3]] += blk
+        self.R = cv
+        self.T = T
+        self.n = n
+
+    def hk(self, kp):
+        """H(k) = h0 + sum_neigh exp(i k.R) T_neigh, kp: [P, 3] -> [P, n, n]."""
+        kp = np.atleast_2d(kp)
+        ph = np.exp(1j * (kp @ self.R.T))                      # [P, nNeigh]
+        H = np.tensordot(ph, self.T, axes=([1], [0]))           # [P, n, n]
+        return H + self.h0[None]
+
+    def green(self, z, kp):
+        """G = (z 1 - h0 - H_nl(k))^-1 for arrays z [P] and kp [P, 3]."""
+        H = self.hk(kp)
+        z = np.broadcast_to(np.asarray(z, dtype=complex), (H.shape[0],))
+        A = z[:, None, None] * np.eye(self.n)[None] - H
+        return np.linalg.inv(A)
+
+
+def _blk(G, ia, norbs, i, j, spins):
+    si, sj = _SPIN[spins[0]], _SPIN[spins[1]]
+    r0 = ia[i][0] + si * norbs[i]
+    c0 = ia[j][0] + sj * norbs[j]
+    return G[:, r0:r0 + norbs[i], c0:c0 + norbs[j]]
+
+
+def _chunks(P, size):
+    for s in range(0, P, size):
+        yield slice(s, min(P, s + size))
+
+
+def eintshechi(model: Model, mesh, real_bz, q, e, Ef, eta, etap, x2=None, p2=None, chunk=4096):
+    """chi0_HF(q, e) of eintshechi.F90:2-178 (before the MPI reduction).
+
+    ``mesh`` is the imaginary-axis (E, k) list; ``real_bz`` = (kp, w) of the
+    real-axis BZ; (x2, p2) the real-axis energy points (generated by the caller
+    with generate_real_epoints).  Returns chiorb_hf[dimens, dimens].
+    """
+    s = model.system
+    ia = s.ia()
+    norbs = s.norbs
+    nat = s.n_atoms
+    sidx = s.sigmaimunu2i()
+    D = s.dimens
+    chi = np.zeros((D, D), dtype=complex)
+    fint = np.zeros((D, D), dtype=complex)
+    q = np.asarray(q, float)
+
+    def scatter(target, i, j, s1, s2, block):
+        # block[mu, nu, gama, xi] -> target[sigmaimunu2i(s1,i,mu,nu), sigmaimunu2i(s2,j,gama,xi)]
+        ni, nj = norbs[i], norbs[j]
+        rows = sidx[s1 - 1, i, :ni, :ni].reshape(-1)
+        cols = sidx[s2 - 1, j, :nj, :nj].reshape(-1)
+        target[np.ix_(rows, cols)] += block.reshape(ni * ni, nj * nj)
+
+    y = mesh.point_energy()
+    for sl in _chunks(mesh.n_points, chunk):
+        kp = mesh.kp[sl]
+        w = mesh.weight[sl]
+        ep = y[sl]
+        g1 = model.green(Ef + e + 1j * (ep + eta), kp + q[None, :])   # gfq
+        g2 = model.green(Ef + 1j * (ep + etap), kp)                   # gf
+        for j in range(nat):
+            for i in range(nat):
+                for (s1, s2), (x1, y1) in TERM1.items():
+                    a = _blk(g1, ia, norbs, i, j, x1) * w[:, None, None]   # [P, nu, gama]
+                    b = _blk(g2, ia, norbs, j, i, y1)                      # [P, xi, mu]
+                    t1 = np.einsum("pvg,pxm->mvgx", a, b, optimize=True)
+                    x2s, y2s = TERM2[(s1, s2)]
+                    c = _blk(g2, ia, norbs, i, j, x2s) * w[:, None, None]  # [P, mu, xi]
+                    d = _blk(g1, ia, norbs, j, i, y2s)                     # [P, gama, nu]
+                    t2 = np.conj(np.einsum("pmx,pgv->mvgx", c, d, optimize=True))
+                    scatter(chi, i, j, s1, s2, t1 + t2)
+    if x2 is not None and len(x2) > 0:
+        kpr, wr = real_bz
+        nkr = kpr.shape[0]
+        for nep in range(len(x2)):
+            for sl in _chunks(nkr, chunk):
+                kp = kpr[sl]
+                w = p2[nep] * wr[sl]
+                g1 = model.green(x2[nep] + e + 1j * eta, kp + q[None, :])
+                g2 = model.green(x2[nep] + 1j * etap, kp)
+                for j in range(nat):
+                    for i in range(nat):
+                        for (s1, s2), (a1, a2, b1) in REAL.items():
+                            A = _blk(g1, ia, norbs, i, j, a1) - np.conj(np.swapaxes(_blk(g1, ia, norbs, j, i, a2), 1, 2))
+                            A = A * w[:, None, None]                           # [P, nu, gama]
+                            B = np.conj(_blk(g2, ia, norbs, i, j, b1))          # [P, mu, xi]
+                            blk = -1j * np.einsum("pvg,pmx->mvgx", A, B, optimize=True)
+                            scatter(fint, i, j, s1, s2, blk)
+    return (chi + fint) / TPI
+
+
+def umatrix(system):
+    """Umatorb of build_identity_and_U_matrix (mod_susceptibilities.F90:106-159)."""
+    D = system.dimens
+    U = np.zeros((D, D), dtype=complex)
+    sidx = system.sigmaimunu2i()
+    Un, Um = system.Un(), system.Um()
+    for i, dl in enumerate(system.dorbs):
+        for xi in dl:
+            for ga in dl:
+                for nu in dl:
+                    for mu in dl:
+                        if mu != nu or ga != xi:
+                            continue
+                        U[sidx[0, i, mu, nu], sidx[0, i, ga, xi]] = Um[i]
+                        U[sidx[1, i, mu, nu], sidx[1, i, ga, xi]] = Un[i]
+                        U[sidx[2, i, mu, nu], sidx[2, i, ga, xi]] = Un[i]
+                        U[sidx[3, i, mu, nu], sidx[3, i, ga, xi]] = Um[i]
+    for i, dl in enumerate(system.dorbs):
+        for xi in dl:
+            for ga in dl:
+                for nu in dl:
+                    for mu in dl:
+                        if mu != xi or nu != ga:
+                            continue
+                        for a in (1, 2):
+                            for b in (1, 2):
+                                U[sidx[a, i, mu, nu], sidx[b, i, ga, xi]] -= Un[i]
+    return U
+
+
+def dyson(chi_hf, U):
+    """chi_RPA = (1 + chi_HF U)^-1 chi_HF (calculate_chi.F90:85-89)."""
+    D = chi_hf.shape[0]
+    temp = np.eye(D, dtype=complex) + chi_hf @ U
+    return np.linalg.inv(temp) @ chi_hf
+
+
+def site_reduce(system, chi):
+    """4x4 site blocks schi(sigmai2i(s,i), sigmai2i(s',j)) = sum_{mu,nu} chi(s,i,mu,mu; s',j,nu,nu)."""
+    nat = system.n_atoms
+    sidx = system.sigmaimunu2i()
+    out = np.zeros((4 * nat, 4 * nat), dtype=complex)
+    for j in range(nat):
+        for i in range(nat):
+            for sp in range(4):
+                for sg in range(4):
+                    r = [sidx[sg, i, m, m] for m in range(system.norbs[i])]
+                    c = [sidx[sp, j, n, n] for n in range(system.norbs[j])]
+                    out[sg * nat + i, sp * nat + j] = chi[np.ix_(r, c)].sum()
+    return out
+
+
+def golden_row(system, e, q_abs, schi, i, j):
+    """Values of one output line ((Re, Im) schi(n,i; m,j), n = 1..4), m = 1..4 (mod_susceptibilities.F90:331-336)."""
+    nat = system.n_atoms
+    vals = [e, q_abs]
+    for m in range(4):
+        for n in range(4):
+            v = schi[n * nat + i, m * nat + j]
+            vals += [v.real, v.imag]
+    return vals
+
+
+def expectation(model: Model, mesh, Ef, eta, chunk=4096):
+    """rho, mx, my, mz, mp per (site, orbital) (mod_expectation.F90:28-149)."""
+    s = model.system
+    ia = s.ia()
+    nat = s.n_atoms
+    nmax = max(s.norbs)
+    imguu = np.zeros((nat, nmax))
+    imgdd = np.zeros((nat, nmax))
+    gud = np.zeros((nat, nmax), dtype=complex)
+    gdu = np.zeros((nat, nmax), dtype=complex)
+    y = mesh.point_energy()
+    for sl in _chunks(mesh.n_points, chunk):
+        G = model.green(Ef + 1j * (y[sl] + eta), mesh.kp[sl])
+        w = mesh.weight[sl]
+        for i in range(nat):
+            n = s.norbs[i]
+            b = ia[i][0]
+            for mu in range(n):
+                mup = mu + n
+                gud[i, mu] += np.sum(G[:, b + mu, b + mup] * w)
+                gdu[i, mu] += np.sum(G[:, b + mup, b + mu] * w)
+                imguu[i, mu] += np.sum(G[:, b + mu, b + mu].real * w)
+                imgdd[i, mu] += np.sum(G[:, b + mup, b + mup].real * w)
+    imguu /= PI
+    imgdd /= PI
+    mp = (gdu + np.conj(gud)) / PI
+    imguu = 0.5 + imguu
+    imgdd = 0.5 + imgdd
+    for i in range(nat):
+        imguu[i, s.norbs[i]:] = 0.0
+        imgdd[i, s.norbs[i]:] = 0.0
+    rho = imguu + imgdd
+    mz = imguu - imgdd
+    return rho, mp.real.copy(), mp.imag.copy(), mz, mp
+
+
+# ---------------------------------------------------------------------------
+# Self-consistency unknowns and the analytic Jacobian
+# ---------------------------------------------------------------------------
+def equation_layout(system, fixEf=False):
+    """neq_per_atom and neq (mod_self_consistency.F90:517-523), constr_type = default."""
+    per = [0]
+    for i in range(system.n_atoms):
+        nd = len(system.dorbs[i])
+        c = (nd if abs(system.Un()[i]) > 1e-8 else 0) + (3 if abs(system.Um()[i]) > 1e-8 else 0)
+        per.append(per[-1] + c)
+    neq = per[-1] + (0 if fixEf else 1)
+    return per, neq
+
+
+def _pauli_site(n, which, dorbs, d_only):
+    """pauli_orb / pauli_dorb(which) of one site, 2n x 2n (mod_constants.F90:83-148)."""
+    P = np.zeros((2 * n, 2 * n), dtype=complex)
+    orbs = dorbs if d_only else range(n)
+    for mu in orbs:
+        nu = mu + n
+        if which == 0:
+            P[mu, mu] = 1
+            P[nu, nu] = 1
+        elif which == 1:
+            P[mu, nu] = 1
+            P[nu, mu] = 1
+        elif which == 2:
+            P[mu, nu] = -1j
+            P[nu, mu] = 1j
+        elif which == 3:
+            P[mu, mu] = 1
+            P[nu, nu] = -1
+    return P
+
+
+def jacobian(model: Model, mesh, real_bz, Ef, eta, fixEf=False, chunk=2048):
+    """calcJacobian_greenfunction (mod_self_consistency.F90:795-1205), plain GF path."""
+    s = model.system
+    per, neq = equation_layout(s, fixEf)
+    J = np.zeros((neq, neq))
+    ia = s.ia()
+    nat = s.n_atoms
+    Un, Um = s.Un(), s.Um()
+    halfUn = -0.5 * Un
+    halfUm = -0.5 * Um
+
+    def site_block(G, i, j):
+        return G[:, ia[i][0]:ia[i][3], ia[j][0]:ia[j][3]]
+
+    y = mesh.point_energy()
+    for sl in _chunks(mesh.n_points, chunk):
+        G = model.green(Ef + 1j * (y[sl] + eta), mesh.kp[sl])
+        w = mesh.weight[sl]
+        for j in range(nat):
+            nj = s.norbs[j]
+            dj = s.dorbs[j]
+            for i in range(nat):
+                ni = s.norbs[i]
+                di = s.dorbs[i]
+                gij = site_block(G, i, j)
+                gji = site_block(G, j, i)
+                temp1 = [np.einsum("ab,pbc->pac", _pauli_site(ni, sg, di, sg != 0), gij) for sg in range(4)]
+
+                def diag_sum(t1, t2, orbs_list):
+                    # real(temp(mud,mud) + temp(nud,nud)) summed over points with weight
+                    d = np.einsum("prc,pcr->pr", t1, t2)          # diag of t1 @ t2
+                    vals = []
+                    for mu in orbs_list:
+                        vals.append(np.sum((d[:, mu] + d[:, mu + ni]) * w).real)
+                    return vals
+
+                kountj = per[j]
+                if abs(Un[j]) > 1e-8:
+                    for nu_i, nud in enumerate(dj):
+                        kounti = per[i]
+                        pt = _pauli_site(nj, 0, dj, True)
+                        pt[nud, nud] -= 2.0
+                        pt[nud + nj, nud + nj] -= 2.0
+                        t2 = halfUn[j] * np.einsum("ab,pbc->pac", pt, gji)
+                        if abs(Un[i]) > 1e-8:
+                            v = diag_sum(temp1[0], t2, di)
+                            for m, val in enumerate(v):
+                                J[kounti + m, kountj + nu_i] += val
+                            kounti = per[i] + len(di)
+                        if not fixEf:
+                            J[neq - 1, kountj + nu_i] += sum(diag_sum(temp1[0], t2, range(ni)))
+                        if abs(Um[i]) > 1e-8:
+                            for sg in range(1, 4):
+                                J[kounti + sg - 1, kountj + nu_i] += sum(diag_sum(temp1[sg], t2, di))
+                    kountj = per[j] + len(dj)
+                if abs(Um[j]) > 1e-8:
+                    t2s = {sp: halfUm[j] * np.einsum("ab,pbc->pac", _pauli_site(nj, sp, dj, True), gji)
+                           for sp in range(1, 4)}
+                    for sp in range(1, 4):
+                        kounti = per[i]
+                        if abs(Un[i]) > 1e-8:
+                            v = diag_sum(temp1[0], t2s[sp], di)
+                            for m, val in enumerate(v):
+                                J[kounti + m, kountj + sp - 1] += val
+                            kounti = per[i] + len(di)
+                        if not fixEf:
+                            J[neq - 1, kountj + sp - 1] += sum(diag_sum(temp1[0], t2s[sp], range(ni)))
+                        if abs(Um[i]) > 1e-8:
+                            for sg in range(1, 4):
+                                J[kounti + sg - 1, kountj + sp - 1] += sum(diag_sum(temp1[sg], t2s[sp], di))
+    if not fixEf:
+        kpr, wr = real_bz
+        for sl in _chunks(kpr.shape[0], chunk):
+            G = model.green(np.full(kpr[sl].shape[0], Ef + 1j * eta), kpr[sl])
+            w = wr[sl]
+            for i in range(nat):
+                ni = s.norbs[i]
+                di = s.dorbs[i]
+                gii = site_block(G, i, i)
+                kounti = per[i]
+                tmp = np.einsum("ab,pbc->pac", _pauli_site(ni, 0, di, False), gii) * w[:, None, None]
+                dg = np.einsum("prr->pr", tmp).sum(axis=0)
+                if abs(Un[i]) > 1e-8:
+                    for m, mud in enumerate(di):
+                        J[kounti + m, neq - 1] -= (dg[mud] + dg[mud + ni]).imag
+                    kounti = per[i] + len(di)
+                J[neq - 1, neq - 1] -= sum((dg[mu] + dg[mu + ni]).imag for mu in range(ni))
+                if abs(Um[i]) > 1e-8:
+                    for sg in range(1, 4):
+                        tmp = np.einsum("ab,pbc->pac", _pauli_site(ni, sg, di, True), gii) * w[:, None, None]
+                        dg = np.einsum("prr->pr", tmp).sum(axis=0)
+                        J[kounti + sg - 1, neq - 1] -= sum((dg[mud] + dg[mud + ni]).imag for mud in di)
+    J /= PI
+    for k in range(neq - 1):
+        J[k, k] -= 1.0
+    return J
+
+
+def unknowns_from_state(system, state, fixEf=False):
+    """set_hamiltonian_variables(set=.false.) (mod_self_consistency.F90:1754-1780)."""
+    per, neq = equation_layout(system, fixEf)
+    x = np.zeros(neq)
+    rd, xd, yd, zd = state.d_totals(system.dorbs)
+    for i in range(system.n_atoms):
+        k = per[i]
+        if abs(system.Un()[i]) > 1e-8:
+            for m, mu in enumerate(system.dorbs[i]):
+                x[k + m] = state.rho[i, mu]
+            k = per[i] + len(system.dorbs[i])
+        if abs(system.Um()[i]) > 1e-8:
+            x[k:k + 3] = [xd[i], yd[i], zd[i]]
+    if not fixEf:
+        x[neq - 1] = state.Ef
+    return x
+
+
+def state_from_unknowns(system, x, template, fixEf=False):
+    """set_hamiltonian_variables(set=.true.): the inputs that enter hee (and Ef)."""
+    from titan_b200.host.system import MagState
+    per, neq = equation_layout(system, fixEf)
+    st = MagState(template.rho.copy(), np.zeros_like(template.mx), np.zeros_like(template.my),
+                  np.zeros_like(template.mz), template.Ef)
+    for i in range(system.n_atoms):
+        k = per[i]
+        dl = system.dorbs[i]
+        if abs(system.Un()[i]) > 1e-8:
+            for m, mu in enumerate(dl):
+                st.rho[i, mu] = x[k + m]
+            k = per[i] + len(dl)
+        if abs(system.Um()[i]) > 1e-8:
+            # only the d totals enter hee; spread them over the d orbitals
+            for mu in dl:
+                st.mx[i, mu] = x[k] / len(dl)
+                st.my[i, mu] = x[k + 1] / len(dl)
+                st.mz[i, mu] = x[k + 2] / len(dl)
+    if not fixEf:
+        st.Ef = float(x[neq - 1])
+    return st
+
+
+def sc_residual(system, model_factory, mesh, x, template, fixEf=False):
+    """sc_eqs: fvec = out - in, plus the charge-neutrality line (mod_self_consistency.F90:1516-1628)."""
+    per, neq = equation_layout(system, fixEf)
+    st_in = state_from_unknowns(system, x, template, fixEf)
+    model = model_factory(st_in)
+    rho, mx, my, mz, mp = expectation(model, mesh, st_in.Ef, system.eta)
+    out = template.__class__(rho, mx, my, mz, st_in.Ef)
+    rd, xd, yd, zd = out.d_totals(system.dorbs)
+    rdi, xdi, ydi, zdi = st_in.d_totals(system.dorbs)
+    f = np.zeros(neq)
+    for i in range(system.n_atoms):
+        k = per[i]
+        dl = system.dorbs[i]
+        if abs(system.Un()[i]) > 1e-8:
+            for m, mu in enumerate(dl):
+                f[k + m] = rho[i, mu] - st_in.rho[i, mu]
+            k = per[i] + len(dl)
+        if abs(system.Um()[i]) > 1e-8:
+            f[k:k + 3] = [xd[i] - xdi[i], yd[i] - ydi[i], zd[i] - zdi[i]]
+    if not fixEf:
+        f[neq - 1] = rho.sum() - system.total_occupation()
+    return f, out, model
+
+
+def self_consistency(system, model_factory, mesh, real_bz, state0, fixEf=False, tol=1e-12, maxit=40):
+    """Newton iteration with the analytic Jacobian to the root dnsqe finds."""
+    x = unknowns_from_state(system, state0, fixEf)
+    template = state0
+    out = None
+    for it in range(maxit):
+        f, out, model = sc_residual(system, model_factory, mesh, x, template, fixEf)
+        Ef = x[-1] if not fixEf else template.Ef
+        J = jacobian(model, mesh, real_bz, Ef, system.eta, fixEf)
+        dx = np.linalg.solve(J, -f)
+        x = x + dx
+        if np.max(np.abs(dx)) <= tol * max(1.0, np.max(np.abs(x))):
+            break
+    f, out, model = sc_residual(system, model_factory, mesh, x, template, fixEf)
+    return x, out, f, it + 1

@@ -1,0 +1,58 @@
+"""Copy the reference's own regression fixtures for the Green-function path.
+
+The reference tests this path only through example runs compared against
+``results_correct`` files (its CI: .gitlab-ci.yml, jobs Fe_bulk, Fe_bulk:susc,
+graphene_pz).  This script copies those example input decks and golden
+outputs, unchanged, into ``tests/golden/<example>/`` so the tests can run
+without the reference tree.  Run it from the repository root:
+
+    python tests/golden/make_fixtures.py /path/to/reference
+"""
+import os
+import shutil
+import sys
+
+FILES = {
+    "Fe_bulk_susc": [
+        "input", "basis", "Fe",
+        "results_correct/scResult",
+        "results_correct/TSOC/selfconsistency/selfconsistency_1Sites_dfttype=S_parts=2_norb=9_nkpt=1000_eta=1.0E-03.dat",
+        "results_correct/TSOC/1Sites/HF/chihf_1_1_parts=2_parts3=1_norb=9_nkpt=1000_eta=1.0E-03.dat",
+        "results_correct/TSOC/1Sites/RPA/chi_1_1_parts=2_parts3=1_norb=9_nkpt=1000_eta=1.0E-03.dat",
+    ],
+    "graphene": [
+        "input", "basis", "Gr",
+        "results_correct/scResult",
+    ],
+}
+
+# golden files are stored flat under short names
+SHORT = {
+    "results_correct/scResult": "scResult",
+    "results_correct/TSOC/selfconsistency/selfconsistency_1Sites_dfttype=S_parts=2_norb=9_nkpt=1000_eta=1.0E-03.dat": "selfconsistency.dat",
+    "results_correct/TSOC/1Sites/HF/chihf_1_1_parts=2_parts3=1_norb=9_nkpt=1000_eta=1.0E-03.dat": "chihf_1_1.dat",
+    "results_correct/TSOC/1Sites/RPA/chi_1_1_parts=2_parts3=1_norb=9_nkpt=1000_eta=1.0E-03.dat": "chi_1_1.dat",
+}
+
+
+def main(ref_root: str) -> None:
+    here = os.path.dirname(os.path.abspath(__file__))
+    for ex, files in FILES.items():
+        dst = os.path.join(here, ex)
+        os.makedirs(dst, exist_ok=True)
+        for f in files:
+            src = os.path.join(ref_root, "examples", ex, f)
+            shutil.copyfile(src, os.path.join(dst, SHORT.get(f, os.path.basename(f))))
+        # the graphene self-consistency file has a run-dependent name
+        if ex == "graphene":
+            sc_dir = os.path.join(ref_root, "examples", ex, "results_correct", "FSOC", "selfconsistency")
+            if os.path.isdir(sc_dir):
+                for f in sorted(os.listdir(sc_dir)):
+                    if f.startswith("selfconsistency_"):
+                        shutil.copyfile(os.path.join(sc_dir, f), os.path.join(dst, "selfconsistency.dat"))
+                        break
+    print("fixtures written to", here)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
