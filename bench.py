@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""chi0(q, omega) throughput on one or more B200s: (k,E)-points per second.
+
+Workload (default): the 2D square monolayer with 2 spd atoms per cell
+(dimH = 36, chi dimension 648), seeded Slater-Koster model, 200 x 200 k mesh
+(40 401 points after boundary folding), 128 imaginary-axis energies
+(5 171 328 (E,k) points) plus 64 real-axis energies x the 40 401-point BZ for
+every omega != 0, 32 frequencies in [0, 0.5] eV at q = 0.  One step is one
+call of the public batched entry point (tg_chi0_batch) over --omegas-per-step
+frequencies; steps walk through the 32 frequencies.  A unit is one (k, E)
+quadrature point for one (q, omega): n_imag + n_real(omega) * nk per omega.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision split|fp64]
+    python bench.py --impl reference ...     # CPU oracle on a bounded sample
+
+With N > 1 (torchrun) every rank computes its own frequencies (the
+reference's frequency-group split, no collective on the data path): weak
+scaling, value = all ranks' units / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np
+
+METRIC = "χ⁰(q,ω) (k,E)-points/s: split-precision vs FP64 on 1 B200 at rel err ≤1e-9"
+UNIT = "(k,E)-points/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="split", choices=["split", "fp64"])
+    ap.add_argument("--config", default="sq2")
+    ap.add_argument("--omegas-per-step", type=int, default=4)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--compare-fp64", action="store_true", help="also time the FP64 path and report the ratio")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- workload
+def workload(config: str):
+    from titan_b200.host import synthetic
+    from titan_b200.host.system import initial_state
+    deck = synthetic.make_deck(config)
+    s = deck.system
+    h0 = s.h0(initial_state(s))
+    omegas = deck.frequencies()
+    reals = [deck.real_points(e, s.Ef) for e in omegas]
+    return deck, h0, omegas, reals
+
+
+def units_of(deck, omegas_idx, reals):
+    nimag = deck.ek.n_points
+    nk = deck.real_kp.shape[0]
+    return sum(nimag + len(reals[i][0]) * nk for i in omegas_idx)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def cpu_baseline(deck, h0, reals, omegas, seconds_target=15.0):
+    """The oracle (numpy/LAPACK, all host threads) on a bounded sample of the workload."""
+    from oracle import titan_oracle as O
+    from titan_b200.host.mesh import EKMesh
+    s = deck.system
+    m = O.Model(s, h0)
+    w_idx = 1 if len(omegas) > 1 else 0
+    e = float(omegas[w_idx])
+    x2, p2 = reals[w_idx]
+    n_imag_s = 1500
+    ek = deck.ek
+    sub = EKMesh(ek.y, ek.wght, ek.energy_index[:n_imag_s], ek.kp[:n_imag_s], ek.weight[:n_imag_s])
+    nk_s = 24 if len(x2) else 0
+    rk = (deck.real_kp[:max(nk_s, 1)], deck.real_w[:max(nk_s, 1)])
+    t0 = time.perf_counter()
+    O.eintshechi(m, sub, rk, np.zeros(3), e, s.Ef, s.eta, s.etap, x2 if nk_s else None, p2 if nk_s else None)
+    dt = time.perf_counter() - t0
+    units = n_imag_s + len(x2) * nk_s
+    cores = os.cpu_count()
+    return {"value": units / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle eintshechi (numpy/LAPACK, {cores} threads) on {n_imag_s} imaginary-axis points + "
+                      f"{len(x2)} real-axis energies x {nk_s} k of the {deck.system.name} workload at omega={e:.4g} "
+                      f"({units} units, {dt:.1f} s)"}
+
+
+# --------------------------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    deck, h0, omegas, reals = workload(args.config)
+    cb = None
+    vals = []
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        cpu_baseline(deck, h0, reals, omegas)
+    for _ in range(args.steps):
+        cb = cpu_baseline(deck, h0, reals, omegas)
+        vals.append(cb["value"])
+    v = statistics.median(vals)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SK model)", "impl": "reference",
+            "config": {"workload": f"{args.config}: chi0(q=0) sample, CPU restatement of eintshechi"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": "port", "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- our arm
+def timed_steps(gpu, deck, h0, omegas, reals, steps, start, per, precision, prof=True):
+    """Run `steps` chi0_batch calls; returns (device ms list, units, launches)."""
+    s = deck.system
+    n_om = len(omegas)
+    ms, units, launches = [], 0, 0
+    for st in range(steps):
+        idx = [(start + st * per + j) % n_om for j in range(per)]
+        es = [float(omegas[i]) for i in idx]
+        gpu.chi0_batch(np.zeros(3), es, s.Ef, s.eta, s.etap, [reals[i][0] for i in idx],
+                       [reals[i][1] for i in idx], precision)
+        t = gpu.last_timing()
+        ms.append(t[3])
+        launches += int(t[10])
+        units += units_of(deck, idx, reals)
+    return ms, units, launches, t
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from titan_b200.native import GreenGPU
+    torch.cuda.set_device(local_rank)
+    deck, h0, omegas, reals = workload(args.config)
+    s = deck.system
+    gpu = GreenGPU(local_rank)
+    gpu.setup(deck, h0)
+    gpu.profile(True)
+    per = args.omegas_per_step
+    start = rank * per * (args.steps + args.warmup)     # ranks take different frequencies
+    # warm-up (untimed)
+    timed_steps(gpu, deck, h0, omegas, reals, args.warmup, start, per, args.precision)
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local_rank)
+    clk.start()
+    ms, units, launches, last = timed_steps(gpu, deck, h0, omegas, reals, args.steps, start + args.warmup * per, per,
+                                            args.precision)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier(world)
+    total_ms = sum(ms)
+    total_ms_max = allreduce_max(total_ms, world)
+    units_all = allreduce_sum(units, world)
+    value = units_all / (total_ms_max / 1e3)
+    # dominant kernel: the chi0 contraction (kind 1), algorithmic flops 8 * dimens^2 per unit
+    con_ms, con_n = last[6], last[7]
+    grn_ms, grn_n = last[4], last[5]
+    last_units = units_of(deck, [(start + args.warmup * per + (args.steps - 1) * per + j) % len(omegas)
+                                 for j in range(per)], reals)
+    pk, pk_kind = peaks()
+    flops_con = 8.0 * s.dimens ** 2 * last_units
+    achieved = flops_con / (con_ms / 1e3) / 1e12 if con_ms > 0 else None
+    peak = pk.get("bf16_tflops_sustained" if False else "bf16_tflops")
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": None,
+            "kernel": "chi0 contraction (" + ("tcgen05 int8-sliced" if args.precision == "split" else "fp64 SIMT") + ")",
+            "peak_source": f"{pk_kind} bf16 dense (MEASURED_PEAKS.json)" if pk_kind == "measured" else "fallback 1.59 PF",
+            "launches_in_last_step": int(con_n), "avg_launch_ms": (con_ms / con_n) if con_n else None,
+            "inversion_ms_last_step": grn_ms, "inversion_launches_last_step": int(grn_n),
+            "inversion_fp64_tflops": (8.0 * s.dimH ** 3 * (2 * last_units)) / (grn_ms / 1e3) / 1e12 if grn_ms else None}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "s8 tensor-core slices + f64" if args.precision == "split" else "f64",
+            "data": "synthetic (seeded Slater-Koster model, no external data)",
+            "config": {"workload": f"{args.config}: dimH={s.dimH}, chi dim={s.dimens}, {deck.ek.n_points} imag (E,k) "
+                                   f"points, {deck.real_kp.shape[0]} real-axis k x 64 energies, 32 omega in [0,0.5], q=0",
+                       "omegas_per_step": per, "precision": args.precision,
+                       "l2": "inputs larger than L2 (mesh 200+ MB, operands GBs per pass)"},
+            "roofline": roof, "gpu_launches": launches, "clocks": clocks}
+    if args.compare_fp64 and args.precision != "fp64":
+        ms64, u64, _, _ = timed_steps(gpu, deck, h0, omegas, reals, 1, start, per, "fp64")
+        line["fp64_path"] = {"value": u64 / (sum(ms64) / 1e3), "unit": UNIT, "ms_per_step": sum(ms64)}
+        line["split_over_fp64"] = value / world / line["fp64_path"]["value"]
+    # end to end: public API from pinned host buffers, full set-up + call + read-back every step
+    if not args.no_e2e:
+        e2e = run_e2e(gpu, deck, h0, omegas, reals, args, start + args.warmup * per, per, world)
+        line["e2e"] = e2e
+    if rank == 0 and not args.no_cpu and world == 1:
+        line["cpu_baseline"] = cpu_baseline(deck, h0, reals, omegas)
+    gpu.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(gpu, deck, h0, omegas, reals, args, start, per, world):
+    import torch
+    s = deck.system
+    ek = deck.ek
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+
+    y = pinned(np.ascontiguousarray(ek.point_energy(), np.float64))
+    kp = pinned(np.ascontiguousarray(ek.kp, np.float64))
+    w = pinned(np.ascontiguousarray(ek.weight, np.float64))
+    rk = pinned(np.ascontiguousarray(deck.real_kp, np.float64))
+    rw = pinned(np.ascontiguousarray(deck.real_w, np.float64))
+    h0p = pinned(np.ascontiguousarray(h0, np.complex128).view(np.float64))
+    out = torch.empty((per, s.dimens, s.dimens * 2), dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
+    gpu.profile(False)
+    h2d = y.nbytes + kp.nbytes + w.nbytes + rk.nbytes + rw.nbytes + h0p.nbytes
+    units = 0
+    barrier(world)
+    t0 = time.perf_counter()
+    for st in range(args.steps):
+        idx = [(start + st * per + j) % len(omegas) for j in range(per)]
+        gpu.set_system(s)
+        gpu.set_h0(h0p.view(np.complex128).reshape(s.dimH, s.dimH))
+        gpu.set_imag_mesh_arrays(y, kp.reshape(-1, 3), w)
+        gpu.set_real_mesh(rk.reshape(-1, 3), rw)
+        gpu.chi0_batch(np.zeros(3), [float(omegas[i]) for i in idx], s.Ef, s.eta, s.etap,
+                       [reals[i][0] for i in idx], [reals[i][1] for i in idx], args.precision, out=out)
+        units += units_of(deck, idx, reals)
+    dt = time.perf_counter() - t0
+    dt_max = allreduce_max(dt, world)
+    units_all = allreduce_sum(units, world)
+    return {"value": units_all / dt_max, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(out.nbytes), "timer": "host wall clock around the public API calls"}
+
+
+# --------------------------------------------------------------------------- distributed helpers
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

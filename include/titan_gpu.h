@@ -1,0 +1,131 @@
+/*
+ * titan_gpu.h -- C ABI of the B200 Green-function path (k-mesh x complex energy).
+ *
+ * Drop-in boundary for the reference's swappable Green-function routines.  A
+ * Fortran host binds these with ISO_C_BINDING; every
+ * array is caller-owned HOST memory in Fortran (column-major) order, complex
+ * numbers are interleaved (re, im) doubles, and every call returns a status:
+ *
+ *     0            success
+ *     > 0          singular (z - H(k)) at the returned 1-based point index
+ *                  (the LAPACK info convention of invers, mod_tools.F90:814-827)
+ *     TG_ERR_*     < 0, see below; tg_last_error() has the message
+ *
+ * One context per process and GPU; calls on one context are not re-entrant
+ * (the reference calls these from the master thread only,
+ * mod_mpi_pars.F90:49).
+ */
+#ifndef TITAN_GPU_H
+#define TITAN_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TG_OK            0
+#define TG_ERR_ARG      (-1)   /* bad argument (size, pointer, unsupported dimension) */
+#define TG_ERR_CUDA     (-2)   /* CUDA runtime error */
+#define TG_ERR_STATE    (-3)   /* call order: system / h0 / mesh not set */
+#define TG_ERR_TIMEOUT  (-4)   /* a bounded device wait gave up */
+#define TG_ERR_NOMEM    (-5)   /* device allocation failed */
+
+/* Precision of the chi0 contraction (tg_chi0). */
+#define TG_PREC_FP64     0     /* FP64 SIMT contraction */
+#define TG_PREC_SPLIT    1     /* INT8-sliced tensor-core contraction (tcgen05), FP64 recombination */
+
+typedef struct tg_ctx tg_ctx;
+
+/* Context lifecycle.  Replaces create_handle / destroy_handle
+ * (source/mod_cuda.F90:34,80; called at source/main.F90:81,431). */
+int tg_create(int device, tg_ctx** ctx);
+int tg_destroy(tg_ctx* ctx);
+const char* tg_last_error(const tg_ctx* ctx);
+
+/* Neighbour table of the tight-binding model: the data calchk reads
+ * (source/mod_hamiltonian.F90:183-243; AtomTypes.F90:53-68).
+ *   norb[n_atoms]                         orbitals per site
+ *   cell_vec(3, n_neigh)                  Neighbors(k)%CellVector
+ *   basis_idx(n_neigh)                    Neighbors(k)%BasisIndex (1-based)
+ *   is_hopping(n_atoms, n_neigh)          Neighbors(k)%isHopping(i) (0/1)
+ *   t0i(norb_max, norb_max, n_atoms, n_neigh) complex: Neighbors(k)%t0i(:,:,i)
+ */
+int tg_set_system(tg_ctx* ctx, int n_atoms, const int* norb, int norb_max, int n_neigh,
+                  const double* cell_vec, const int* basis_idx, const int* is_hopping,
+                  const double* t0i);
+
+/* Local Hamiltonian h0(dimH, dimH) complex (mod_hamiltonian.F90:35-87, the
+ * module array h0 that green() adds).  Set again whenever hee changes. */
+int tg_set_h0(tg_ctx* ctx, int dimH, const double* h0);
+
+/* Imaginary-axis (E, k) list: the flattened E_k_imag_mesh of
+ * adaptiveMesh.F90:76-161 with y(E), bzs(E)%kp and wght(E)*bzs(E)%w per point. */
+int tg_set_imag_mesh(tg_ctx* ctx, int64_t n_points, const double* y, const double* kp,
+                     const double* w);
+
+/* Real-axis BZ (realBZ%kp(3, nk), realBZ%w(nk), mod_BrillouinZone.F90:64-110). */
+int tg_set_real_mesh(tg_ctx* ctx, int64_t n_k, const double* kp, const double* w);
+
+/* chi0_HF(q, e): replaces eintshechi(q, e) (source/eintshechi.F90:2-178).
+ *   (x2, p2)[n_real]   real-axis points of generate_real_epoints(e) (ignored when |e| < 1e-15)
+ *   chiorb_hf(dimens, dimens) complex, the module array of mod_susceptibilities,
+ *   already divided by 2 pi (eintshechi.F90:174).  precision: TG_PREC_*. */
+int tg_chi0(tg_ctx* ctx, const double* q, double e, double Ef, double eta, double etap,
+            int n_real, const double* x2, const double* p2, int precision, int dimens,
+            double* chiorb_hf);
+
+/* Batched chi0 over n_omega frequencies at one q: the imaginary-axis G(k, Ef+iy)
+ * is computed once and reused for every frequency (it does not depend on e).
+ *   e[n_omega]; x2, p2: (n_real, n_omega), column w = real-axis points of e[w];
+ *   chiorb_hf(dimens, dimens, n_omega). */
+int tg_chi0_batch(tg_ctx* ctx, const double* q, int n_omega, const double* e, double Ef,
+                  double eta, double etap, int n_real, const double* x2, const double* p2,
+                  int precision, int dimens, double* chiorb_hf);
+
+/* Occupations and moments: replaces expectation_values_greenfunction
+ * (source/mod_expectation.F90:28-149).  All outputs (norb_max, n_atoms). */
+int tg_expectation(tg_ctx* ctx, double Ef, double eta, double* rho, double* mx, double* my,
+                   double* mz, double* mp);
+
+/* Orbital-diagonal GG tensor for the Jacobian and its adjoint:
+ *   T(16, ncol, nrow, n_atoms(j), n_atoms(i)) complex with
+ *   T[s',t,t',s; i,g; j,h] = sum_p w_p sum_{mu in g} sum_{nu in h}
+ *        G(i s' mu, j t nu) G(j t' nu, i s mu),  G at Ef + i(y_p + eta),
+ *   spin index order s' + 2 t + 4 t' + 8 s (0 = up).
+ * Row groups of site i: d orbitals one by one, then all non-d orbitals summed
+ * (nrow = nd + 1); column groups: d orbitals one by one (ncol = nd) when
+ * orbital_resolved != 0; dmask(norb_max, n_atoms) flags the d orbitals
+ * (Types%dOrbs) and may be null otherwise.  With orbital_resolved == 0 every site has one row
+ * group and one column group holding all its orbitals (the (V, B) adjoint).
+ * This is the contraction inside calcJacobian_greenfunction
+ * (mod_self_consistency.F90:843-1127); the host maps it onto the Jacobian. */
+int tg_gg_tensor(tg_ctx* ctx, double Ef, double eta, int orbital_resolved, const int* dmask, double* T);
+
+/* Fermi-level column of calcJacobian_greenfunction (mod_self_consistency.F90:1131-1196):
+ *   D(4, norb_max, n_atoms) complex: sum_k w_k tr_spin[sigma_a G_ii(mu,mu)](Ef + i eta)
+ *   over realBZ, sigma_a = (1, x, y, z). */
+int tg_fermi_column(tg_ctx* ctx, double Ef, double eta, double* D);
+
+/* RPA Dyson solve chi = (1 + chi_hf U)^-1 chi_hf in FP64 on the GPU
+ * (calculate_chi.F90:85-89).  All matrices (dimens, dimens) complex. */
+int tg_dyson(tg_ctx* ctx, int dimens, const double* chi_hf, const double* umat, double* chi);
+
+/* Test hooks.  G(dimH, dimH, nz) = (z - h0 - H(k))^-1 for nz (k, z) pairs,
+ * and H(dimH, dimH, nk) = h0 + calchk(k). */
+int tg_green_batch(tg_ctx* ctx, int64_t nz, const double* z, const double* kp, double* G);
+int tg_hamiltk_batch(tg_ctx* ctx, int64_t nk, const double* kp, double* H);
+
+/* Device timing of the last tg_chi0/tg_chi0_batch call (CUDA events on the
+ * context's stream): ms[0] imaginary-axis G2 inversions, ms[1] contraction and
+ * the other inversions, ms[2] epilogue, ms[3] whole call; when per-launch
+ * profiling is on (tg_profile), ms[4..9] = (total ms, launches) of the
+ * inversion, contraction and epilogue kernels; ms[10] = kernels launched.
+ * ms must hold 11 doubles. */
+int tg_last_timing(const tg_ctx* ctx, double* ms);
+int tg_profile(tg_ctx* ctx, int enable);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TITAN_GPU_H */

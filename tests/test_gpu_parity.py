@@ -1,0 +1,158 @@
+"""CUDA path vs the CPU oracle, through the C ABI (needs a B200)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import titan_oracle as O
+from titan_b200.host import synthetic
+from titan_b200.host.system import initial_state
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from titan_b200.native import GreenGPU
+    g = GreenGPU(0)
+    yield g
+    g.close()
+
+
+def _setup(gpu, deck, state=None):
+    s = deck.system
+    st = state if state is not None else initial_state(s)
+    h0 = s.h0(st)
+    gpu.setup(deck, h0)
+    return s, h0
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("shape", ["bcc1", "sq2", "bcc4", "slab5"])
+def test_hamiltk_matches_calchk(gpu, shape):
+    deck = synthetic.make_deck(shape, mesh=False)
+    s = deck.system
+    h0 = s.h0(initial_state(s))
+    gpu.set_system(s)
+    gpu.set_h0(h0)
+    kp = np.random.default_rng(1).uniform(-2, 2, size=(40, 3))
+    H = gpu.hamiltk_batch(kp)
+    Hr = O.Model(s, h0).hk(kp)
+    assert np.max(np.abs(H - Hr)) < 1e-13 * max(1.0, np.max(np.abs(Hr)))
+
+
+@pytest.mark.parametrize("shape", ["bcc1", "sq2", "bcc4", "slab5"])
+def test_green_batch_matches_lapack_inverse(gpu, shape):
+    deck = synthetic.make_deck(shape, mesh=False)
+    s = deck.system
+    h0 = s.h0(initial_state(s))
+    gpu.set_system(s)
+    gpu.set_h0(h0)
+    rng = np.random.default_rng(2)
+    n = 37
+    kp = rng.uniform(-2, 2, size=(n, 3))
+    # near the real axis (Im z = eta = 1e-3) up to far away
+    z = s.Ef + rng.uniform(-3, 3, n) + 1j * 10.0 ** rng.uniform(-3, 1, n)
+    G = gpu.green_batch(z, kp)
+    m = O.Model(s, h0)
+    Gr = m.green(z, kp)
+    for p in range(n):
+        assert np.max(np.abs(G[p] - Gr[p])) <= 1e-12 * np.max(np.abs(Gr[p])) * s.dimH
+    H = m.hk(kp)
+    R = np.einsum("pab,pbc->pac", G, z[:, None, None] * np.eye(s.dimH)[None] - H)
+    assert np.max(np.abs(R - np.eye(s.dimH)[None])) < 1e-9
+
+
+def test_singular_matrix_reports_point_index(gpu):
+    """z - H exactly singular (H = 0, z = 0 at the third point) -> status 3."""
+    from titan_b200.native import TitanGPUError
+    deck = synthetic.make_deck("bcc1", mesh=False)
+    s = deck.system
+    s_empty = synthetic.make_system("bcc1")
+    s_empty.neighbors = []
+    s_empty.t0i = {}
+    gpu.set_system(s_empty)
+    gpu.set_h0(np.zeros((s.dimH, s.dimH), complex))
+    z = np.array([1.0 + 1j, 2.0 + 0.5j, 0.0 + 0.0j, 3.0 + 0j])
+    with pytest.raises(TitanGPUError) as ei:
+        gpu.green_batch(z, np.zeros((4, 3)))
+    assert ei.value.code == 3
+
+
+@pytest.mark.parametrize("shape,nk,e,q", [
+    ("bcc1", (4, 4, 4), 0.0, (0, 0, 0)),
+    ("bcc1", (4, 4, 4), 0.05, (0, 0, 0)),
+    ("bcc1", (3, 3, 3), 0.02, (0.1, 0.0, 0.2)),
+    ("sq2", (6, 6, 1), 0.0, (0, 0, 0)),
+    ("sq2", (5, 5, 1), 0.1, (0.05, 0.02, 0.0)),
+])
+def test_chi0_fp64_matches_oracle(gpu, shape, nk, e, q):
+    deck = synthetic.make_deck(shape, nk=nk, n1gl=8, parts=1, n3gl=6)
+    s, h0 = _setup(gpu, deck)
+    x2, p2 = deck.real_points(e, s.Ef)
+    chi = gpu.chi0(np.array(q, float), e, s.Ef, s.eta, s.etap, x2, p2)
+    ref = O.eintshechi(O.Model(s, h0), deck.ek, (deck.real_kp, deck.real_w), np.array(q, float), e, s.Ef, s.eta,
+                       s.etap, x2, p2)
+    assert rel(chi, ref) < 1e-10
+
+
+def test_chi0_batch_equals_single_calls(gpu):
+    deck = synthetic.make_deck("bcc1", nk=(3, 3, 3), n1gl=6, parts=1, n3gl=4)
+    s, h0 = _setup(gpu, deck)
+    es = [0.0, 0.03, 0.07]
+    xs = [deck.real_points(e, s.Ef) for e in es]
+    batch = gpu.chi0_batch(np.zeros(3), es, s.Ef, s.eta, s.etap, [x[0] for x in xs], [x[1] for x in xs])
+    for w, e in enumerate(es):
+        single = gpu.chi0(np.zeros(3), e, s.Ef, s.eta, s.etap, xs[w][0], xs[w][1])
+        assert rel(batch[w], single) < 1e-13
+
+
+def test_fe_golden_through_gpu(gpu, fe_deck, fe_chi_golden):
+    """The reference's Fe_bulk_susc chi_HF / chi_RPA rows through the GPU path."""
+    s = fe_deck.system
+    h0 = s.h0(fe_deck.state)
+    gpu.setup(fe_deck, h0)
+    ghf, grpa = fe_chi_golden
+    U = O.umatrix(s)
+    for idx in (0, 1, 5):
+        e = fe_deck.frequencies()[idx]
+        x2, p2 = fe_deck.real_points(e, s.Ef)
+        chi = gpu.chi0(np.zeros(3), e, s.Ef, s.eta, s.etap, x2, p2)
+        rpa = gpu.dyson(chi, U)
+        hf_row = O.golden_row(s, e, 0.0, O.site_reduce(s, chi), 0, 0)
+        rpa_row = O.golden_row(s, e, 0.0, O.site_reduce(s, rpa), 0, 0)
+        for a, b in zip(hf_row, ghf[idx]):
+            if abs(b) > 1e-6:
+                assert abs(a - b) <= 1e-8 * abs(b), (idx, a, b)
+        for a, b in zip(rpa_row, grpa[idx]):
+            if abs(b) > 1e-6:
+                assert abs(a - b) <= 5e-8 * abs(b), (idx, a, b)
+
+
+def test_expectation_matches_oracle_and_fe_fixed_point(gpu, fe_deck):
+    s = fe_deck.system
+    st = fe_deck.state
+    h0 = s.h0(st)
+    gpu.setup(fe_deck, h0)
+    rho, mx, my, mz, mp = gpu.expectation(st.Ef, s.eta)
+    assert np.max(np.abs(rho - st.rho)) < 1e-7
+    assert np.max(np.abs(mz - st.mz)) < 1e-7
+    r2, x2, y2, z2, mp2 = O.expectation(O.Model(s, h0), fe_deck.ek, st.Ef, s.eta)
+    for a, b in ((rho, r2), (mx, x2), (my, y2), (mz, z2)):
+        assert np.max(np.abs(a - b)) < 1e-12
+
+
+def test_dyson_matches_numpy(gpu):
+    rng = np.random.default_rng(3)
+    n = 100
+    chi = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    U = np.zeros((n, n), complex)
+    U[np.arange(0, n, 3), np.arange(0, n, 3)] = 0.3
+    out = gpu.dyson(chi, U)
+    ref = O.dyson(chi, U)
+    assert rel(out, ref) < 1e-12

@@ -1,0 +1,989 @@
+// C ABI of libtitan_gpu (declared in include/titan_gpu.h).
+//
+// The context owns every device buffer; host arrays stay caller-owned.  The
+// orchestration per chi0(q, omega) call mirrors eintshechi.F90:2-178:
+//   imaginary axis, in passes of P points:  G2 = G(k, Ef + i(y + eta'))  -> B operand
+//                                           G1 = G(k+q, Ef + e + i(y + eta)) -> A operand
+//                                           C += A^T B per site pair (contraction)
+//   real axis (|e| >= 1e-15), same with z on [Ef - e, Ef]             -> D
+//   epilogue: chiorb_hf = (C + conj(C_swapped) - i D) / 2 pi
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/titan_gpu.h"
+#include "tg_internal.cuh"
+#include "tg_split.cuh"
+
+using namespace tg;
+
+namespace tg {
+int dyson_device(int n, const double2* chi_hf, const double2* U, double2* work, double2* chi, int* piv, int* status,
+                 cudaStream_t s);
+}
+
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+template <class T>
+struct DevArray {
+  T* p = nullptr;
+  size_t n = 0;
+  void free_() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t ensure(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    free_();
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    n = count;
+    return cudaSuccess;
+  }
+  cudaError_t upload(const T* h, size_t count, cudaStream_t s) {
+    cudaError_t e = ensure(count);
+    if (e != cudaSuccess) return e;
+    if (count == 0) return cudaSuccess;
+    return cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+};
+
+}  // namespace
+
+struct tg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  std::string err;
+  bool sys_set = false, h0_set = false, imag_set = false, real_set = false;
+  // system
+  int n_atoms = 0, nmax = 0, dimH = 0, dimens = 0, n_neigh = 0;
+  std::vector<int> norb, ia;            // ia[i] = first row of site i
+  std::vector<int> pair_M, pair_aoff;   // per pair (i*nat + j)
+  std::vector<int64_t> pair_coff;
+  std::vector<PairTile> tiles;
+  DevArray<double> d_R;
+  DevArray<int> d_pair_start, d_pair_neigh, d_row_atom, d_row_orb, d_row_spin, d_outmap, d_decode, d_norb,
+      d_pair_M, d_pair_aoff, d_exp_rows, d_gg_desc;
+  DevArray<int64_t> d_pair_coff;
+  DevArray<double2> d_pair_t, d_h0;
+  DevArray<PairTile> d_tiles;
+  // meshes
+  int64_t n_imag = 0, n_realk = 0;
+  DevArray<double> d_y, d_kp, d_w, d_rkp, d_rw, d_x2, d_p2;
+  // workspace
+  DevArray<double2> d_A, d_B, d_C, d_D, d_chi, d_acc, d_acc_red;
+  DevArray<double2> d_zlist, d_gout;
+  DevArray<double> d_klist;
+  DevArray<int> d_status;
+  DevArray<unsigned char> d_split_ws;
+  DevArray<double2> d_dy;
+  DevArray<int> d_piv;
+  cudaEvent_t ev[8] = {};
+  double last_ms[4] = {0, 0, 0, 0};
+  // optional per-launch timing: (kind, start, stop) event pairs of the last call
+  bool profile = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
+  double kind_ms[4] = {0, 0, 0, 0};
+  int kind_n[4] = {0, 0, 0, 0};
+  int64_t launches = 0;   // kernels launched by the last chi0 call
+  int64_t pass_points = 0;     // points per pass (bounded workspace)
+  int gg_blocks = 0, gg_nrow = 0, gg_ncol = 0, gg_mode = -1;
+};
+
+namespace {
+
+// launch-kind timing (kind 0 = green/inversion, 1 = contraction, 2 = epilogue)
+cudaEvent_t pool_event(tg_ctx* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct KindTimer {
+  tg_ctx* c;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  KindTimer(tg_ctx* ctx, int k) : c(ctx), kind(k) {
+    if (!c->profile) return;
+    a = pool_event(c);
+    b = pool_event(c);
+    cudaEventRecord(a, c->stream);
+  }
+  ~KindTimer() {
+    if (kind != 1) c->launches += 1;   // contraction launches are counted by contract()
+    if (!c->profile) return;
+    cudaEventRecord(b, c->stream);
+    c->ev_used.push_back({kind, {a, b}});
+  }
+};
+
+void profile_begin(tg_ctx* c) {
+  c->launches = 0;
+  for (int k = 0; k < 4; ++k) {
+    c->kind_ms[k] = 0;
+    c->kind_n[k] = 0;
+  }
+}
+
+void profile_end(tg_ctx* c) {
+  if (!c->profile) return;
+  cudaStreamSynchronize(c->stream);
+  for (auto& u : c->ev_used) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, u.second.first, u.second.second);
+    c->kind_ms[u.first] += ms;
+    c->kind_n[u.first] += 1;
+    c->ev_pool.push_back(u.second.first);
+    c->ev_pool.push_back(u.second.second);
+  }
+  c->ev_used.clear();
+}
+
+int set_err(tg_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_err(tg_ctx* c, cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return TG_OK;
+  std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return set_err(c, TG_ERR_NOMEM, m);
+  return set_err(c, TG_ERR_CUDA, m);
+}
+
+#define TG_CHECK(c, call, where)                      \
+  do {                                                \
+    cudaError_t _e = (call);                          \
+    if (_e != cudaSuccess) return cuda_err(c, _e, where); \
+  } while (0)
+
+GreenArgs base_args(tg_ctx* c) {
+  GreenArgs a;
+  a.n = c->dimH;
+  a.n_neigh = c->n_neigh;
+  a.R = c->d_R.p;
+  a.pair_start = c->d_pair_start.p;
+  a.pair_neigh = c->d_pair_neigh.p;
+  a.pair_t = c->d_pair_t.p;
+  a.nmax = c->nmax;
+  a.n_atoms = c->n_atoms;
+  a.row_atom = c->d_row_atom.p;
+  a.row_orb = c->d_row_orb.p;
+  a.row_spin = c->d_row_spin.p;
+  a.h0 = c->d_h0.p;
+  a.outmap = c->d_outmap.p;
+  a.status = c->d_status.p;
+  return a;
+}
+
+int check_ready(tg_ctx* c, bool need_imag, bool need_real) {
+  if (!c) return TG_ERR_ARG;
+  if (!c->sys_set) return set_err(c, TG_ERR_STATE, "tg_set_system has not been called");
+  if (!c->h0_set) return set_err(c, TG_ERR_STATE, "tg_set_h0 has not been called");
+  if (need_imag && !c->imag_set) return set_err(c, TG_ERR_STATE, "tg_set_imag_mesh has not been called");
+  if (need_real && !c->real_set) return set_err(c, TG_ERR_STATE, "tg_set_real_mesh has not been called");
+  return TG_OK;
+}
+
+int reset_status(tg_ctx* c) {
+  const int big = 0x7fffffff;
+  TG_CHECK(c, cudaMemcpyAsync(c->d_status.p, &big, sizeof(int), cudaMemcpyHostToDevice, c->stream), "status");
+  return TG_OK;
+}
+
+int read_status(tg_ctx* c) {
+  int st = 0;
+  TG_CHECK(c, cudaMemcpyAsync(&st, c->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");
+  TG_CHECK(c, cudaStreamSynchronize(c->stream), "sync");
+  if (st != 0x7fffffff) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "singular (z - H(k)) at point %d", st);
+    c->err = buf;
+    return st;
+  }
+  return TG_OK;
+}
+
+int64_t pass_size(tg_ctx* c, int64_t np) {
+  // two operand buffers of P * dimH^2 complex each, bounded to ~6 GiB
+  const int64_t per = (int64_t)c->dimH * c->dimH * sizeof(double2);
+  int64_t P = (int64_t)3 << 30;
+  P /= per;
+  P = std::max<int64_t>(P, 1024);
+  P = (P / 64) * 64;
+  return std::min<int64_t>(P, std::max<int64_t>(np, 1));
+}
+
+int nsplit_for(tg_ctx* c) {
+  const int nt = (int)c->tiles.size();
+  int s = std::max(1, c->num_sms / std::max(nt, 1));
+  return std::min(s, 64);
+}
+
+// contraction of one pass into Cpart: FP64 SIMT path or the sliced tensor-core path
+int contract(tg_ctx* c, int precision, const double2* A, const double2* B, int64_t np, double2* Cpart,
+             int nsplit, int64_t cstride) {
+  if (precision == TG_PREC_FP64) {
+    c->launches += 1;
+    TG_CHECK(c, launch_gemm64(A, B, (int64_t)c->dimH * c->dimH, np, nsplit, c->d_tiles.p, (int)c->tiles.size(),
+                              c->d_pair_M.p, c->d_pair_aoff.p, c->d_pair_coff.p, Cpart, cstride, c->stream),
+             "contraction (fp64)");
+    return TG_OK;
+  }
+  SplitArgs sa;
+  sa.A = A;
+  sa.B = B;
+  sa.ld = (int64_t)c->dimH * c->dimH;
+  sa.np = np;
+  sa.n_pairs = c->n_atoms * c->n_atoms;
+  sa.pair_M = c->pair_M.data();
+  sa.pair_aoff = c->pair_aoff.data();
+  sa.pair_coff = c->pair_coff.data();
+  sa.d_pair_M = c->d_pair_M.p;
+  sa.d_pair_aoff = c->d_pair_aoff.p;
+  sa.d_pair_coff = c->d_pair_coff.p;
+  sa.C = Cpart;   // split partial 0 receives the FP64 recombination
+  sa.num_sms = c->num_sms;
+  size_t need = split_workspace_bytes(sa);
+  TG_CHECK(c, c->d_split_ws.ensure(need), "split workspace");
+  sa.ws = c->d_split_ws.p;
+  sa.ws_bytes = c->d_split_ws.n;
+  int nl = 0;
+  cudaError_t e = launch_split_contraction(sa, c->stream, &nl);
+  c->launches += nl;
+  if (e == cudaErrorNotSupported) return set_err(c, TG_ERR_ARG, "split-precision contraction: unsupported pair size");
+  TG_CHECK(c, e, "contraction (split)");
+  (void)nsplit;
+  (void)cstride;
+  return TG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tg_create(int device, tg_ctx** out) {
+  if (!out) return TG_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return TG_ERR_CUDA;
+  if (device < 0 || device >= ndev) return TG_ERR_ARG;
+  tg_ctx* c = new tg_ctx();
+  c->device = device;
+  e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+  if (e == cudaSuccess) e = c->d_status.ensure(1);
+  if (e != cudaSuccess) {
+    tg_destroy(c);
+    return TG_ERR_CUDA;
+  }
+  *out = c;
+  return TG_OK;
+}
+
+int tg_destroy(tg_ctx* c) {
+  if (!c) return TG_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->d_R.free_(); c->d_pair_start.free_(); c->d_pair_neigh.free_(); c->d_row_atom.free_();
+  c->d_row_orb.free_(); c->d_row_spin.free_(); c->d_outmap.free_(); c->d_decode.free_(); c->d_norb.free_();
+  c->d_pair_M.free_(); c->d_pair_aoff.free_(); c->d_exp_rows.free_(); c->d_gg_desc.free_(); c->d_pair_coff.free_();
+  c->d_pair_t.free_(); c->d_h0.free_(); c->d_tiles.free_(); c->d_y.free_(); c->d_kp.free_(); c->d_w.free_();
+  c->d_rkp.free_(); c->d_rw.free_(); c->d_x2.free_(); c->d_p2.free_(); c->d_A.free_(); c->d_B.free_();
+  c->d_C.free_(); c->d_D.free_(); c->d_chi.free_(); c->d_acc.free_(); c->d_acc_red.free_(); c->d_zlist.free_();
+  c->d_gout.free_(); c->d_klist.free_(); c->d_status.free_(); c->d_split_ws.free_();
+  c->d_dy.free_(); c->d_piv.free_();
+  for (int i = 0; i < 8; ++i)
+    if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  for (auto& u : c->ev_used) {
+    cudaEventDestroy(u.second.first);
+    cudaEventDestroy(u.second.second);
+  }
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return TG_OK;
+}
+
+const char* tg_last_error(const tg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int tg_set_system(tg_ctx* c, int n_atoms, const int* norb, int norb_max, int n_neigh, const double* cell_vec,
+                  const int* basis_idx, const int* is_hopping, const double* t0i) {
+  if (!c) return TG_ERR_ARG;
+  if (n_atoms <= 0 || n_atoms > 1023 || !norb || norb_max <= 0 || norb_max > 63 || n_neigh < 0)
+    return set_err(c, TG_ERR_ARG, "tg_set_system: bad sizes");
+  if (n_neigh > 0 && (!cell_vec || !basis_idx || !is_hopping || !t0i))
+    return set_err(c, TG_ERR_ARG, "tg_set_system: null neighbour arrays");
+  cudaSetDevice(c->device);
+  c->n_atoms = n_atoms;
+  c->nmax = norb_max;
+  c->n_neigh = n_neigh;
+  c->norb.assign(norb, norb + n_atoms);
+  for (int i = 0; i < n_atoms; ++i)
+    if (c->norb[i] <= 0 || c->norb[i] > norb_max) return set_err(c, TG_ERR_ARG, "tg_set_system: norb out of range");
+  c->ia.resize(n_atoms);
+  int pos = 0, dens = 0;
+  for (int i = 0; i < n_atoms; ++i) {
+    c->ia[i] = pos;
+    pos += 2 * c->norb[i];
+    dens += c->norb[i] * c->norb[i];
+  }
+  c->dimH = pos;
+  c->dimens = 4 * dens;
+  if (!green_supported(c->dimH)) {
+    char b[128];
+    snprintf(b, sizeof b, "dimH = %d has no Gauss-Jordan tile configuration", c->dimH);
+    return set_err(c, TG_ERR_ARG, b);
+  }
+  const int n = c->dimH;
+  // row tables
+  std::vector<int> ratom(n), rorb(n), rspin(n);
+  for (int i = 0; i < n_atoms; ++i)
+    for (int s = 0; s < 2; ++s)
+      for (int o = 0; o < c->norb[i]; ++o) {
+        const int r = c->ia[i] + s * c->norb[i] + o;
+        ratom[r] = i;
+        rorb[r] = o;
+        rspin[r] = s;
+      }
+  // hopping blocks grouped by (row atom = neighbour basis index j, col atom = i)
+  const int np2 = n_atoms * n_atoms;
+  std::vector<std::vector<std::pair<int, int>>> lists(np2);   // (neighbour, site i)
+  for (int k = 0; k < n_neigh; ++k) {
+    const int j = basis_idx[k] - 1;
+    if (j < 0 || j >= n_atoms) return set_err(c, TG_ERR_ARG, "tg_set_system: basis_idx out of range");
+    for (int i = 0; i < n_atoms; ++i)
+      if (is_hopping[(size_t)k * n_atoms + i]) lists[j * n_atoms + i].push_back({k, i});
+  }
+  std::vector<int> pstart(np2 + 1, 0), pneigh;
+  std::vector<double2> pt;
+  const size_t blk = (size_t)norb_max * norb_max;
+  for (int pidx = 0; pidx < np2; ++pidx) {
+    pstart[pidx] = (int)pneigh.size();
+    for (auto& kv : lists[pidx]) {
+      const int k = kv.first, i = kv.second;
+      pneigh.push_back(k);
+      const double* src = t0i + 2 * (((size_t)k * n_atoms + i) * blk);
+      for (size_t e = 0; e < blk; ++e) pt.push_back(make_double2(src[2 * e], src[2 * e + 1]));
+    }
+  }
+  pstart[np2] = (int)pneigh.size();
+  // pair-block operand layout, C offsets, output map, gemm tiles
+  c->pair_M.assign(np2, 0);
+  c->pair_aoff.assign(np2, 0);
+  c->pair_coff.assign(np2, 0);
+  std::vector<int> outmap((size_t)n * n);
+  int aoff = 0;
+  int64_t coff = 0;
+  c->tiles.clear();
+  const int T = gemm64_tile();
+  for (int i = 0; i < n_atoms; ++i)
+    for (int j = 0; j < n_atoms; ++j) {
+      const int p = i * n_atoms + j;
+      const int M = 4 * c->norb[i] * c->norb[j];
+      c->pair_M[p] = M;
+      c->pair_aoff[p] = aoff;
+      c->pair_coff[p] = coff;
+      const int ni2 = 2 * c->norb[i], nj2 = 2 * c->norb[j];
+      for (int x = 0; x < ni2; ++x)
+        for (int y = 0; y < nj2; ++y) outmap[aoff + x * nj2 + y] = (c->ia[i] + x) * n + (c->ia[j] + y);
+      for (int u0 = 0; u0 < M; u0 += T)
+        for (int v0 = 0; v0 < M; v0 += T) c->tiles.push_back(PairTile{p, u0, v0});
+      aoff += M;
+      coff += (int64_t)M * M;
+    }
+  // chi row decode: sigmaimunu2i order (sigma fastest, then nu, mu, site)
+  std::vector<int> decode(c->dimens);
+  int kount = 0;
+  for (int i = 0; i < n_atoms; ++i)
+    for (int mu = 0; mu < c->norb[i]; ++mu)
+      for (int nu = 0; nu < c->norb[i]; ++nu)
+        for (int s = 0; s < 4; ++s) decode[kount++] = s | (i << 2) | (mu << 12) | (nu << 18);
+  // expectation rows (up, down) per orbital
+  std::vector<int> exprows(n);
+  {
+    int o = 0;
+    for (int i = 0; i < n_atoms; ++i)
+      for (int mu = 0; mu < c->norb[i]; ++mu) {
+        exprows[2 * o] = c->ia[i] + mu;
+        exprows[2 * o + 1] = c->ia[i] + c->norb[i] + mu;
+        ++o;
+      }
+  }
+  cudaStream_t s = c->stream;
+  std::vector<double> R(cell_vec, cell_vec + 3 * (size_t)n_neigh);
+  TG_CHECK(c, c->d_R.upload(R.data(), R.size(), s), "upload R");
+  TG_CHECK(c, c->d_pair_start.upload(pstart.data(), pstart.size(), s), "upload");
+  TG_CHECK(c, c->d_pair_neigh.upload(pneigh.data(), pneigh.size(), s), "upload");
+  TG_CHECK(c, c->d_pair_t.upload(pt.data(), pt.size(), s), "upload");
+  TG_CHECK(c, c->d_row_atom.upload(ratom.data(), n, s), "upload");
+  TG_CHECK(c, c->d_row_orb.upload(rorb.data(), n, s), "upload");
+  TG_CHECK(c, c->d_row_spin.upload(rspin.data(), n, s), "upload");
+  TG_CHECK(c, c->d_outmap.upload(outmap.data(), outmap.size(), s), "upload");
+  TG_CHECK(c, c->d_decode.upload(decode.data(), decode.size(), s), "upload");
+  TG_CHECK(c, c->d_norb.upload(c->norb.data(), n_atoms, s), "upload");
+  TG_CHECK(c, c->d_pair_M.upload(c->pair_M.data(), np2, s), "upload");
+  TG_CHECK(c, c->d_pair_aoff.upload(c->pair_aoff.data(), np2, s), "upload");
+  TG_CHECK(c, c->d_pair_coff.upload(c->pair_coff.data(), np2, s), "upload");
+  TG_CHECK(c, c->d_tiles.upload(c->tiles.data(), c->tiles.size(), s), "upload");
+  TG_CHECK(c, c->d_exp_rows.upload(exprows.data(), exprows.size(), s), "upload");
+  TG_CHECK(c, cudaStreamSynchronize(s), "sync");
+  c->sys_set = true;
+  c->h0_set = false;
+  c->gg_mode = -1;
+  return TG_OK;
+}
+
+int tg_set_h0(tg_ctx* c, int dimH, const double* h0) {
+  if (!c) return TG_ERR_ARG;
+  if (!c->sys_set) return set_err(c, TG_ERR_STATE, "tg_set_system has not been called");
+  if (dimH != c->dimH || !h0) return set_err(c, TG_ERR_ARG, "tg_set_h0: dimH mismatch");
+  cudaSetDevice(c->device);
+  TG_CHECK(c, c->d_h0.upload(reinterpret_cast<const double2*>(h0), (size_t)dimH * dimH, c->stream), "upload h0");
+  TG_CHECK(c, cudaStreamSynchronize(c->stream), "sync");
+  c->h0_set = true;
+  return TG_OK;
+}
+
+int tg_set_imag_mesh(tg_ctx* c, int64_t n_points, const double* y, const double* kp, const double* w) {
+  if (!c) return TG_ERR_ARG;
+  if (n_points < 0 || (n_points > 0 && (!y || !kp || !w))) return set_err(c, TG_ERR_ARG, "tg_set_imag_mesh: bad args");
+  cudaSetDevice(c->device);
+  TG_CHECK(c, c->d_y.upload(y, n_points, c->stream), "upload y");
+  TG_CHECK(c, c->d_kp.upload(kp, 3 * n_points, c->stream), "upload kp");
+  TG_CHECK(c, c->d_w.upload(w, n_points, c->stream), "upload w");
+  TG_CHECK(c, cudaStreamSynchronize(c->stream), "sync");
+  c->n_imag = n_points;
+  c->imag_set = true;
+  return TG_OK;
+}
+
+int tg_set_real_mesh(tg_ctx* c, int64_t n_k, const double* kp, const double* w) {
+  if (!c) return TG_ERR_ARG;
+  if (n_k < 0 || (n_k > 0 && (!kp || !w))) return set_err(c, TG_ERR_ARG, "tg_set_real_mesh: bad args");
+  cudaSetDevice(c->device);
+  TG_CHECK(c, c->d_rkp.upload(kp, 3 * n_k, c->stream), "upload kp");
+  TG_CHECK(c, c->d_rw.upload(w, n_k, c->stream), "upload w");
+  TG_CHECK(c, cudaStreamSynchronize(c->stream), "sync");
+  c->n_realk = n_k;
+  c->real_set = true;
+  return TG_OK;
+}
+
+int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, double Ef, double eta, double etap,
+                  int n_real, const double* x2, const double* p2, int precision, int dimens, double* chiorb_hf) {
+  int rc = check_ready(c, true, false);
+  if (rc) return rc;
+  if (!q || !e || n_omega <= 0 || !chiorb_hf) return set_err(c, TG_ERR_ARG, "tg_chi0: null argument");
+  if (dimens != c->dimens) return set_err(c, TG_ERR_ARG, "tg_chi0: dimens mismatch");
+  if (precision != TG_PREC_FP64 && precision != TG_PREC_SPLIT) return set_err(c, TG_ERR_ARG, "tg_chi0: precision");
+  bool any_real = false;
+  for (int w = 0; w < n_omega; ++w) any_real |= std::fabs(e[w]) >= 1e-15;
+  if (any_real && (n_real <= 0 || !x2 || !p2)) return set_err(c, TG_ERR_ARG, "tg_chi0: real-axis points missing");
+  if (any_real && !c->real_set) return set_err(c, TG_ERR_STATE, "tg_set_real_mesh has not been called");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int n = c->dimH;
+  const int64_t nn = (int64_t)n * n;
+  const int nsplit = (precision == TG_PREC_FP64) ? nsplit_for(c) : 1;
+  const int64_t cstride = (int64_t)c->dimens * c->dimens;
+  // workspace
+  const int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, (int64_t)n_real * c->n_realk));
+  TG_CHECK(c, c->d_A.ensure((size_t)P * nn), "alloc A");
+  TG_CHECK(c, c->d_B.ensure((size_t)P * nn), "alloc B");
+  TG_CHECK(c, c->d_C.ensure((size_t)n_omega * nsplit * cstride), "alloc C");
+  TG_CHECK(c, c->d_D.ensure((size_t)n_omega * nsplit * cstride), "alloc D");
+  TG_CHECK(c, c->d_chi.ensure((size_t)cstride), "alloc chi");
+  TG_CHECK(c, cudaMemsetAsync(c->d_C.p, 0, sizeof(double2) * n_omega * nsplit * cstride, s), "memset");
+  TG_CHECK(c, cudaMemsetAsync(c->d_D.p, 0, sizeof(double2) * n_omega * nsplit * cstride, s), "memset");
+  if (any_real) {
+    TG_CHECK(c, c->d_x2.upload(x2, (size_t)n_omega * n_real, s), "upload x2");
+    TG_CHECK(c, c->d_p2.upload(p2, (size_t)n_omega * n_real, s), "upload p2");
+  }
+  rc = reset_status(c);
+  if (rc) return rc;
+  profile_begin(c);
+  float t_green = 0, t_con = 0, t_epi = 0;
+  cudaEvent_t *ev = c->ev;
+  TG_CHECK(c, cudaEventRecord(ev[0], s), "event");
+  // ---------------- imaginary axis ----------------
+  const bool q_zero = q[0] == 0.0 && q[1] == 0.0 && q[2] == 0.0;
+  for (int64_t p0 = 0; p0 < c->n_imag; p0 += P) {
+    const int64_t np = std::min<int64_t>(P, c->n_imag - p0);
+    GreenArgs g2 = base_args(c);
+    g2.pts.kind = 0;
+    g2.pts.y = c->d_y.p;
+    g2.pts.kp = c->d_kp.p;
+    g2.pts.w = c->d_w.p;
+    g2.p0 = p0;
+    g2.np = np;
+    g2.zr = Ef;
+    g2.zi = etap;
+    g2.mode = MODE_B_IMAG;
+    g2.out = c->d_B.p;
+    // G1 = G2 when e = 0, q = 0 and eta = eta': one inversion feeds both operands
+    int w_start = 0;
+    if (e[0] == 0.0 && q_zero && eta == etap) {
+      g2.out2 = c->d_A.p;
+      g2.mode2 = MODE_A_IMAG;
+      w_start = 1;
+    }
+    cudaEventRecord(ev[1], s);
+    {
+      KindTimer kt(c, 0);
+      TG_CHECK(c, launch_green(g2, c->num_sms, s, nullptr), "green (imag, G2)");
+    }
+    cudaEventRecord(ev[2], s);
+    float ms = 0;
+    if (w_start == 1) {
+      KindTimer kt(c, 1);
+      rc = contract(c, precision, c->d_A.p, c->d_B.p, np, c->d_C.p, nsplit, cstride);
+      if (rc) return rc;
+    }
+    for (int w = w_start; w < n_omega; ++w) {
+      GreenArgs g1 = base_args(c);
+      g1.pts = g2.pts;
+      g1.p0 = p0;
+      g1.np = np;
+      g1.zr = Ef + e[w];
+      g1.zi = eta;
+      g1.q[0] = q[0]; g1.q[1] = q[1]; g1.q[2] = q[2];
+      g1.mode = MODE_A_IMAG;
+      g1.out = c->d_A.p;
+      {
+        KindTimer kt(c, 0);
+        TG_CHECK(c, launch_green(g1, c->num_sms, s, nullptr), "green (imag, G1)");
+      }
+      {
+        KindTimer kt(c, 1);
+        rc = contract(c, precision, c->d_A.p, c->d_B.p, np, c->d_C.p + (size_t)w * nsplit * cstride, nsplit, cstride);
+      }
+      if (rc) return rc;
+    }
+    cudaEventRecord(ev[4], s);
+    TG_CHECK(c, cudaEventSynchronize(ev[4]), "sync");
+    cudaEventElapsedTime(&ms, ev[1], ev[2]);
+    t_green += ms;
+    cudaEventElapsedTime(&ms, ev[2], ev[4]);
+    t_con += ms;   // includes the G1 inversions of w >= 1 (split below is approximate)
+  }
+  // ---------------- real axis ----------------
+  for (int w = 0; w < n_omega; ++w) {
+    if (std::fabs(e[w]) < 1e-15) continue;
+    const int64_t ntot = (int64_t)n_real * c->n_realk;
+    for (int64_t p0 = 0; p0 < ntot; p0 += P) {
+      const int64_t np = std::min<int64_t>(P, ntot - p0);
+      GreenArgs gr = base_args(c);
+      gr.pts.kind = 1;
+      gr.pts.kp = c->d_rkp.p;
+      gr.pts.w = c->d_rw.p;
+      gr.pts.x2 = c->d_x2.p + (size_t)w * n_real;
+      gr.pts.p2 = c->d_p2.p + (size_t)w * n_real;
+      gr.pts.nk = c->n_realk;
+      gr.p0 = p0;
+      gr.np = np;
+      // G2 = G(k, x2 + i eta') -> conj(G2)
+      gr.zr = 0.0;
+      gr.zi = etap;
+      gr.mode = MODE_B_REAL;
+      gr.out = c->d_B.p;
+      {
+        KindTimer kt(c, 0);
+        TG_CHECK(c, launch_green(gr, c->num_sms, s, nullptr), "green (real, G2)");
+      }
+      // G1 = G(k + q, x2 + e + i eta) -> w (G1 - G1^dagger)
+      gr.zr = e[w];
+      gr.zi = eta;
+      gr.q[0] = q[0]; gr.q[1] = q[1]; gr.q[2] = q[2];
+      gr.mode = MODE_A_REAL;
+      gr.out = c->d_A.p;
+      {
+        KindTimer kt(c, 0);
+        TG_CHECK(c, launch_green(gr, c->num_sms, s, nullptr), "green (real, G1)");
+      }
+      {
+        KindTimer kt(c, 1);
+        rc = contract(c, precision, c->d_A.p, c->d_B.p, np, c->d_D.p + (size_t)w * nsplit * cstride, nsplit, cstride);
+      }
+      if (rc) return rc;
+    }
+  }
+  cudaEventRecord(ev[5], s);
+  // ---------------- epilogue per frequency ----------------
+  for (int w = 0; w < n_omega; ++w) {
+    KindTimer kt(c, 2);
+    TG_CHECK(c, launch_chi_epilogue(c->d_C.p + (size_t)w * nsplit * cstride, c->d_D.p + (size_t)w * nsplit * cstride,
+                                    nsplit, cstride, c->dimens, c->d_decode.p, c->d_norb.p, c->d_pair_coff.p,
+                                    c->n_atoms, 1.0 / (2.0 * kPi), c->d_chi.p, s),
+             "epilogue");
+    TG_CHECK(c, cudaMemcpyAsync(chiorb_hf + 2 * (size_t)w * cstride, c->d_chi.p, sizeof(double2) * cstride,
+                                cudaMemcpyDeviceToHost, s),
+             "copy chi");
+  }
+  cudaEventRecord(ev[6], s);
+  TG_CHECK(c, cudaEventSynchronize(ev[6]), "sync");
+  float ms_real = 0, ms_epi = 0, ms_tot = 0;
+  cudaEventElapsedTime(&ms_real, ev[4], ev[5]);
+  cudaEventElapsedTime(&ms_epi, ev[5], ev[6]);
+  cudaEventElapsedTime(&ms_tot, ev[0], ev[6]);
+  t_epi = ms_epi;
+  c->last_ms[0] = t_green;
+  c->last_ms[1] = t_con + ms_real;
+  c->last_ms[2] = t_epi;
+  c->last_ms[3] = ms_tot;
+  profile_end(c);
+  return read_status(c);
+}
+
+int tg_chi0(tg_ctx* c, const double* q, double e, double Ef, double eta, double etap, int n_real, const double* x2,
+            const double* p2, int precision, int dimens, double* chiorb_hf) {
+  return tg_chi0_batch(c, q, 1, &e, Ef, eta, etap, n_real, x2, p2, precision, dimens, chiorb_hf);
+}
+
+int tg_last_timing(const tg_ctx* c, double* ms) {
+  if (!c || !ms) return TG_ERR_ARG;
+  for (int i = 0; i < 4; ++i) ms[i] = c->last_ms[i];
+  for (int i = 0; i < 3; ++i) {
+    ms[4 + 2 * i] = c->kind_ms[i];
+    ms[5 + 2 * i] = c->kind_n[i];
+  }
+  ms[10] = (double)c->launches;
+  return TG_OK;
+}
+
+int tg_profile(tg_ctx* c, int enable) {
+  if (!c) return TG_ERR_ARG;
+  c->profile = enable != 0;
+  return TG_OK;
+}
+
+int tg_expectation(tg_ctx* c, double Ef, double eta, double* rho, double* mx, double* my, double* mz, double* mp) {
+  int rc = check_ready(c, true, false);
+  if (rc) return rc;
+  if (!rho || !mx || !my || !mz || !mp) return set_err(c, TG_ERR_ARG, "tg_expectation: null output");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int n = c->dimH;
+  const int len = 2 * n;   // 4 complex per orbital, n/2 orbitals
+  GreenArgs a = base_args(c);
+  a.pts.kind = 0;
+  a.pts.y = c->d_y.p;
+  a.pts.kp = c->d_kp.p;
+  a.pts.w = c->d_w.p;
+  a.p0 = 0;
+  a.np = c->n_imag;
+  a.zr = Ef;
+  a.zi = eta;
+  a.mode = MODE_EXPECT;
+  a.gg_desc = c->d_exp_rows.p;
+  const int maxgrid = c->num_sms * 8;
+  TG_CHECK(c, c->d_acc.ensure((size_t)maxgrid * len), "alloc acc");
+  TG_CHECK(c, c->d_acc_red.ensure(len), "alloc acc");
+  a.acc = c->d_acc.p;
+  a.acc_len = 0;   // EXPECT keeps its sums in registers
+  rc = reset_status(c);
+  if (rc) return rc;
+  int grid = 0;
+  TG_CHECK(c, launch_green(a, c->num_sms, s, &grid), "green (expectation)");
+  TG_CHECK(c, launch_reduce_blocks(c->d_acc.p, grid, len, c->d_acc_red.p, s), "reduce");
+  std::vector<double2> h(len);
+  TG_CHECK(c, cudaMemcpyAsync(h.data(), c->d_acc_red.p, sizeof(double2) * len, cudaMemcpyDeviceToHost, s), "copy");
+  rc = read_status(c);
+  if (rc) return rc;
+  // mod_expectation.F90:121-147
+  int o = 0;
+  const double pi = kPi;
+  for (int i = 0; i < c->n_atoms; ++i) {
+    for (int mu = 0; mu < c->nmax; ++mu) {
+      const size_t idx = (size_t)i * c->nmax + mu;
+      if (mu >= c->norb[i]) {
+        rho[idx] = mx[idx] = my[idx] = mz[idx] = 0.0;
+        mp[2 * idx] = mp[2 * idx + 1] = 0.0;
+        continue;
+      }
+      const double2 uu = h[4 * o], dd = h[4 * o + 1], ud = h[4 * o + 2], du = h[4 * o + 3];
+      const double nu_ = 0.5 + uu.x / pi, nd_ = 0.5 + dd.x / pi;
+      rho[idx] = nu_ + nd_;
+      mz[idx] = nu_ - nd_;
+      const double mpr = (du.x + ud.x) / pi, mpi = (du.y - ud.y) / pi;
+      mx[idx] = mpr;
+      my[idx] = mpi;
+      mp[2 * idx] = mpr;
+      mp[2 * idx + 1] = mpi;
+      ++o;
+    }
+  }
+  return TG_OK;
+}
+
+int tg_gg_tensor(tg_ctx* c, double Ef, double eta, int orbital_resolved, const int* dmask, double* T) {
+  int rc = check_ready(c, true, false);
+  if (rc) return rc;
+  if (!T || (orbital_resolved && !dmask)) return set_err(c, TG_ERR_ARG, "tg_gg_tensor: null argument");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int nat = c->n_atoms;
+  // groups per site
+  std::vector<std::vector<std::vector<int>>> rowg(nat), colg(nat);
+  int nrow = 0, ncol = 0;
+  for (int i = 0; i < nat; ++i) {
+    // d orbitals of the site from dmask(norb_max, n_atoms) (Types%dOrbs)
+    const int no = c->norb[i];
+    if (orbital_resolved) {
+      std::vector<int> rest;
+      for (int o = 0; o < no; ++o) {
+        if (dmask[(size_t)i * c->nmax + o]) {
+          rowg[i].push_back({o});
+          colg[i].push_back({o});
+        } else {
+          rest.push_back(o);
+        }
+      }
+      rowg[i].push_back(rest);
+    } else {
+      std::vector<int> all;
+      for (int o = 0; o < no; ++o) all.push_back(o);
+      rowg[i].push_back(all);
+      colg[i].push_back(all);
+    }
+    nrow = std::max<int>(nrow, (int)rowg[i].size());
+    ncol = std::max<int>(ncol, (int)colg[i].size());
+  }
+  // descriptors: per block (i, g, j, h) in output order T(16, ncol, nrow, j, i)
+  std::vector<int> desc, lists;
+  std::vector<int> block_of;   // output slot per descriptor block
+  int nblocks = 0;
+  std::vector<int> list_off;
+  auto add_list = [&](const std::vector<int>& l) {
+    const int off = (int)lists.size();
+    lists.push_back((int)l.size());
+    for (int x : l) lists.push_back(x);
+    return off;
+  };
+  for (int i = 0; i < nat; ++i)
+    for (int j = 0; j < nat; ++j)
+      for (int g = 0; g < (int)rowg[i].size(); ++g)
+        for (int h = 0; h < (int)colg[j].size(); ++h) {
+          desc.push_back(c->ia[i]);
+          desc.push_back(c->ia[i] + c->norb[i]);
+          desc.push_back(c->ia[j]);
+          desc.push_back(c->ia[j] + c->norb[j]);
+          desc.push_back(-1);
+          desc.push_back(-1);
+          block_of.push_back(((i * nat + j) * nrow + g) * ncol + h);
+          ++nblocks;
+        }
+  // list offsets (relative to the list area start)
+  {
+    int b = 0;
+    for (int i = 0; i < nat; ++i)
+      for (int j = 0; j < nat; ++j)
+        for (int g = 0; g < (int)rowg[i].size(); ++g)
+          for (int h = 0; h < (int)colg[j].size(); ++h) {
+            desc[6 * b + 4] = add_list(rowg[i][g]);
+            desc[6 * b + 5] = add_list(colg[j][h]);
+            ++b;
+          }
+  }
+  std::vector<int> all(desc);
+  all.insert(all.end(), lists.begin(), lists.end());
+  TG_CHECK(c, c->d_gg_desc.upload(all.data(), all.size(), s), "upload gg desc");
+  const int acc_len = 16 * nblocks;
+  GreenArgs a = base_args(c);
+  a.pts.kind = 0;
+  a.pts.y = c->d_y.p;
+  a.pts.kp = c->d_kp.p;
+  a.pts.w = c->d_w.p;
+  a.np = c->n_imag;
+  a.zr = Ef;
+  a.zi = eta;
+  a.mode = MODE_GG;
+  a.gg_desc = c->d_gg_desc.p;
+  a.acc_len = acc_len;
+  const int maxgrid = c->num_sms * 8;
+  TG_CHECK(c, c->d_acc.ensure((size_t)maxgrid * acc_len), "alloc acc");
+  TG_CHECK(c, c->d_acc_red.ensure(acc_len), "alloc acc");
+  a.acc = c->d_acc.p;
+  rc = reset_status(c);
+  if (rc) return rc;
+  int grid = 0;
+  cudaError_t e = launch_green(a, c->num_sms, s, &grid);
+  if (e == cudaErrorInvalidValue) return set_err(c, TG_ERR_ARG, "tg_gg_tensor: accumulator does not fit in shared memory");
+  TG_CHECK(c, e, "green (gg)");
+  TG_CHECK(c, launch_reduce_blocks(c->d_acc.p, grid, acc_len, c->d_acc_red.p, s), "reduce");
+  std::vector<double2> h(acc_len);
+  TG_CHECK(c, cudaMemcpyAsync(h.data(), c->d_acc_red.p, sizeof(double2) * acc_len, cudaMemcpyDeviceToHost, s), "copy");
+  rc = read_status(c);
+  if (rc) return rc;
+  const size_t total = (size_t)nat * nat * nrow * ncol * 16;
+  std::memset(T, 0, sizeof(double) * 2 * total);
+  for (int b = 0; b < nblocks; ++b)
+    for (int q = 0; q < 16; ++q) {
+      const size_t dst = (size_t)block_of[b] * 16 + q;
+      T[2 * dst] = h[16 * b + q].x;
+      T[2 * dst + 1] = h[16 * b + q].y;
+    }
+  return TG_OK;
+}
+
+int tg_fermi_column(tg_ctx* c, double Ef, double eta, double* D) {
+  int rc = check_ready(c, false, true);
+  if (rc) return rc;
+  if (!D) return set_err(c, TG_ERR_ARG, "tg_fermi_column: null output");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int n = c->dimH;
+  const int acc_len = 2 * n;   // 4 per orbital
+  double one = 1.0, ef = Ef;
+  TG_CHECK(c, c->d_x2.upload(&ef, 1, s), "upload");
+  TG_CHECK(c, c->d_p2.upload(&one, 1, s), "upload");
+  TG_CHECK(c, c->d_gg_desc.upload(nullptr, 0, s), "upload");
+  std::vector<int> rows(n);
+  {
+    int o = 0;
+    for (int i = 0; i < c->n_atoms; ++i)
+      for (int mu = 0; mu < c->norb[i]; ++mu) {
+        rows[2 * o] = c->ia[i] + mu;
+        rows[2 * o + 1] = c->ia[i] + c->norb[i] + mu;
+        ++o;
+      }
+  }
+  TG_CHECK(c, c->d_gg_desc.upload(rows.data(), rows.size(), s), "upload");
+  GreenArgs a = base_args(c);
+  a.pts.kind = 1;
+  a.pts.kp = c->d_rkp.p;
+  a.pts.w = c->d_rw.p;
+  a.pts.x2 = c->d_x2.p;
+  a.pts.p2 = c->d_p2.p;
+  a.pts.nk = c->n_realk;
+  a.np = c->n_realk;
+  a.zr = 0.0;
+  a.zi = eta;
+  a.mode = MODE_DIAG4;
+  a.gg_desc = c->d_gg_desc.p;
+  a.acc_len = acc_len;
+  const int maxgrid = c->num_sms * 8;
+  TG_CHECK(c, c->d_acc.ensure((size_t)maxgrid * acc_len), "alloc acc");
+  TG_CHECK(c, c->d_acc_red.ensure(acc_len), "alloc acc");
+  a.acc = c->d_acc.p;
+  rc = reset_status(c);
+  if (rc) return rc;
+  int grid = 0;
+  TG_CHECK(c, launch_green(a, c->num_sms, s, &grid), "green (fermi column)");
+  TG_CHECK(c, launch_reduce_blocks(c->d_acc.p, grid, acc_len, c->d_acc_red.p, s), "reduce");
+  std::vector<double2> h(acc_len);
+  TG_CHECK(c, cudaMemcpyAsync(h.data(), c->d_acc_red.p, sizeof(double2) * acc_len, cudaMemcpyDeviceToHost, s), "copy");
+  rc = read_status(c);
+  if (rc) return rc;
+  // D(4, norb_max, n_atoms); orbital counter o runs over the sites' orbitals
+  int o = 0;
+  for (int i = 0; i < c->n_atoms; ++i) {
+    for (int mu = 0; mu < c->nmax; ++mu)
+      for (int q = 0; q < 4; ++q) {
+        const size_t dst = ((size_t)i * c->nmax + mu) * 4 + q;
+        if (mu < c->norb[i]) {
+          D[2 * dst] = h[4 * (o + mu) + q].x;
+          D[2 * dst + 1] = h[4 * (o + mu) + q].y;
+        } else {
+          D[2 * dst] = D[2 * dst + 1] = 0.0;
+        }
+      }
+    o += c->norb[i];
+  }
+  return TG_OK;
+}
+
+int tg_green_batch(tg_ctx* c, int64_t nz, const double* z, const double* kp, double* G) {
+  int rc = check_ready(c, false, false);
+  if (rc) return rc;
+  if (nz < 0 || (nz > 0 && (!z || !kp || !G))) return set_err(c, TG_ERR_ARG, "tg_green_batch: bad args");
+  if (nz == 0) return TG_OK;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int64_t nn = (int64_t)c->dimH * c->dimH;
+  TG_CHECK(c, c->d_zlist.upload(reinterpret_cast<const double2*>(z), nz, s), "upload z");
+  TG_CHECK(c, c->d_klist.upload(kp, 3 * nz, s), "upload k");
+  TG_CHECK(c, c->d_gout.ensure((size_t)nz * nn), "alloc G");
+  GreenArgs a = base_args(c);
+  a.pts.kind = 2;
+  a.pts.z = c->d_zlist.p;
+  a.pts.kp = c->d_klist.p;
+  a.np = nz;
+  a.mode = MODE_RAW;
+  a.out = c->d_gout.p;
+  rc = reset_status(c);
+  if (rc) return rc;
+  TG_CHECK(c, launch_green(a, c->num_sms, s, nullptr), "green (batch)");
+  TG_CHECK(c, cudaMemcpyAsync(G, c->d_gout.p, sizeof(double2) * nz * nn, cudaMemcpyDeviceToHost, s), "copy G");
+  return read_status(c);
+}
+
+int tg_hamiltk_batch(tg_ctx* c, int64_t nk, const double* kp, double* H) {
+  int rc = check_ready(c, false, false);
+  if (rc) return rc;
+  if (nk < 0 || (nk > 0 && (!kp || !H))) return set_err(c, TG_ERR_ARG, "tg_hamiltk_batch: bad args");
+  if (nk == 0) return TG_OK;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int64_t nn = (int64_t)c->dimH * c->dimH;
+  std::vector<double2> zeros(nk, make_double2(0.0, 0.0));
+  TG_CHECK(c, c->d_zlist.upload(zeros.data(), nk, s), "upload z");
+  TG_CHECK(c, c->d_klist.upload(kp, 3 * nk, s), "upload k");
+  TG_CHECK(c, c->d_gout.ensure((size_t)nk * nn), "alloc H");
+  GreenArgs a = base_args(c);
+  a.pts.kind = 2;
+  a.pts.z = c->d_zlist.p;
+  a.pts.kp = c->d_klist.p;
+  a.np = nk;
+  a.mode = MODE_HK;
+  a.out = c->d_gout.p;
+  TG_CHECK(c, launch_green(a, c->num_sms, s, nullptr), "hamiltk");
+  TG_CHECK(c, cudaMemcpyAsync(H, c->d_gout.p, sizeof(double2) * nk * nn, cudaMemcpyDeviceToHost, s), "copy H");
+  TG_CHECK(c, cudaStreamSynchronize(s), "sync");
+  return TG_OK;
+}
+
+int tg_dyson(tg_ctx* c, int dimens, const double* chi_hf, const double* umat, double* chi) {
+  if (!c) return TG_ERR_ARG;
+  if (dimens <= 0 || !chi_hf || !umat || !chi) return set_err(c, TG_ERR_ARG, "tg_dyson: bad args");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const size_t nn = (size_t)dimens * dimens;
+  TG_CHECK(c, c->d_dy.ensure(4 * nn), "alloc dyson");
+  TG_CHECK(c, c->d_piv.ensure(dimens), "alloc piv");
+  double2* X = c->d_dy.p;
+  double2* U = X + nn;
+  double2* W = U + nn;
+  double2* R = W + nn;
+  TG_CHECK(c, cudaMemcpyAsync(X, chi_hf, sizeof(double2) * nn, cudaMemcpyHostToDevice, s), "upload");
+  TG_CHECK(c, cudaMemcpyAsync(U, umat, sizeof(double2) * nn, cudaMemcpyHostToDevice, s), "upload");
+  int rc = reset_status(c);
+  if (rc) return rc;
+  if (dyson_device(dimens, X, U, W, R, c->d_piv.p, c->d_status.p, s) != 0)
+    return cuda_err(c, cudaGetLastError(), "dyson");
+  TG_CHECK(c, cudaMemcpyAsync(chi, R, sizeof(double2) * nn, cudaMemcpyDeviceToHost, s), "copy");
+  return read_status(c);
+}
+
+}  // extern "C"

@@ -1,0 +1,127 @@
+// Internal declarations shared by the CUDA translation units of libtitan_gpu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace tg {
+
+// ---------------------------------------------------------------------------
+// complex FP64 helpers (double2 = re, im)
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ double2 cmk(double r, double i) { return make_double2(r, i); }
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+// acc + a*b
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 acc) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+  return acc;
+}
+// acc - a*b
+__device__ __forceinline__ double2 cfms(double2 a, double2 b, double2 acc) {
+  acc.x = fma(-a.x, b.x, acc.x);
+  acc.x = fma(a.y, b.y, acc.x);
+  acc.y = fma(-a.x, b.y, acc.y);
+  acc.y = fma(-a.y, b.x, acc.y);
+  return acc;
+}
+// 1/a with scaling against overflow
+__device__ __forceinline__ double2 crecip(double2 a) {
+  double s = fmax(fabs(a.x), fabs(a.y));
+  if (s == 0.0) return make_double2(0.0, 0.0);
+  double xr = a.x / s, yr = a.y / s;
+  double den = s * (xr * xr + yr * yr);
+  return make_double2(xr / den, -yr / den);
+}
+
+// ---------------------------------------------------------------------------
+// Output transforms of the Green-function kernel
+// ---------------------------------------------------------------------------
+enum GreenMode : int {
+  MODE_RAW = 0,       // G column-major per point (test hook)
+  MODE_A_IMAG = 1,    // w * G, pair-block layout
+  MODE_B_IMAG = 2,    // G^T, pair-block layout
+  MODE_A_REAL = 3,    // w * (G - G^dagger), pair-block layout
+  MODE_B_REAL = 4,    // conj(G), pair-block layout
+  MODE_EXPECT = 5,    // accumulate diagonal site blocks (occupations / moments)
+  MODE_GG = 6,        // accumulate the orbital-diagonal GG tensor (Jacobian)
+  MODE_DIAG4 = 7,     // accumulate w * sigma-traces of diagonal orbitals (Fermi column)
+  MODE_HK = 8,        // H(k) only (no inversion), column-major per point
+};
+
+// A set of (k, z) points.  kind 0: flattened imaginary-axis list (y, kp, w per
+// point).  kind 1: real axis, point p = nep * nk + ik with energy x2[nep],
+// weight p2[nep] * w[ik], k = kp[ik].  kind 2: explicit (z, k) list (test hook).
+struct PointSet {
+  int kind = 0;
+  const double* y = nullptr;
+  const double* kp = nullptr;
+  const double* w = nullptr;
+  const double* x2 = nullptr;
+  const double* p2 = nullptr;
+  const double2* z = nullptr;
+  int64_t nk = 0;
+};
+
+struct GreenArgs {
+  PointSet pts;
+  int64_t p0 = 0, np = 0;     // point range
+  double zr = 0.0, zi = 0.0;  // z = (zr + x2) + i (zi + y)
+  double q[3] = {0, 0, 0};
+  int mode = MODE_RAW;
+  // system
+  int n = 0;                  // dimH
+  int n_neigh = 0;
+  const double* R = nullptr;  // [n_neigh][3]
+  const int* pair_start = nullptr;   // [nat*nat+1]
+  const int* pair_neigh = nullptr;   // [nblk]
+  const double2* pair_t = nullptr;   // [nblk][nmax*nmax], t(or, oc) at oc*nmax + or
+  int nmax = 0;
+  int n_atoms = 0;
+  const int* row_atom = nullptr;     // [n]
+  const int* row_orb = nullptr;      // [n]
+  const int* row_spin = nullptr;     // [n]
+  const double2* h0 = nullptr;       // column-major n x n
+  // outputs
+  double2* out = nullptr;            // per-point operand / matrix
+  double2* out2 = nullptr;           // optional second operand from the same inverse
+  int mode2 = MODE_RAW;
+  const int* outmap = nullptr;       // [n*n] row*n + col of pair-block slot o
+  double2* acc = nullptr;            // per-CTA accumulators (EXPECT / GG / DIAG4)
+  int acc_len = 0;                   // complex entries per CTA
+  const int* gg_desc = nullptr;      // GG entry descriptors
+  int* status = nullptr;             // first singular point (1-based), atomicMin
+};
+
+// Launch the fused H(k) + Gauss-Jordan kernel for any supported n.
+// Returns cudaErrorInvalidValue for an unsupported dimension.
+cudaError_t launch_green(const GreenArgs& a, int num_sms, cudaStream_t s, int* grid_used);
+int green_supported(int n);
+int green_acc_ctas(int n, int64_t np, int num_sms);
+
+// FP64 pair-block contraction: Cpart[split][cpair_off + u*M + v] += sum_p A[p][off+u] B[p][off+v]
+struct PairTile { int pair; int u0; int v0; };
+cudaError_t launch_gemm64(const double2* A, const double2* B, int64_t ld, int64_t np, int nsplit,
+                          const PairTile* tiles, int ntiles, const int* pair_M, const int* pair_aoff,
+                          const int64_t* pair_coff, double2* Cpart, int64_t cstride, cudaStream_t s);
+
+// chi assembly: chi(R, C) column-major from C/D partial sums.
+cudaError_t launch_chi_epilogue(const double2* Cpart, const double2* Dpart, int nsplit, int64_t cstride,
+                                int dimens, const int* decode, const int* norb, const int64_t* pair_coff,
+                                int n_atoms, double scale, double2* chi, cudaStream_t s);
+
+int gemm64_tile();
+cudaError_t launch_reduce_blocks(const double2* part, int nblocks, int len, double2* out, cudaStream_t s);
+
+}  // namespace tg

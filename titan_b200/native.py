@@ -1,0 +1,251 @@
+"""ctypes binding of libtitan_gpu (include/titan_gpu.h).
+
+``GreenGPU`` is the host-side mirror of the reference's Green-function call
+surface: ``chi0`` replaces eintshechi(q, e) (eintshechi.F90:2), ``expectation``
+replaces expectation_values_greenfunction (mod_expectation.F90:28),
+``gg_tensor`` / ``fermi_column`` feed calcJacobian_greenfunction
+(mod_self_consistency.F90:795), ``green_batch`` is green() for a batch
+(mod_greenfunction.F90:19).  Arrays cross the boundary in Fortran order, as
+the C ABI specifies.  There is no CPU fallback: constructing a GreenGPU
+without the built library or without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtitan_gpu.so")
+
+TG_PREC_FP64 = 0
+TG_PREC_SPLIT = 1
+_PREC = {"fp64": TG_PREC_FP64, "split": TG_PREC_SPLIT}
+
+_lib = None
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+SIGNATURES = {
+    "tg_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "tg_destroy": (C.c_int, [C.c_void_p]),
+    "tg_last_error": (C.c_char_p, [C.c_void_p]),
+    "tg_set_system": (C.c_int, [C.c_void_p, C.c_int, _ip, C.c_int, C.c_int, _dp, _ip, _ip, _dp]),
+    "tg_set_h0": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "tg_set_imag_mesh": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp]),
+    "tg_set_real_mesh": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp]),
+    "tg_chi0": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp,
+                          C.c_int, C.c_int, _dp]),
+    "tg_chi0_batch": (C.c_int, [C.c_void_p, _dp, C.c_int, _dp, C.c_double, C.c_double, C.c_double, C.c_int, _dp,
+                                _dp, C.c_int, C.c_int, _dp]),
+    "tg_expectation": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp]),
+    "tg_gg_tensor": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int, _ip, _dp]),
+    "tg_fermi_column": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
+    "tg_dyson": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),
+    "tg_green_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp]),
+    "tg_hamiltk_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp]),
+    "tg_last_timing": (C.c_int, [C.c_void_p, _dp]),
+    "tg_profile": (C.c_int, [C.c_void_p, C.c_int]),
+}
+
+
+class TitanGPUError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the shared library and declare every entry point of titan_gpu.h."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is not built (run: python -m titan_b200.build)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p(a, ctype=C.c_double):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def _fortran_complex(m):
+    """numpy [row, col] complex matrix -> Fortran-ordered complex128 buffer."""
+    return np.ascontiguousarray(np.asarray(m, dtype=np.complex128).T)
+
+
+class GreenGPU:
+    """One context on one GPU (tg_create / tg_destroy)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.tg_create(device, C.byref(h))
+        if rc != 0:
+            raise TitanGPUError(rc, f"tg_create(device={device}) failed (no usable CUDA device?)")
+        self.h = h
+        self.system = None
+        self.dimH = 0
+        self.dimens = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = self.lib.tg_last_error(self.h)
+            raise TitanGPUError(rc, msg.decode() if msg else "")
+        return rc
+
+    # ---- set-up -----------------------------------------------------------
+    def set_system(self, system):
+        """Neighbour table of a TBSystem (the calchk data)."""
+        cv, bi, ish, t = system.neighbor_table()
+        nat = system.n_atoms
+        nmax = max(system.norbs)
+        norb = np.array(system.norbs, np.int32)
+        cvF = np.ascontiguousarray(cv, np.float64)                       # (3, nNeigh) Fortran
+        biF = np.ascontiguousarray(bi + 1, np.int32)                     # 1-based
+        ishF = np.ascontiguousarray(ish, np.int32)                       # (nAtoms, nNeigh) Fortran
+        # t[k, i, b, a] = t0i(b, a, i) of neighbour k -> Fortran t0i(b, a, i, k)
+        tF = np.ascontiguousarray(np.transpose(t, (0, 1, 3, 2)), np.complex128)
+        rc = self.lib.tg_set_system(self.h, nat, _p(norb, C.c_int), nmax, cv.shape[0], _p(cvF), _p(biF, C.c_int),
+                                    _p(ishF, C.c_int), _p(tF.view(np.float64)))
+        self._check(rc)
+        self.system = system
+        self.dimH = system.dimH
+        self.dimens = system.dimens
+        self.nmax = nmax
+
+    def set_h0(self, h0):
+        hF = _fortran_complex(h0)
+        self._check(self.lib.tg_set_h0(self.h, self.dimH, _p(hF.view(np.float64))))
+
+    def set_imag_mesh(self, ek):
+        self.set_imag_mesh_arrays(np.ascontiguousarray(ek.point_energy(), np.float64),
+                                  np.ascontiguousarray(ek.kp, np.float64),
+                                  np.ascontiguousarray(ek.weight, np.float64))
+
+    def set_imag_mesh_arrays(self, y, kp, w):
+        """Flattened (E, k) list from contiguous float64 arrays (may be pinned host memory)."""
+        self._check(self.lib.tg_set_imag_mesh(self.h, y.shape[0], _p(y), _p(kp), _p(w)))
+
+    def set_real_mesh(self, kp, w):
+        kp = np.ascontiguousarray(kp, np.float64)
+        w = np.ascontiguousarray(w, np.float64)
+        self._check(self.lib.tg_set_real_mesh(self.h, w.shape[0], _p(kp), _p(w)))
+
+    def setup(self, deck, h0):
+        self.set_system(deck.system)
+        self.set_h0(h0)
+        self.set_imag_mesh(deck.ek)
+        self.set_real_mesh(deck.real_kp, deck.real_w)
+
+    # ---- hot path -----------------------------------------------------------
+    def chi0(self, q, e, Ef, eta, etap, x2=None, p2=None, precision="fp64"):
+        """chiorb_hf(q, e) as a [dimens, dimens] numpy array (eintshechi)."""
+        return self.chi0_batch(q, [e], Ef, eta, etap, None if x2 is None else [x2], None if p2 is None else [p2],
+                               precision)[0]
+
+    def chi0_batch(self, q, es, Ef, eta, etap, x2s=None, p2s=None, precision="fp64", out=None):
+        es = np.ascontiguousarray(es, np.float64)
+        nw = es.shape[0]
+        nreal = 0
+        if x2s is not None:
+            nreal = max(len(x) for x in x2s)
+        X2 = np.zeros((nw, max(nreal, 1)))
+        P2 = np.zeros((nw, max(nreal, 1)))
+        if nreal:
+            for w in range(nw):
+                if len(x2s[w]):
+                    X2[w, :len(x2s[w])] = x2s[w]
+                    P2[w, :len(p2s[w])] = p2s[w]
+        qa = np.ascontiguousarray(q, np.float64)
+        D = self.dimens
+        buf = out if out is not None else np.empty((nw, D, D), np.complex128)
+        rc = self.lib.tg_chi0_batch(self.h, _p(qa), nw, _p(es), Ef, eta, etap, nreal, _p(X2), _p(P2),
+                                    _PREC[precision], D, _p(buf.view(np.float64)))
+        self._check(rc)
+        return np.swapaxes(buf, 1, 2)      # Fortran (row, col) -> numpy [row, col]
+
+    def last_timing(self):
+        """Device ms of the last chi0 call (see tg_last_timing)."""
+        ms = np.zeros(11)
+        self._check(self.lib.tg_last_timing(self.h, _p(ms)))
+        return ms
+
+    def profile(self, enable=True):
+        self._check(self.lib.tg_profile(self.h, 1 if enable else 0))
+
+    def expectation(self, Ef, eta):
+        """rho, mx, my, mz [nAtoms, nOrbMax] and mp (mod_expectation.F90:28-149)."""
+        nat = self.system.n_atoms
+        out = [np.zeros((nat, self.nmax)) for _ in range(4)]
+        mp = np.zeros((nat, self.nmax), np.complex128)
+        rc = self.lib.tg_expectation(self.h, Ef, eta, *[_p(o) for o in out], _p(mp.view(np.float64)))
+        self._check(rc)
+        return out[0], out[1], out[2], out[3], mp
+
+    def gg_tensor(self, Ef, eta, orbital_resolved=True):
+        """GG tensor T[i, j, g, h, 16] (see titan_gpu.h)."""
+        s = self.system
+        nat = s.n_atoms
+        dmask = np.zeros((nat, self.nmax), np.int32)
+        for i, dl in enumerate(s.dorbs):
+            dmask[i, dl] = 1
+        if orbital_resolved:
+            nrow = max(len(d) for d in s.dorbs) + 1
+            ncol = max(len(d) for d in s.dorbs)
+        else:
+            nrow = ncol = 1
+        T = np.zeros((nat, nat, nrow, ncol, 16), np.complex128)
+        rc = self.lib.tg_gg_tensor(self.h, Ef, eta, 1 if orbital_resolved else 0, _p(dmask, C.c_int),
+                                   _p(T.view(np.float64)))
+        self._check(rc)
+        return T
+
+    def fermi_column(self, Ef, eta):
+        nat = self.system.n_atoms
+        D = np.zeros((nat, self.nmax, 4), np.complex128)
+        self._check(self.lib.tg_fermi_column(self.h, Ef, eta, _p(D.view(np.float64))))
+        return D
+
+    def dyson(self, chi_hf, U):
+        n = chi_hf.shape[0]
+        a = _fortran_complex(chi_hf)
+        u = _fortran_complex(U)
+        out = np.empty((n, n), np.complex128)
+        self._check(self.lib.tg_dyson(self.h, n, _p(a.view(np.float64)), _p(u.view(np.float64)),
+                                      _p(out.view(np.float64))))
+        return out.T
+
+    def green_batch(self, z, kp):
+        z = np.ascontiguousarray(z, np.complex128)
+        kp = np.ascontiguousarray(kp, np.float64).reshape(-1, 3)
+        nz = z.shape[0]
+        G = np.empty((nz, self.dimH, self.dimH), np.complex128)
+        self._check(self.lib.tg_green_batch(self.h, nz, _p(z.view(np.float64)), _p(kp), _p(G.view(np.float64))))
+        return np.swapaxes(G, 1, 2)
+
+    def hamiltk_batch(self, kp):
+        kp = np.ascontiguousarray(kp, np.float64).reshape(-1, 3)
+        nk = kp.shape[0]
+        H = np.empty((nk, self.dimH, self.dimH), np.complex128)
+        self._check(self.lib.tg_hamiltk_batch(self.h, nk, _p(kp), _p(H.view(np.float64))))
+        return np.swapaxes(H, 1, 2)
