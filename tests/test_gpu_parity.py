@@ -156,3 +156,22 @@ def test_dyson_matches_numpy(gpu):
     out = gpu.dyson(chi, U)
     ref = O.dyson(chi, U)
     assert rel(out, ref) < 1e-12
+
+
+def test_chi0_adaptive_mesh_matches_oracle(gpu):
+    """Non-uniform (E, k) list: per-energy k counts decay (adaptiveMesh.F90:199-218)."""
+    from titan_b200.host.deck import Deck
+    base = synthetic.make_deck("bcc1", nk=(4, 4, 4), n1gl=6, parts=1, n3gl=4, mesh=False)
+    p = dict(base.params)
+    p["nk_per_energy"] = [64, 64, 27, 27, 8, 8]
+    deck = Deck.from_system(base.system, p, True)
+    s, h0 = _setup(gpu, deck)
+    e = 0.04
+    x2, p2 = deck.real_points(e, s.Ef)
+    chi = gpu.chi0(np.zeros(3), e, s.Ef, s.eta, s.etap, x2, p2)
+    ref = O.eintshechi(O.Model(s, h0), deck.ek, (deck.real_kp, deck.real_w), np.zeros(3), e, s.Ef, s.eta,
+                       s.etap, x2, p2)
+    assert rel(chi, ref) < 1e-10
+    rho, mx, my, mz, mp = gpu.expectation(s.Ef, s.eta)
+    r2, x2_, y2, z2, mp2 = O.expectation(O.Model(s, h0), deck.ek, s.Ef, s.eta)
+    assert np.max(np.abs(rho - r2)) < 1e-12 and np.max(np.abs(mz - z2)) < 1e-12

@@ -82,6 +82,11 @@ struct tg_ctx {
   // meshes
   int64_t n_imag = 0, n_realk = 0;
   DevArray<double> d_y, d_kp, d_w, d_rkp, d_rw, d_x2, d_p2;
+  // uniform imaginary-axis mesh: n_e energies x the same nk_u k points (energy-major)
+  bool imag_uniform = false;
+  int64_t n_e_u = 0, nk_u = 0;
+  DevArray<double> d_ylist, d_klist_u, d_qvec;
+  DevArray<double2> d_htab[4], d_hphase;   // H(k), H(k+q) for the imaginary and real k lists
   // workspace
   DevArray<double2> d_A, d_B, d_C, d_D, d_chi, d_acc, d_acc_red;
   DevArray<double2> d_zlist, d_gout;
@@ -238,6 +243,18 @@ int nsplit_for(tg_ctx* c) {
   return std::min(s, 64);
 }
 
+// H(k + q) table for a k list into d_htab[slot]
+int build_htab(tg_ctx* c, int slot, const double* d_k, int64_t nk, const double* q) {
+  const size_t nn = (size_t)c->dimH * c->dimH;
+  TG_CHECK(c, c->d_htab[slot].ensure((size_t)nk * nn), "alloc H table");
+  TG_CHECK(c, c->d_hphase.ensure((size_t)nk * std::max(c->n_neigh, 1)), "alloc phases");
+  TG_CHECK(c, c->d_qvec.upload(q, 3, c->stream), "upload q");
+  GreenArgs a = base_args(c);
+  TG_CHECK(c, launch_hk_table(a, d_k, nk, c->d_qvec.p, c->d_hphase.p, c->d_htab[slot].p, c->stream), "H table");
+  c->launches += 2;
+  return TG_OK;
+}
+
 // contraction of one pass into Cpart: FP64 SIMT path or the sliced tensor-core path
 int contract(tg_ctx* c, int precision, const double2* A, const double2* B, int64_t np, double2* Cpart,
              int nsplit, int64_t cstride) {
@@ -314,6 +331,8 @@ int tg_destroy(tg_ctx* c) {
   c->d_C.free_(); c->d_D.free_(); c->d_chi.free_(); c->d_acc.free_(); c->d_acc_red.free_(); c->d_zlist.free_();
   c->d_gout.free_(); c->d_klist.free_(); c->d_status.free_(); c->d_split_ws.free_();
   c->d_dy.free_(); c->d_piv.free_();
+  c->d_ylist.free_(); c->d_klist_u.free_(); c->d_qvec.free_(); c->d_hphase.free_();
+  for (int t = 0; t < 4; ++t) c->d_htab[t].free_();
   for (int i = 0; i < 8; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -473,6 +492,30 @@ int tg_set_imag_mesh(tg_ctx* c, int64_t n_points, const double* y, const double*
   TG_CHECK(c, c->d_y.upload(y, n_points, c->stream), "upload y");
   TG_CHECK(c, c->d_kp.upload(kp, 3 * n_points, c->stream), "upload kp");
   TG_CHECK(c, c->d_w.upload(w, n_points, c->stream), "upload w");
+  // uniform structure: consecutive blocks of constant y, all with the first block's k list
+  c->imag_uniform = false;
+  if (n_points > 0) {
+    int64_t nk = 1;
+    while (nk < n_points && y[nk] == y[0]) ++nk;
+    bool ok = (n_points % nk) == 0;
+    const int64_t ne = ok ? n_points / nk : 0;
+    std::vector<double> ylist;
+    for (int64_t e = 0; ok && e < ne; ++e) {
+      const double ye = y[e * nk];
+      ylist.push_back(ye);
+      for (int64_t i = 0; i < nk && ok; ++i) {
+        const int64_t p = e * nk + i;
+        ok = y[p] == ye && kp[3 * p] == kp[3 * i] && kp[3 * p + 1] == kp[3 * i + 1] && kp[3 * p + 2] == kp[3 * i + 2];
+      }
+    }
+    if (ok && ne > 1) {
+      TG_CHECK(c, c->d_ylist.upload(ylist.data(), ne, c->stream), "upload ylist");
+      TG_CHECK(c, c->d_klist_u.upload(kp, 3 * nk, c->stream), "upload klist");
+      c->imag_uniform = true;
+      c->n_e_u = ne;
+      c->nk_u = nk;
+    }
+  }
   TG_CHECK(c, cudaStreamSynchronize(c->stream), "sync");
   c->n_imag = n_points;
   c->imag_set = true;
@@ -527,8 +570,26 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   float t_green = 0, t_con = 0, t_epi = 0;
   cudaEvent_t *ev = c->ev;
   TG_CHECK(c, cudaEventRecord(ev[0], s), "event");
-  // ---------------- imaginary axis ----------------
+  // ---------------- H(k) tables (k-major traversal) ----------------
   const bool q_zero = q[0] == 0.0 && q[1] == 0.0 && q[2] == 0.0;
+  const double zero3[3] = {0.0, 0.0, 0.0};
+  const bool tab_imag = c->imag_uniform && (int64_t)c->nk_u * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
+  const bool tab_real = any_real && (int64_t)c->n_realk * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
+  if (tab_imag) {
+    if ((rc = build_htab(c, 0, c->d_klist_u.p, c->nk_u, zero3))) return rc;
+    if (!q_zero && (rc = build_htab(c, 1, c->d_klist_u.p, c->nk_u, q))) return rc;
+  }
+  if (tab_real) {
+    if ((rc = build_htab(c, 2, c->d_rkp.p, c->n_realk, zero3))) return rc;
+    if (!q_zero && (rc = build_htab(c, 3, c->d_rkp.p, c->n_realk, q))) return rc;
+  }
+  auto use_table = [&](GreenArgs& g, int slot, int64_t n_e, int64_t nk, const double* ylist) {
+    g.htab = c->d_htab[slot].p;
+    g.n_e = n_e;
+    g.nk_tab = nk;
+    g.ylist = ylist;
+  };
+  // ---------------- imaginary axis ----------------
   for (int64_t p0 = 0; p0 < c->n_imag; p0 += P) {
     const int64_t np = std::min<int64_t>(P, c->n_imag - p0);
     GreenArgs g2 = base_args(c);
@@ -542,6 +603,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     g2.zi = etap;
     g2.mode = MODE_B_IMAG;
     g2.out = c->d_B.p;
+    if (tab_imag) use_table(g2, 0, c->n_e_u, c->nk_u, c->d_ylist.p);
     // G1 = G2 when e = 0, q = 0 and eta = eta': one inversion feeds both operands
     int w_start = 0;
     if (e[0] == 0.0 && q_zero && eta == etap) {
@@ -562,15 +624,17 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       if (rc) return rc;
     }
     for (int w = w_start; w < n_omega; ++w) {
-      GreenArgs g1 = base_args(c);
-      g1.pts = g2.pts;
-      g1.p0 = p0;
-      g1.np = np;
+      GreenArgs g1 = g2;
+      g1.out2 = nullptr;
       g1.zr = Ef + e[w];
       g1.zi = eta;
       g1.q[0] = q[0]; g1.q[1] = q[1]; g1.q[2] = q[2];
       g1.mode = MODE_A_IMAG;
       g1.out = c->d_A.p;
+      if (tab_imag) {
+        use_table(g1, q_zero ? 0 : 1, c->n_e_u, c->nk_u, c->d_ylist.p);
+        g1.q[0] = g1.q[1] = g1.q[2] = 0.0;   // q is inside the table
+      }
       {
         KindTimer kt(c, 0);
         TG_CHECK(c, launch_green(g1, c->num_sms, s, nullptr), "green (imag, G1)");
@@ -608,6 +672,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       gr.zi = etap;
       gr.mode = MODE_B_REAL;
       gr.out = c->d_B.p;
+      if (tab_real) use_table(gr, 2, n_real, c->n_realk, nullptr);
       {
         KindTimer kt(c, 0);
         TG_CHECK(c, launch_green(gr, c->num_sms, s, nullptr), "green (real, G2)");
@@ -618,6 +683,10 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       gr.q[0] = q[0]; gr.q[1] = q[1]; gr.q[2] = q[2];
       gr.mode = MODE_A_REAL;
       gr.out = c->d_A.p;
+      if (tab_real) {
+        use_table(gr, q_zero ? 2 : 3, n_real, c->n_realk, nullptr);
+        gr.q[0] = gr.q[1] = gr.q[2] = 0.0;
+      }
       {
         KindTimer kt(c, 0);
         TG_CHECK(c, launch_green(gr, c->num_sms, s, nullptr), "green (real, G1)");
@@ -697,6 +766,14 @@ int tg_expectation(tg_ctx* c, double Ef, double eta, double* rho, double* mx, do
   a.zi = eta;
   a.mode = MODE_EXPECT;
   a.gg_desc = c->d_exp_rows.p;
+  if (c->imag_uniform && (int64_t)c->nk_u * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30)) {
+    const double zero3[3] = {0.0, 0.0, 0.0};
+    if ((rc = build_htab(c, 0, c->d_klist_u.p, c->nk_u, zero3))) return rc;
+    a.htab = c->d_htab[0].p;
+    a.n_e = c->n_e_u;
+    a.nk_tab = c->nk_u;
+    a.ylist = c->d_ylist.p;
+  }
   const int maxgrid = c->num_sms * 8;
   TG_CHECK(c, c->d_acc.ensure((size_t)maxgrid * len), "alloc acc");
   TG_CHECK(c, c->d_acc_red.ensure(len), "alloc acc");

@@ -45,6 +45,31 @@ __device__ __forceinline__ double2 crecip(double2 a) {
   return make_double2(xr / den, -yr / den);
 }
 
+// Reciprocal of a positive double by Newton-Raphson: start from the
+// hardware approximation (rcp.approx.ftz.f64, about 20 correct bits) and
+// apply r <- r + r (1 - s r) three times (quadratic convergence, so well past
+// 53 bits); the result is within a few ulp of 1/s.
+__device__ __forceinline__ double rcp_newton(double s) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(s));
+  double e = fma(-s, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-s, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-s, r, 1.0);
+  r = fma(r, e, r);
+  return r;
+}
+
+// 1/a = conj(a) / |a|^2 for pivots of moderate magnitude (|a|^2 well inside
+// the double range, true for z - H(k) entries); returns 0 for a == 0.
+__device__ __forceinline__ double2 crecip_fast(double2 a) {
+  const double s = fma(a.x, a.x, a.y * a.y);
+  if (s == 0.0) return make_double2(0.0, 0.0);
+  const double r = rcp_newton(s);
+  return make_double2(a.x * r, -a.y * r);
+}
+
 // ---------------------------------------------------------------------------
 // Output transforms of the Green-function kernel
 // ---------------------------------------------------------------------------
@@ -102,12 +127,20 @@ struct GreenArgs {
   int acc_len = 0;                   // complex entries per CTA
   const int* gg_desc = nullptr;      // GG entry descriptors
   int* status = nullptr;             // first singular point (1-based), atomicMin
+  // optional precomputed H(k) table (row-major n x n per k) with a k-major
+  // traversal: work item wi -> k index wi / n_e, energy index wi % n_e
+  const double2* htab = nullptr;
+  int64_t n_e = 0;
+  int64_t nk_tab = 0;
+  const double* ylist = nullptr;     // imaginary parts of the energies (structured imaginary axis)
 };
 
 // Launch the fused H(k) + Gauss-Jordan kernel for any supported n.
 // Returns cudaErrorInvalidValue for an unsupported dimension.
 cudaError_t launch_green(const GreenArgs& a, int num_sms, cudaStream_t s, int* grid_used);
 int green_supported(int n);
+int green_warp_supported(int n, int mode);
+cudaError_t launch_green_warp(const GreenArgs& a, int num_sms, cudaStream_t s, int* grid_used);
 int green_acc_ctas(int n, int64_t np, int num_sms);
 
 // FP64 pair-block contraction: Cpart[split][cpair_off + u*M + v] += sum_p A[p][off+u] B[p][off+v]
@@ -122,6 +155,9 @@ cudaError_t launch_chi_epilogue(const double2* Cpart, const double2* Dpart, int 
                                 int n_atoms, double scale, double2* chi, cudaStream_t s);
 
 int gemm64_tile();
+// H(k) table for a k list (plus q): H[k][r][c] = h0 + H_nl(k + q)
+cudaError_t launch_hk_table(const GreenArgs& a, const double* kp, int64_t nk, const double* d_q, double2* phase_ws,
+                            double2* H, cudaStream_t s);
 cudaError_t launch_reduce_blocks(const double2* part, int nblocks, int len, double2* out, cudaStream_t s);
 
 }  // namespace tg
