@@ -175,3 +175,37 @@ def test_chi0_adaptive_mesh_matches_oracle(gpu):
     rho, mx, my, mz, mp = gpu.expectation(s.Ef, s.eta)
     r2, x2_, y2, z2, mp2 = O.expectation(O.Model(s, h0), deck.ek, s.Ef, s.eta)
     assert np.max(np.abs(rho - r2)) < 1e-12 and np.max(np.abs(mz - z2)) < 1e-12
+
+
+@pytest.mark.parametrize("shape,nk,e,q", [
+    ("bcc1", (4, 4, 4), 0.0, (0, 0, 0)),
+    ("bcc1", (3, 3, 3), 0.02, (0.1, 0.0, 0.2)),
+    ("sq2", (6, 6, 1), 0.0, (0, 0, 0)),
+    ("sq2", (5, 5, 1), 0.1, (0.05, 0.02, 0.0)),
+])
+def test_chi0_split_matches_fp64_and_oracle(gpu, shape, nk, e, q):
+    """int8-sliced tensor-core contraction: normwise relative error <= 1e-9."""
+    deck = synthetic.make_deck(shape, nk=nk, n1gl=8, parts=1, n3gl=6)
+    s, h0 = _setup(gpu, deck)
+    x2, p2 = deck.real_points(e, s.Ef)
+    qv = np.array(q, float)
+    sp = gpu.chi0(qv, e, s.Ef, s.eta, s.etap, x2, p2, precision="split")
+    fp = gpu.chi0(qv, e, s.Ef, s.eta, s.etap, x2, p2, precision="fp64")
+    assert rel(sp, fp) < 1e-9
+    ref = O.eintshechi(O.Model(s, h0), deck.ek, (deck.real_kp, deck.real_w), qv, e, s.Ef, s.eta, s.etap, x2, p2)
+    assert rel(sp, ref) < 1e-9
+
+
+def test_chi0_split_fe_golden(gpu, fe_deck, fe_chi_golden):
+    """The reference's Fe_bulk_susc chi_HF rows through the split-precision path."""
+    s = fe_deck.system
+    gpu.setup(fe_deck, s.h0(fe_deck.state))
+    ghf, _ = fe_chi_golden
+    for idx in (0, 5):
+        e = fe_deck.frequencies()[idx]
+        x2, p2 = fe_deck.real_points(e, s.Ef)
+        chi = gpu.chi0(np.zeros(3), e, s.Ef, s.eta, s.etap, x2, p2, precision="split")
+        hf_row = O.golden_row(s, e, 0.0, O.site_reduce(s, chi), 0, 0)
+        for a, b in zip(hf_row, ghf[idx]):
+            if abs(b) > 1e-6:
+                assert abs(a - b) <= 1e-8 * abs(b), (idx, a, b)

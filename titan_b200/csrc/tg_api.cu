@@ -92,7 +92,14 @@ struct tg_ctx {
   DevArray<double2> d_zlist, d_gout;
   DevArray<double> d_klist;
   DevArray<int> d_status;
-  DevArray<unsigned char> d_split_ws;
+  // split-precision contraction
+  SplitLayout split;
+  DevArray<SplitGroup> d_sgA, d_sgB;
+  DevArray<SplitTile> d_stiles;
+  DevArray<int8_t> d_digA, d_digB;
+  DevArray<unsigned long long> d_m64A, d_m64B;
+  DevArray<int> d_EA, d_EB, d_chunks, d_split_err;
+  std::vector<double> h_y;   // imaginary-axis energies per point (chunk boundaries)
   DevArray<double2> d_dy;
   DevArray<int> d_piv;
   cudaEvent_t ev[8] = {};
@@ -255,41 +262,103 @@ int build_htab(tg_ctx* c, int slot, const double* d_k, int64_t nk, const double*
   return TG_OK;
 }
 
-// contraction of one pass into Cpart: FP64 SIMT path or the sliced tensor-core path
-int contract(tg_ctx* c, int precision, const double2* A, const double2* B, int64_t np, double2* Cpart,
-             int nsplit, int64_t cstride) {
-  if (precision == TG_PREC_FP64) {
-    c->launches += 1;
-    TG_CHECK(c, launch_gemm64(A, B, (int64_t)c->dimH * c->dimH, np, nsplit, c->d_tiles.p, (int)c->tiles.size(),
-                              c->d_pair_M.p, c->d_pair_aoff.p, c->d_pair_coff.p, Cpart, cstride, c->stream),
-             "contraction (fp64)");
-    return TG_OK;
+// contraction of one pass into Cpart on the FP64 SIMT path
+int contract(tg_ctx* c, const double2* A, const double2* B, int64_t np, double2* Cpart, int nsplit,
+             int64_t cstride) {
+  c->launches += 1;
+  TG_CHECK(c, launch_gemm64(A, B, (int64_t)c->dimH * c->dimH, np, nsplit, c->d_tiles.p, (int)c->tiles.size(),
+                            c->d_pair_M.p, c->d_pair_aoff.p, c->d_pair_coff.p, Cpart, cstride, c->stream),
+           "contraction (fp64)");
+  return TG_OK;
+}
+
+// chunks of a pass: runs of equal key (energy), at most kSplitMaxChunk points each
+template <class Key>
+SplitChunks make_chunks(int64_t np, Key key) {
+  SplitChunks ch;
+  int64_t i = 0;
+  ch.kstart.push_back(0);
+  while (i < np) {
+    const auto k0 = key(i);
+    int64_t j = i + 1;
+    while (j < np && j - i < kSplitMaxChunk && key(j) == k0) ++j;
+    const int cnt = (int)(j - i);
+    const int nk = (cnt + kSplitK - 1) / kSplitK;
+    const int ci = (int)ch.count.size();
+    ch.slot0.push_back((int)i);
+    ch.count.push_back(cnt);
+    ch.kstart.push_back(ch.kstart.back() + nk);
+    for (int t = 0; t < nk; ++t) ch.kchunk.push_back(ci);
+    i = j;
   }
-  SplitArgs sa;
-  sa.A = A;
-  sa.B = B;
+  return ch;
+}
+
+// uploads the chunk tables and sizes the digit / exponent buffers of a pass
+int split_prepare(tg_ctx* c, const SplitChunks& ch, SplitPassDev& pd) {
+  const int nc = ch.n_chunks(), nks = ch.n_ksteps();
+  std::vector<int> buf;
+  buf.reserve(3 * nc + 1 + nks);
+  buf.insert(buf.end(), ch.slot0.begin(), ch.slot0.end());
+  buf.insert(buf.end(), ch.count.begin(), ch.count.end());
+  buf.insert(buf.end(), ch.kstart.begin(), ch.kstart.end());
+  buf.insert(buf.end(), ch.kchunk.begin(), ch.kchunk.end());
+  TG_CHECK(c, c->d_chunks.upload(buf.data(), buf.size(), c->stream), "upload chunks");
+  pd.n_chunks = nc;
+  pd.n_ksteps = nks;
+  pd.slot0 = c->d_chunks.p;
+  pd.count = c->d_chunks.p + nc;
+  pd.kstart = c->d_chunks.p + 2 * nc;
+  pd.kchunk = c->d_chunks.p + 3 * nc + 1;
+  const size_t ld = (size_t)c->dimH * c->dimH;
+  TG_CHECK(c, c->d_digA.ensure((size_t)nks * c->split.groupsA.size() * kSplitABlock), "alloc digits A");
+  TG_CHECK(c, c->d_digB.ensure((size_t)nks * c->split.groupsB.size() * kSplitBBlock), "alloc digits B");
+  TG_CHECK(c, c->d_m64A.ensure((size_t)nc * ld), "alloc");
+  TG_CHECK(c, c->d_m64B.ensure((size_t)nc * ld), "alloc");
+  TG_CHECK(c, c->d_EA.ensure((size_t)nc * ld), "alloc");
+  TG_CHECK(c, c->d_EB.ensure((size_t)nc * ld), "alloc");
+  return TG_OK;
+}
+
+// FP64 operand of a pass -> digits (which = 0: A, 1: B)
+int split_quantize_operand(tg_ctx* c, int which, const double2* X, const SplitPassDev& pd) {
+  const int64_t ld = (int64_t)c->dimH * c->dimH;
+  unsigned long long* m64 = which ? c->d_m64B.p : c->d_m64A.p;
+  TG_CHECK(c, cudaMemsetAsync(m64, 0, sizeof(unsigned long long) * pd.n_chunks * ld, c->stream), "memset");
+  TG_CHECK(c, split_rowmax(X, ld, pd, m64, c->stream), "split rowmax");
+  if (which == 0)
+    TG_CHECK(c, split_quantize(X, ld, pd, c->d_sgA.p, (int)c->split.groupsA.size(), kSplitRowsA, m64, c->d_EA.p,
+                               c->d_digA.p, c->stream),
+             "split quantize A");
+  else
+    TG_CHECK(c, split_quantize(X, ld, pd, c->d_sgB.p, (int)c->split.groupsB.size(), kSplitColsB, m64, c->d_EB.p,
+                               c->d_digB.p, c->stream),
+             "split quantize B");
+  c->launches += 2;
+  return TG_OK;
+}
+
+int split_contract_pass(tg_ctx* c, const SplitPassDev& pd, double2* Cpart, int nsplit, int64_t cstride) {
+  SplitContractArgs sa;
+  sa.A = c->d_digA.p;
+  sa.B = c->d_digB.p;
+  sa.GA = (int)c->split.groupsA.size();
+  sa.GB = (int)c->split.groupsB.size();
+  sa.tiles = c->d_stiles.p;
+  sa.ntiles = (int)c->split.tiles.size();
+  sa.nsplit = nsplit;
+  sa.pass = pd;
+  sa.EA = c->d_EA.p;
+  sa.EB = c->d_EB.p;
   sa.ld = (int64_t)c->dimH * c->dimH;
-  sa.np = np;
-  sa.n_pairs = c->n_atoms * c->n_atoms;
-  sa.pair_M = c->pair_M.data();
-  sa.pair_aoff = c->pair_aoff.data();
-  sa.pair_coff = c->pair_coff.data();
-  sa.d_pair_M = c->d_pair_M.p;
-  sa.d_pair_aoff = c->d_pair_aoff.p;
-  sa.d_pair_coff = c->d_pair_coff.p;
-  sa.C = Cpart;   // split partial 0 receives the FP64 recombination
-  sa.num_sms = c->num_sms;
-  size_t need = split_workspace_bytes(sa);
-  TG_CHECK(c, c->d_split_ws.ensure(need), "split workspace");
-  sa.ws = c->d_split_ws.p;
-  sa.ws_bytes = c->d_split_ws.n;
-  int nl = 0;
-  cudaError_t e = launch_split_contraction(sa, c->stream, &nl);
-  c->launches += nl;
-  if (e == cudaErrorNotSupported) return set_err(c, TG_ERR_ARG, "split-precision contraction: unsupported pair size");
-  TG_CHECK(c, e, "contraction (split)");
-  (void)nsplit;
-  (void)cstride;
+  sa.pair_M = c->d_pair_M.p;
+  sa.pair_aoff = c->d_pair_aoff.p;
+  sa.pair_coff = c->d_pair_coff.p;
+  sa.C = Cpart;
+  sa.cstride = cstride;
+  sa.err = c->d_split_err.p;
+  c->launches += 1;
+  TG_CHECK(c, split_contract(sa, c->stream), "contraction (split)");
   return TG_OK;
 }
 
@@ -329,7 +398,9 @@ int tg_destroy(tg_ctx* c) {
   c->d_pair_t.free_(); c->d_h0.free_(); c->d_tiles.free_(); c->d_y.free_(); c->d_kp.free_(); c->d_w.free_();
   c->d_rkp.free_(); c->d_rw.free_(); c->d_x2.free_(); c->d_p2.free_(); c->d_A.free_(); c->d_B.free_();
   c->d_C.free_(); c->d_D.free_(); c->d_chi.free_(); c->d_acc.free_(); c->d_acc_red.free_(); c->d_zlist.free_();
-  c->d_gout.free_(); c->d_klist.free_(); c->d_status.free_(); c->d_split_ws.free_();
+  c->d_gout.free_(); c->d_klist.free_(); c->d_status.free_();
+  c->d_sgA.free_(); c->d_sgB.free_(); c->d_stiles.free_(); c->d_digA.free_(); c->d_digB.free_();
+  c->d_m64A.free_(); c->d_m64B.free_(); c->d_EA.free_(); c->d_EB.free_(); c->d_chunks.free_(); c->d_split_err.free_();
   c->d_dy.free_(); c->d_piv.free_();
   c->d_ylist.free_(); c->d_klist_u.free_(); c->d_qvec.free_(); c->d_hphase.free_();
   for (int t = 0; t < 4; ++t) c->d_htab[t].free_();
@@ -467,6 +538,10 @@ int tg_set_system(tg_ctx* c, int n_atoms, const int* norb, int norb_max, int n_n
   TG_CHECK(c, c->d_pair_coff.upload(c->pair_coff.data(), np2, s), "upload");
   TG_CHECK(c, c->d_tiles.upload(c->tiles.data(), c->tiles.size(), s), "upload");
   TG_CHECK(c, c->d_exp_rows.upload(exprows.data(), exprows.size(), s), "upload");
+  split_build_layout(np2, c->pair_M.data(), c->pair_aoff.data(), c->split);
+  TG_CHECK(c, c->d_sgA.upload(c->split.groupsA.data(), c->split.groupsA.size(), s), "upload");
+  TG_CHECK(c, c->d_sgB.upload(c->split.groupsB.data(), c->split.groupsB.size(), s), "upload");
+  TG_CHECK(c, c->d_stiles.upload(c->split.tiles.data(), c->split.tiles.size(), s), "upload");
   TG_CHECK(c, cudaStreamSynchronize(s), "sync");
   c->sys_set = true;
   c->h0_set = false;
@@ -492,6 +567,7 @@ int tg_set_imag_mesh(tg_ctx* c, int64_t n_points, const double* y, const double*
   TG_CHECK(c, c->d_y.upload(y, n_points, c->stream), "upload y");
   TG_CHECK(c, c->d_kp.upload(kp, 3 * n_points, c->stream), "upload kp");
   TG_CHECK(c, c->d_w.upload(w, n_points, c->stream), "upload w");
+  c->h_y.assign(y, y + n_points);
   // uniform structure: consecutive blocks of constant y, all with the first block's k list
   c->imag_uniform = false;
   if (n_points > 0) {
@@ -549,10 +625,15 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   cudaStream_t s = c->stream;
   const int n = c->dimH;
   const int64_t nn = (int64_t)n * n;
-  const int nsplit = (precision == TG_PREC_FP64) ? nsplit_for(c) : 1;
+  const bool split = precision == TG_PREC_SPLIT;
   const int64_t cstride = (int64_t)c->dimens * c->dimens;
   // workspace
   const int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, (int64_t)n_real * c->n_realk));
+  const int nsplit = split ? split_nsplit((int)c->split.tiles.size(), c->num_sms, P / kSplitK) : nsplit_for(c);
+  if (split) {
+    TG_CHECK(c, c->d_split_err.ensure(1), "alloc");
+    TG_CHECK(c, cudaMemsetAsync(c->d_split_err.p, 0, sizeof(int), s), "memset");
+  }
   TG_CHECK(c, c->d_A.ensure((size_t)P * nn), "alloc A");
   TG_CHECK(c, c->d_B.ensure((size_t)P * nn), "alloc B");
   TG_CHECK(c, c->d_C.ensure((size_t)n_omega * nsplit * cstride), "alloc C");
@@ -618,9 +699,21 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     }
     cudaEventRecord(ev[2], s);
     float ms = 0;
+    SplitPassDev pd;
+    if (split) {
+      KindTimer kt(c, 1);
+      const double* yv = c->h_y.data() + p0;
+      if ((rc = split_prepare(c, make_chunks(np, [&](int64_t i) { return yv[i]; }), pd))) return rc;
+      if ((rc = split_quantize_operand(c, 1, c->d_B.p, pd))) return rc;
+    }
     if (w_start == 1) {
       KindTimer kt(c, 1);
-      rc = contract(c, precision, c->d_A.p, c->d_B.p, np, c->d_C.p, nsplit, cstride);
+      if (split) {
+        if ((rc = split_quantize_operand(c, 0, c->d_A.p, pd))) return rc;
+        rc = split_contract_pass(c, pd, c->d_C.p, nsplit, cstride);
+      } else {
+        rc = contract(c, c->d_A.p, c->d_B.p, np, c->d_C.p, nsplit, cstride);
+      }
       if (rc) return rc;
     }
     for (int w = w_start; w < n_omega; ++w) {
@@ -641,7 +734,13 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       }
       {
         KindTimer kt(c, 1);
-        rc = contract(c, precision, c->d_A.p, c->d_B.p, np, c->d_C.p + (size_t)w * nsplit * cstride, nsplit, cstride);
+        double2* Cw = c->d_C.p + (size_t)w * nsplit * cstride;
+        if (split) {
+          rc = split_quantize_operand(c, 0, c->d_A.p, pd);
+          if (!rc) rc = split_contract_pass(c, pd, Cw, nsplit, cstride);
+        } else {
+          rc = contract(c, c->d_A.p, c->d_B.p, np, Cw, nsplit, cstride);
+        }
       }
       if (rc) return rc;
     }
@@ -693,7 +792,17 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       }
       {
         KindTimer kt(c, 1);
-        rc = contract(c, precision, c->d_A.p, c->d_B.p, np, c->d_D.p + (size_t)w * nsplit * cstride, nsplit, cstride);
+        double2* Dw = c->d_D.p + (size_t)w * nsplit * cstride;
+        if (split) {
+          SplitPassDev pr;
+          const int64_t nrk = c->n_realk, pbase = p0;
+          rc = split_prepare(c, make_chunks(np, [&](int64_t i) { return (pbase + i) / nrk; }), pr);
+          if (!rc) rc = split_quantize_operand(c, 1, c->d_B.p, pr);
+          if (!rc) rc = split_quantize_operand(c, 0, c->d_A.p, pr);
+          if (!rc) rc = split_contract_pass(c, pr, Dw, nsplit, cstride);
+        } else {
+          rc = contract(c, c->d_A.p, c->d_B.p, np, Dw, nsplit, cstride);
+        }
       }
       if (rc) return rc;
     }
@@ -722,7 +831,18 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   c->last_ms[2] = t_epi;
   c->last_ms[3] = ms_tot;
   profile_end(c);
-  return read_status(c);
+  rc = read_status(c);
+  if (rc) return rc;
+  if (split) {
+    int err = 0;
+    TG_CHECK(c, cudaMemcpy(&err, c->d_split_err.p, sizeof(int), cudaMemcpyDeviceToHost), "split status");
+    if (err) {
+      char b[128];
+      snprintf(b, sizeof b, "split contraction: a bounded wait expired (site %d)", err);
+      return set_err(c, TG_ERR_TIMEOUT, b);
+    }
+  }
+  return TG_OK;
 }
 
 int tg_chi0(tg_ctx* c, const double* q, double e, double Ef, double eta, double etap, int n_real, const double* x2,

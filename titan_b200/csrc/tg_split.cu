@@ -1,0 +1,513 @@
+// Split-precision chi0 contraction on the tcgen05 tensor cores (int8 slices,
+// exact int32 level sums in TMEM, FP64 recombination per chunk).
+//
+// Three kernels per pass and operand: split_rowmax_kernel (per chunk and
+// element, the largest |Re|, |Im|), split_quantize_kernel (FP64 operand ->
+// five int8 digit planes, K-step blocks) and split_contract_kernel (warp-
+// specialised: one producer warp stages digit blocks with bulk copies into a
+// six-stage shared-memory ring, one warp issues the 19 MMAs per K-step, four
+// warps drain the six int32 level accumulators from TMEM at every chunk end).
+// Every wait on an mbarrier is bounded (2 s of %globaltimer); on a timeout the
+// kernel records an error code, waits (bounded) for its own copies and MMAs in
+// flight, frees its TMEM and returns.
+#include "tg_internal.cuh"
+#include "tg_split.cuh"
+
+#include <algorithm>
+#include <cstdio>
+
+namespace tg {
+
+namespace {
+
+// ----------------------------------------------------------------------------
+// FP64 -> digits
+// ----------------------------------------------------------------------------
+
+constexpr int kRowmaxSlots = 64;
+
+__global__ void split_rowmax_kernel(const double2* __restrict__ X, int64_t ld, const int* __restrict__ slot0,
+                                    const int* __restrict__ count, unsigned long long* __restrict__ M64) {
+  const int c = blockIdx.y;
+  const int cnt = count[c];
+  const int s_begin = blockIdx.x * kRowmaxSlots;
+  if (s_begin >= cnt) return;
+  const int s_end = min(cnt, s_begin + kRowmaxSlots);
+  const int64_t base = (int64_t)slot0[c];
+  for (int64_t e = threadIdx.x; e < ld; e += blockDim.x) {
+    double m = 0.0;
+    for (int s = s_begin; s < s_end; ++s) {
+      const double2 v = X[(base + s) * ld + e];
+      m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    }
+    if (m > 0.0) atomicMax(&M64[(int64_t)c * ld + e], (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// balanced base-256 digits of 16 values, slice-major: out[i] holds digit i of
+// the 16 values (i = 0 most significant)
+__device__ __forceinline__ void digits16(const long long (&x)[16], uint4 (&out)[kSplitSlices]) {
+  uint32_t w[kSplitSlices][4];
+#pragma unroll
+  for (int i = 0; i < kSplitSlices; ++i)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) w[i][q] = 0u;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    long long r = x[k];
+#pragma unroll
+    for (int i = kSplitSlices - 1; i >= 1; --i) {
+      int d = (int)(r & 255);
+      d -= (d >= 128) ? 256 : 0;
+      r = (r - d) >> 8;
+      w[i][k >> 2] |= ((uint32_t)(d & 255)) << (8 * (k & 3));
+    }
+    w[0][k >> 2] |= ((uint32_t)((int)r & 255)) << (8 * (k & 3));
+  }
+#pragma unroll
+  for (int i = 0; i < kSplitSlices; ++i) out[i] = make_uint4(w[i][0], w[i][1], w[i][2], w[i][3]);
+}
+
+// one thread per (K-step t, k half kc, group g, row r < rows): 16 points of one
+// element, Re and Im parts
+__global__ void split_quantize_kernel(const double2* __restrict__ X, int64_t ld, int n_ksteps,
+                                      const int* __restrict__ kchunk, const int* __restrict__ kstart,
+                                      const int* __restrict__ slot0, const int* __restrict__ count,
+                                      const SplitGroup* __restrict__ groups, int n_groups, int rows,
+                                      const unsigned long long* __restrict__ M64, int* __restrict__ E,
+                                      int8_t* __restrict__ dig) {
+  const int64_t per_t = (int64_t)2 * n_groups * rows;
+  const int64_t total = (int64_t)n_ksteps * per_t;
+  const int64_t block_bytes = (int64_t)kSplitSlices * 2 * rows * kSplitK;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx % rows);
+    const int g = (int)((idx / rows) % n_groups);
+    const int kc = (int)((idx / ((int64_t)rows * n_groups)) % 2);
+    const int t = (int)(idx / per_t);
+    const int c = kchunk[t];
+    const SplitGroup gr = groups[g];
+    const bool valid = r < gr.nvalid;
+    const int64_t e = gr.elem0 + r;
+    int Ex = 0;
+    if (valid) {
+      const double m = __longlong_as_double((long long)M64[(int64_t)c * ld + e]);
+      if (m > 0.0) frexp(m, &Ex);
+      if (t == kstart[c] && kc == 0) E[(int64_t)c * ld + e] = Ex;
+    }
+    const int first = (t - kstart[c]) * kSplitK + kc * 16;   // point within the chunk
+    const int cnt = count[c];
+    const int64_t p0 = (int64_t)slot0[c] + first;
+    long long xr[16], xi[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      double2 v = make_double2(0.0, 0.0);
+      if (valid && first + k < cnt) v = X[(p0 + k) * ld + e];
+      xr[k] = __double2ll_rn(scalbn(v.x, kSplitBits - Ex));
+      xi[k] = __double2ll_rn(scalbn(v.y, kSplitBits - Ex));
+    }
+    int8_t* blk = dig + ((int64_t)t * n_groups + g) * block_bytes + (int64_t)kc * 2 * rows * 16;
+    uint4 d[kSplitSlices];
+    digits16(xr, d);
+#pragma unroll
+    for (int i = 0; i < kSplitSlices; ++i)
+      *reinterpret_cast<uint4*>(blk + (int64_t)i * 2 * rows * kSplitK + (int64_t)r * 16) = d[i];
+    digits16(xi, d);
+#pragma unroll
+    for (int i = 0; i < kSplitSlices; ++i)
+      *reinterpret_cast<uint4*>(blk + (int64_t)i * 2 * rows * kSplitK + (int64_t)(rows + r) * 16) = d[i];
+  }
+}
+
+// ----------------------------------------------------------------------------
+// tcgen05 contraction
+// ----------------------------------------------------------------------------
+
+constexpr int kMmaM = 128;
+constexpr int kMmaN = 2 * kSplitColsB;     // 80
+constexpr int kLevels = 6;                 // L = 2..7
+constexpr int kStages = 6;
+constexpr int kStageBytes = kSplitABlock + kSplitBBlock;   // 33280
+constexpr int kXchBytes = 64 * 8 * 16;                     // 64 rows x 8 complex
+constexpr int kThreads = 192;                              // producer, MMA, 4 epilogue warps
+constexpr uint32_t kTmemCols = 512;
+constexpr int kBarOff = kStages * kStageBytes + kXchBytes;  // 8-byte aligned
+constexpr int kNumBars = 2 * kStages + 3;
+constexpr size_t kSplitSmem = 1024 + kBarOff + kNumBars * 8 + 16;
+constexpr unsigned long long kWaitNs = 2000000000ull;        // 2 s per wait
+
+__host__ __device__ constexpr uint32_t idesc_i8() {
+  // c_format S32 (2), a/b format signed int8 (1), both K-major, N >> 3, M >> 4
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kMmaN >> 3) << 17) | ((uint32_t)(kMmaM >> 4) << 24);
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;   // descriptor version of sm_100; layout type 0 = no swizzle
+  return d;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait; false when the CTA aborted or 2 s passed (then sets the abort flag and err)
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err, int code) {
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  uint32_t spins = 0;
+  while (true) {
+    if (mbar_try(bar, parity)) return true;
+    if ((++spins & 255u) == 0) {
+      if (*abort_flag) return false;
+      if (global_ns() - t0 > kWaitNs) {
+        *abort_flag = 1;
+        atomicExch(err, code);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContractArgs a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1 KB-aligned base for the stage ring
+  const uint32_t raw_addr = (uint32_t)__cvta_generic_to_shared(smem_raw);
+  const uint32_t base = (raw_addr + 1023u) & ~1023u;
+  unsigned char* sbase = smem_raw + (base - raw_addr);
+  const uint32_t bar0 = base + kBarOff;
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (kStages + s); };
+  const uint32_t accfull = bar0 + 8u * (2 * kStages);
+  const uint32_t accempty = accfull + 8u;
+  const uint32_t flushbar = accfull + 16u;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sbase + kBarOff + kNumBars * 8);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sbase + kBarOff + kNumBars * 8 + 4);
+  volatile int* epi_ok = reinterpret_cast<volatile int*>(sbase + kBarOff + kNumBars * 8 + 8);
+  double2* xch = reinterpret_cast<double2*>(sbase + kStages * kStageBytes);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(accfull, 1);
+    mbar_init(accempty, 128);
+    mbar_init(flushbar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(tmem_slot)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  const int ntiles = a.ntiles;
+  const int tile_id = blockIdx.x % ntiles;
+  const int split = blockIdx.x / ntiles;
+  const SplitTile tile = a.tiles[tile_id];
+  const int K = a.pass.n_ksteps;
+  const int k0 = (int)((int64_t)K * split / a.nsplit);
+  const int k1 = (int)((int64_t)K * (split + 1) / a.nsplit);
+
+  if (warp == 0) {
+    // ---------------- producer ----------------
+    if (lane == 0 && k0 < k1) {
+      uint32_t it = 0;
+      uint32_t last_use[kStages];
+      bool armed[kStages];
+      for (int s = 0; s < kStages; ++s) armed[s] = false, last_use[s] = 0;
+      bool ok = true;
+      for (int t = k0; t < k1 && ok; ++t, ++it) {
+        const int s = (int)(it % kStages);
+        const uint32_t use = it / kStages;
+        if (use > 0) ok = mbar_wait(empty_bar(s), (use - 1) & 1u, abort_flag, a.err, 1);
+        if (!ok) break;
+        const uint32_t sa = base + (uint32_t)s * kStageBytes;
+        mbar_expect_tx(full_bar(s), (uint32_t)kStageBytes);
+        bulk_g2s(sa, a.A + ((int64_t)t * a.GA + tile.gA) * kSplitABlock, kSplitABlock, full_bar(s));
+        bulk_g2s(sa + kSplitABlock, a.B + ((int64_t)t * a.GB + tile.gB) * kSplitBBlock, kSplitBBlock, full_bar(s));
+        armed[s] = true;
+        last_use[s] = use;
+      }
+      if (!ok) {
+        // let every copy this thread issued land before the CTA leaves
+        for (int s = 0; s < kStages; ++s) {
+          if (!armed[s]) continue;
+          const uint64_t t0 = global_ns();
+          while (!mbar_try(full_bar(s), last_use[s] & 1u) && global_ns() - t0 < kWaitNs) {
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0 && k0 < k1) {
+      const uint32_t idesc = idesc_i8();
+      uint32_t it = 0, d = 0;
+      bool ok = true;
+      int t = k0;
+      bool issued = false;
+      while (t < k1 && ok) {
+        const int c = a.pass.kchunk[t];
+        const int te = min(k1, a.pass.kstart[c + 1]);
+        if (d > 0) {
+          ok = mbar_wait(accempty, (d - 1) & 1u, abort_flag, a.err, 2);
+          if (!ok) break;
+          tc_fence_after();
+        }
+        for (int tt = t; tt < te; ++tt, ++it) {
+          const int s = (int)(it % kStages);
+          const uint32_t use = it / kStages;
+          ok = mbar_wait(full_bar(s), use & 1u, abort_flag, a.err, 3);
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t sa = base + (uint32_t)s * kStageBytes;
+          const uint32_t sb = sa + kSplitABlock;
+          // digit pairs (i, j) with level l = i + j <= 5, grouped by level
+#pragma unroll
+          for (int l = 0; l < kLevels; ++l) {
+#pragma unroll
+            for (int i = 0; i < kSplitSlices; ++i) {
+              const int j = l - i;
+              if (j < 0 || j >= kSplitSlices) continue;
+              const bool first = i == (l > kSplitSlices - 1 ? l - (kSplitSlices - 1) : 0);
+              const uint64_t ad = smem_desc(sa + (uint32_t)i * (2 * kSplitRowsA * kSplitK), 2 * kSplitRowsA * 16, 128);
+              const uint64_t bd = smem_desc(sb + (uint32_t)j * (2 * kSplitColsB * kSplitK), 2 * kSplitColsB * 16, 128);
+              umma_i8(tmem + (uint32_t)(l * kMmaN), ad, bd, idesc, (tt != t || !first) ? 1u : 0u);
+            }
+          }
+          umma_commit(empty_bar(s));
+          issued = true;
+        }
+        if (!ok) break;
+        umma_commit(accfull);
+        ++d;
+        t = te;
+      }
+      if (!ok && issued) {
+        // wait for the MMAs already issued before TMEM is released
+        umma_commit(flushbar);
+        const uint64_t t0 = global_ns();
+        while (!mbar_try(flushbar, 0) && global_ns() - t0 < kWaitNs) {
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue (TMEM lanes 32 * (warp % 4) ..) ----------------
+    const int ep = threadIdx.x - 64;            // 0..127
+    const int lane_base = 32 * (warp & 3);
+    const int r = lane_base + lane;             // TMEM lane = MMA row
+    const int part = r >> 6;                    // 0: Re A row, 1: Im A row
+    const int rr = r & 63;
+    const int pair = tile.pair;
+    const int M = a.pair_M[pair];
+    const int64_t aoff = a.pair_aoff[pair];
+    const int u = tile.u0 + rr;
+    double2* Cbase = a.C + (int64_t)split * a.cstride + a.pair_coff[pair];
+    uint32_t d = 0;
+    int t = k0;
+    while (t < k1) {
+      const int c = a.pass.kchunk[t];
+      const int te = min(k1, a.pass.kstart[c + 1]);
+      if (ep == 0) *epi_ok = mbar_wait(accfull, d & 1u, abort_flag, a.err, 4) ? 1 : 0;
+      epi_sync();
+      const bool ok = *epi_ok != 0;
+      epi_sync();
+      if (!ok) break;
+      tc_fence_after();
+      const int64_t erow = (int64_t)c * a.ld + aoff;
+      const int ea = (part == 0 && u < M) ? a.EA[erow + u] : 0;
+#pragma unroll 1
+      for (int q = 0; q < kSplitColsB / 8; ++q) {
+        double vr[8], vi[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) vr[k] = vi[k] = 0.0;
+#pragma unroll
+        for (int l = 0; l < kLevels; ++l) {
+          uint32_t x[8], y[8];
+          const uint32_t ta = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(l * kMmaN + 8 * q);
+          tmem_ld8(ta, x);
+          tmem_ld8(ta + kSplitColsB, y);
+          tmem_wait_ld();
+          const double w = ldexp(1.0, 4 - 8 * (l + 2));   // level L = l + 2 weighs 2^(4 - 8L)
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            vr[k] = fma((double)(int)x[k], w, vr[k]);
+            vi[k] = fma((double)(int)y[k], w, vi[k]);
+          }
+        }
+        // part 0 rows hold (Ar Br, Ar Bi), part 1 rows (Ai Br, Ai Bi) of the same complex row
+        if (part == 1) {
+#pragma unroll
+          for (int k = 0; k < 8; ++k) xch[rr * 8 + k] = make_double2(vr[k], vi[k]);
+        }
+        epi_sync();
+        if (part == 0 && u < M) {
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int v = tile.v0 + 8 * q + k;
+            if (v >= M) continue;
+            const double2 y = xch[rr * 8 + k];
+            const int e = ea + a.EB[erow + v];
+            double2* cp = Cbase + (int64_t)u * M + v;
+            double2 cv = *cp;
+            cv.x += ldexp(vr[k] - y.y, e);
+            cv.y += ldexp(vi[k] + y.x, e);
+            *cp = cv;
+          }
+        }
+        epi_sync();
+      }
+      tc_fence_before();
+      mbar_arrive(accempty);
+      ++d;
+      t = te;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  }
+}
+
+}  // namespace
+
+void split_build_layout(int n_pairs, const int* pair_M, const int* pair_aoff, SplitLayout& out) {
+  out.groupsA.clear();
+  out.groupsB.clear();
+  out.tiles.clear();
+  for (int p = 0; p < n_pairs; ++p) {
+    const int M = pair_M[p];
+    const int gA0 = (int)out.groupsA.size(), gB0 = (int)out.groupsB.size();
+    const int na = (M + kSplitRowsA - 1) / kSplitRowsA, nb = (M + kSplitColsB - 1) / kSplitColsB;
+    for (int g = 0; g < na; ++g)
+      out.groupsA.push_back(SplitGroup{pair_aoff[p] + g * kSplitRowsA, std::min(kSplitRowsA, M - g * kSplitRowsA)});
+    for (int g = 0; g < nb; ++g)
+      out.groupsB.push_back(SplitGroup{pair_aoff[p] + g * kSplitColsB, std::min(kSplitColsB, M - g * kSplitColsB)});
+    for (int ga = 0; ga < na; ++ga)
+      for (int gb = 0; gb < nb; ++gb)
+        out.tiles.push_back(SplitTile{p, gA0 + ga, gB0 + gb, ga * kSplitRowsA, gb * kSplitColsB});
+  }
+}
+
+int split_nsplit(int ntiles, int num_sms, int64_t ksteps_hint) {
+  // cost of a split count: waves x (K-steps per unit + a drain and start-up of ~24 K-steps)
+  int best = 1;
+  double best_cost = 1e300;
+  for (int s = 1; s <= 64; ++s) {
+    const int64_t units = (int64_t)ntiles * s;
+    const int64_t waves = (units + num_sms - 1) / num_sms;
+    const double cost = (double)waves * ((double)ksteps_hint / s + 24.0);
+    if (cost < best_cost * 0.999) {
+      best_cost = cost;
+      best = s;
+    }
+  }
+  return best;
+}
+
+cudaError_t split_rowmax(const double2* X, int64_t ld, const SplitPassDev& p, unsigned long long* M64,
+                         cudaStream_t s) {
+  if (p.n_chunks <= 0) return cudaSuccess;
+  const int gx = (kSplitMaxChunk + kRowmaxSlots - 1) / kRowmaxSlots;
+  split_rowmax_kernel<<<dim3(gx, p.n_chunks), 256, 0, s>>>(X, ld, p.slot0, p.count, M64);
+  return cudaGetLastError();
+}
+
+cudaError_t split_quantize(const double2* X, int64_t ld, const SplitPassDev& p, const SplitGroup* groups,
+                           int n_groups, int rows, const unsigned long long* M64, int* E, int8_t* dig,
+                           cudaStream_t s) {
+  if (p.n_ksteps <= 0) return cudaSuccess;
+  const int64_t total = (int64_t)p.n_ksteps * 2 * n_groups * rows;
+  const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  split_quantize_kernel<<<blocks, 256, 0, s>>>(X, ld, p.n_ksteps, p.kchunk, p.kstart, p.slot0, p.count, groups,
+                                               n_groups, rows, M64, E, dig);
+  return cudaGetLastError();
+}
+
+cudaError_t split_contract(const SplitContractArgs& a, cudaStream_t s) {
+  if (a.pass.n_ksteps <= 0 || a.ntiles <= 0) return cudaSuccess;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e =
+        cudaFuncSetAttribute(split_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  split_contract_kernel<<<a.ntiles * a.nsplit, kThreads, kSplitSmem, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace tg
