@@ -357,6 +357,7 @@ int split_contract_pass(tg_ctx* c, const SplitPassDev& pd, double2* Cpart, int n
   sa.C = Cpart;
   sa.cstride = cstride;
   sa.err = c->d_split_err.p;
+  sa.num_ctas = c->num_sms;
   c->launches += 1;
   TG_CHECK(c, split_contract(sa, c->stream), "contraction (split)");
   return TG_OK;

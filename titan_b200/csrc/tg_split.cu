@@ -44,38 +44,42 @@ __global__ void split_rowmax_kernel(const double2* __restrict__ X, int64_t ld, c
   }
 }
 
-// balanced base-256 digits of 16 values, slice-major: out[i] holds digit i of
-// the 16 values (i = 0 most significant)
+// Balanced base-256 digits of 16 integers |X| <= 2^38, slice-major: out[0] holds
+// the top digits, out[1..4] the lower ones (most significant first).  With
+// Y = X + 0x80808080 the low four balanced digits are the bytes of the low word
+// of Y minus 128 (a byte-wise XOR with 0x80), and the top digit is Y >> 32.
 __device__ __forceinline__ void digits16(const long long (&x)[16], uint4 (&out)[kSplitSlices]) {
-  uint32_t w[kSplitSlices][4];
-#pragma unroll
-  for (int i = 0; i < kSplitSlices; ++i)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) w[i][q] = 0u;
+  uint32_t lo[16], top[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
-    long long r = x[k];
-#pragma unroll
-    for (int i = kSplitSlices - 1; i >= 1; --i) {
-      int d = (int)(r & 255);
-      d -= (d >= 128) ? 256 : 0;
-      r = (r - d) >> 8;
-      w[i][k >> 2] |= ((uint32_t)(d & 255)) << (8 * (k & 3));
-    }
-    w[0][k >> 2] |= ((uint32_t)((int)r & 255)) << (8 * (k & 3));
+    const long long y = x[k] + 0x80808080LL;
+    lo[k] = (uint32_t)y ^ 0x80808080u;
+    top[k >> 2] |= ((uint32_t)(int)(y >> 32) & 255u) << (8 * (k & 3));
   }
+  uint32_t b[4][4];   // b[byte][group of four values]
 #pragma unroll
-  for (int i = 0; i < kSplitSlices; ++i) out[i] = make_uint4(w[i][0], w[i][1], w[i][2], w[i][3]);
+  for (int j = 0; j < 4; ++j) {
+    const uint32_t t0 = __byte_perm(lo[4 * j], lo[4 * j + 1], 0x5140);
+    const uint32_t t1 = __byte_perm(lo[4 * j], lo[4 * j + 1], 0x7362);
+    const uint32_t t2 = __byte_perm(lo[4 * j + 2], lo[4 * j + 3], 0x5140);
+    const uint32_t t3 = __byte_perm(lo[4 * j + 2], lo[4 * j + 3], 0x7362);
+    b[0][j] = __byte_perm(t0, t2, 0x5410);
+    b[1][j] = __byte_perm(t0, t2, 0x7632);
+    b[2][j] = __byte_perm(t1, t3, 0x5410);
+    b[3][j] = __byte_perm(t1, t3, 0x7632);
+  }
+  out[0] = make_uint4(top[0], top[1], top[2], top[3]);
+#pragma unroll
+  for (int i = 1; i < kSplitSlices; ++i) out[i] = make_uint4(b[4 - i][0], b[4 - i][1], b[4 - i][2], b[4 - i][3]);
 }
 
 // one thread per (K-step t, k half kc, group g, row r < rows): 16 points of one
 // element, Re and Im parts
-__global__ void split_quantize_kernel(const double2* __restrict__ X, int64_t ld, int n_ksteps,
-                                      const int* __restrict__ kchunk, const int* __restrict__ kstart,
-                                      const int* __restrict__ slot0, const int* __restrict__ count,
-                                      const SplitGroup* __restrict__ groups, int n_groups, int rows,
-                                      const unsigned long long* __restrict__ M64, int* __restrict__ E,
-                                      int8_t* __restrict__ dig) {
+__global__ void __launch_bounds__(256) split_quantize_kernel(
+    const double2* __restrict__ X, int64_t ld, int n_ksteps, const int* __restrict__ kchunk,
+    const int* __restrict__ kstart, const int* __restrict__ slot0, const int* __restrict__ count,
+    const SplitGroup* __restrict__ groups, int n_groups, int rows, const unsigned long long* __restrict__ M64,
+    int* __restrict__ E, int8_t* __restrict__ dig) {
   const int64_t per_t = (int64_t)2 * n_groups * rows;
   const int64_t total = (int64_t)n_ksteps * per_t;
   const int64_t block_bytes = (int64_t)kSplitSlices * 2 * rows * kSplitK;
@@ -87,24 +91,27 @@ __global__ void split_quantize_kernel(const double2* __restrict__ X, int64_t ld,
     const int t = (int)(idx / per_t);
     const int c = kchunk[t];
     const SplitGroup gr = groups[g];
-    const bool valid = r < gr.nvalid;
     const int64_t e = gr.elem0 + r;
+    // scale 2^(38 - E) with max |x| < 2^E; elements below 2^-985 of unit scale count as zero
+    bool valid = r < gr.nvalid;
     int Ex = 0;
     if (valid) {
       const double m = __longlong_as_double((long long)M64[(int64_t)c * ld + e]);
       if (m > 0.0) frexp(m, &Ex);
       if (t == kstart[c] && kc == 0) E[(int64_t)c * ld + e] = Ex;
+      if (m == 0.0 || Ex < -985) valid = false;
     }
+    const double scale = __hiloint2double((1023 + kSplitBits - (valid ? Ex : 0)) << 20, 0);
     const int first = (t - kstart[c]) * kSplitK + kc * 16;   // point within the chunk
     const int cnt = count[c];
-    const int64_t p0 = (int64_t)slot0[c] + first;
+    const double2* src = X + ((int64_t)slot0[c] + first) * ld + e;
     long long xr[16], xi[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
       double2 v = make_double2(0.0, 0.0);
-      if (valid && first + k < cnt) v = X[(p0 + k) * ld + e];
-      xr[k] = __double2ll_rn(scalbn(v.x, kSplitBits - Ex));
-      xi[k] = __double2ll_rn(scalbn(v.y, kSplitBits - Ex));
+      if (valid && first + k < cnt) v = src[(int64_t)k * ld];
+      xr[k] = __double2ll_rn(v.x * scale);
+      xi[k] = __double2ll_rn(v.y * scale);
     }
     int8_t* blk = dig + ((int64_t)t * n_groups + g) * block_bytes + (int64_t)kc * 2 * rows * 16;
     uint4 d[kSplitSlices];
@@ -229,15 +236,17 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 
 __device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
+// Persistent: CTA b takes the units (tile, K-range) b, b + gridDim.x, ...; units
+// are numbered K-range-major so that the CTAs resident at one time share the
+// digit blocks of one K-range in L2.  The stage ring and the drain count run
+// on across units, so the producer prefetches the next unit while the
+// epilogue drains the last one.
 __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContractArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  // 1 KB-aligned base for the stage ring
   const uint32_t raw_addr = (uint32_t)__cvta_generic_to_shared(smem_raw);
   const uint32_t base = (raw_addr + 1023u) & ~1023u;
   unsigned char* sbase = smem_raw + (base - raw_addr);
   const uint32_t bar0 = base + kBarOff;
-  auto full_bar = [&](int s) { return bar0 + 8u * s; };
-  auto empty_bar = [&](int s) { return bar0 + 8u * (kStages + s); };
   const uint32_t accfull = bar0 + 8u * (2 * kStages);
   const uint32_t accempty = accfull + 8u;
   const uint32_t flushbar = accfull + 16u;
@@ -249,8 +258,8 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(full_bar(s), 1);
-      mbar_init(empty_bar(s), 1);
+      mbar_init(bar0 + 8u * s, 1);
+      mbar_init(bar0 + 8u * (kStages + s), 1);
     }
     mbar_init(accfull, 1);
     mbar_init(accempty, 128);
@@ -269,89 +278,94 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  const int ntiles = a.ntiles;
-  const int tile_id = blockIdx.x % ntiles;
-  const int split = blockIdx.x / ntiles;
-  const SplitTile tile = a.tiles[tile_id];
+  const int nunits = a.ntiles * a.nsplit;
   const int K = a.pass.n_ksteps;
-  const int k0 = (int)((int64_t)K * split / a.nsplit);
-  const int k1 = (int)((int64_t)K * (split + 1) / a.nsplit);
+  const int* kchunk = a.pass.kchunk;
+  const int* kstart = a.pass.kstart;
 
   if (warp == 0) {
-    // ---------------- producer ----------------
-    if (lane == 0 && k0 < k1) {
+    // ---------------- producer: one lane stages digit blocks ----------------
+    if (lane == 0) {
       uint32_t it = 0;
       uint32_t last_use[kStages];
       bool armed[kStages];
       for (int s = 0; s < kStages; ++s) armed[s] = false, last_use[s] = 0;
       bool ok = true;
-      for (int t = k0; t < k1 && ok; ++t, ++it) {
-        const int s = (int)(it % kStages);
-        const uint32_t use = it / kStages;
-        if (use > 0) ok = mbar_wait(empty_bar(s), (use - 1) & 1u, abort_flag, a.err, 1);
-        if (!ok) break;
-        const uint32_t sa = base + (uint32_t)s * kStageBytes;
-        mbar_expect_tx(full_bar(s), (uint32_t)kStageBytes);
-        bulk_g2s(sa, a.A + ((int64_t)t * a.GA + tile.gA) * kSplitABlock, kSplitABlock, full_bar(s));
-        bulk_g2s(sa + kSplitABlock, a.B + ((int64_t)t * a.GB + tile.gB) * kSplitBBlock, kSplitBBlock, full_bar(s));
-        armed[s] = true;
-        last_use[s] = use;
+      for (int un = blockIdx.x; un < nunits && ok; un += gridDim.x) {
+        const int split = un / a.ntiles;
+        const SplitTile tile = a.tiles[un % a.ntiles];
+        const int k0 = (int)((int64_t)K * split / a.nsplit), k1 = (int)((int64_t)K * (split + 1) / a.nsplit);
+        const int8_t* srcA = a.A + (int64_t)tile.gA * kSplitABlock;
+        const int8_t* srcB = a.B + (int64_t)tile.gB * kSplitBBlock;
+        for (int t = k0; t < k1; ++t, ++it) {
+          const int s = (int)(it % kStages);
+          const uint32_t use = it / kStages;
+          if (use > 0 && !(ok = mbar_wait(bar0 + 8u * (kStages + s), (use - 1) & 1u, abort_flag, a.err, 1))) break;
+          const uint32_t sa = base + (uint32_t)s * kStageBytes;
+          const uint32_t fb = bar0 + 8u * s;
+          mbar_expect_tx(fb, (uint32_t)kStageBytes);
+          bulk_g2s(sa, srcA + (int64_t)t * a.GA * kSplitABlock, kSplitABlock, fb);
+          bulk_g2s(sa + kSplitABlock, srcB + (int64_t)t * a.GB * kSplitBBlock, kSplitBBlock, fb);
+          armed[s] = true;
+          last_use[s] = use;
+        }
       }
       if (!ok) {
         // let every copy this thread issued land before the CTA leaves
         for (int s = 0; s < kStages; ++s) {
           if (!armed[s]) continue;
           const uint64_t t0 = global_ns();
-          while (!mbar_try(full_bar(s), last_use[s] & 1u) && global_ns() - t0 < kWaitNs) {
+          while (!mbar_try(bar0 + 8u * s, last_use[s] & 1u) && global_ns() - t0 < kWaitNs) {
           }
         }
       }
     }
     __syncwarp();
   } else if (warp == 1) {
-    // ---------------- MMA issuer ----------------
-    if (lane == 0 && k0 < k1) {
+    // ---------------- MMA issuer: one lane ----------------
+    if (lane == 0) {
       const uint32_t idesc = idesc_i8();
       uint32_t it = 0, d = 0;
-      bool ok = true;
-      int t = k0;
-      bool issued = false;
-      while (t < k1 && ok) {
-        const int c = a.pass.kchunk[t];
-        const int te = min(k1, a.pass.kstart[c + 1]);
-        if (d > 0) {
-          ok = mbar_wait(accempty, (d - 1) & 1u, abort_flag, a.err, 2);
-          if (!ok) break;
-          tc_fence_after();
-        }
-        for (int tt = t; tt < te; ++tt, ++it) {
-          const int s = (int)(it % kStages);
-          const uint32_t use = it / kStages;
-          ok = mbar_wait(full_bar(s), use & 1u, abort_flag, a.err, 3);
-          if (!ok) break;
-          tc_fence_after();
-          const uint32_t sa = base + (uint32_t)s * kStageBytes;
-          const uint32_t sb = sa + kSplitABlock;
-          // digit pairs (i, j) with level l = i + j <= 5, grouped by level
-#pragma unroll
-          for (int l = 0; l < kLevels; ++l) {
-#pragma unroll
-            for (int i = 0; i < kSplitSlices; ++i) {
-              const int j = l - i;
-              if (j < 0 || j >= kSplitSlices) continue;
-              const bool first = i == (l > kSplitSlices - 1 ? l - (kSplitSlices - 1) : 0);
-              const uint64_t ad = smem_desc(sa + (uint32_t)i * (2 * kSplitRowsA * kSplitK), 2 * kSplitRowsA * 16, 128);
-              const uint64_t bd = smem_desc(sb + (uint32_t)j * (2 * kSplitColsB * kSplitK), 2 * kSplitColsB * 16, 128);
-              umma_i8(tmem + (uint32_t)(l * kMmaN), ad, bd, idesc, (tt != t || !first) ? 1u : 0u);
-            }
+      bool ok = true, issued = false;
+      for (int un = blockIdx.x; un < nunits && ok; un += gridDim.x) {
+        const int split = un / a.ntiles;
+        const int k0 = (int)((int64_t)K * split / a.nsplit), k1 = (int)((int64_t)K * (split + 1) / a.nsplit);
+        int t = k0;
+        while (t < k1) {
+          const int te = min(k1, kstart[kchunk[t] + 1]);
+          if (d > 0) {
+            if (!(ok = mbar_wait(accempty, (d - 1) & 1u, abort_flag, a.err, 2))) break;
+            tc_fence_after();
           }
-          umma_commit(empty_bar(s));
-          issued = true;
+          for (int tt = t; tt < te; ++tt, ++it) {
+            const int s = (int)(it % kStages);
+            if (!(ok = mbar_wait(bar0 + 8u * s, (it / kStages) & 1u, abort_flag, a.err, 3))) break;
+            tc_fence_after();
+            const uint32_t sa = base + (uint32_t)s * kStageBytes;
+            const uint32_t sb = sa + kSplitABlock;
+            // digit pairs (i, j) with level l = i + j <= 5, grouped by level
+#pragma unroll
+            for (int l = 0; l < kLevels; ++l) {
+#pragma unroll
+              for (int i = 0; i < kSplitSlices; ++i) {
+                const int j = l - i;
+                if (j < 0 || j >= kSplitSlices) continue;
+                const bool first = i == (l > kSplitSlices - 1 ? l - (kSplitSlices - 1) : 0);
+                const uint64_t ad =
+                    smem_desc(sa + (uint32_t)i * (2 * kSplitRowsA * kSplitK), 2 * kSplitRowsA * 16, 128);
+                const uint64_t bd =
+                    smem_desc(sb + (uint32_t)j * (2 * kSplitColsB * kSplitK), 2 * kSplitColsB * 16, 128);
+                umma_i8(tmem + (uint32_t)(l * kMmaN), ad, bd, idesc, (tt != t || !first) ? 1u : 0u);
+              }
+            }
+            umma_commit(bar0 + 8u * (kStages + s));
+            issued = true;
+          }
+          if (!ok) break;
+          umma_commit(accfull);
+          ++d;
+          t = te;
         }
-        if (!ok) break;
-        umma_commit(accfull);
-        ++d;
-        t = te;
       }
       if (!ok && issued) {
         // wait for the MMAs already issued before TMEM is released
@@ -363,75 +377,93 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
     }
     __syncwarp();
   } else {
-    // ---------------- epilogue (TMEM lanes 32 * (warp % 4) ..) ----------------
-    const int ep = threadIdx.x - 64;            // 0..127
+    // ---------------- epilogue: warps 2..5 own TMEM lanes 32 (warp % 4) .. + 31 ----------------
+    const int ep = threadIdx.x - 64;
     const int lane_base = 32 * (warp & 3);
-    const int r = lane_base + lane;             // TMEM lane = MMA row
-    const int part = r >> 6;                    // 0: Re A row, 1: Im A row
+    const int r = lane_base + lane;   // MMA row: 0..63 Re A, 64..127 Im A of complex row r % 64
+    const int part = r >> 6;
     const int rr = r & 63;
-    const int pair = tile.pair;
-    const int M = a.pair_M[pair];
-    const int64_t aoff = a.pair_aoff[pair];
-    const int u = tile.u0 + rr;
-    double2* Cbase = a.C + (int64_t)split * a.cstride + a.pair_coff[pair];
     uint32_t d = 0;
-    int t = k0;
-    while (t < k1) {
-      const int c = a.pass.kchunk[t];
-      const int te = min(k1, a.pass.kstart[c + 1]);
-      if (ep == 0) *epi_ok = mbar_wait(accfull, d & 1u, abort_flag, a.err, 4) ? 1 : 0;
-      epi_sync();
-      const bool ok = *epi_ok != 0;
-      epi_sync();
-      if (!ok) break;
-      tc_fence_after();
-      const int64_t erow = (int64_t)c * a.ld + aoff;
-      const int ea = (part == 0 && u < M) ? a.EA[erow + u] : 0;
+    bool ok = true;
+    for (int un = blockIdx.x; un < nunits && ok; un += gridDim.x) {
+      const int split = un / a.ntiles;
+      const SplitTile tile = a.tiles[un % a.ntiles];
+      const int k0 = (int)((int64_t)K * split / a.nsplit), k1 = (int)((int64_t)K * (split + 1) / a.nsplit);
+      const int M = a.pair_M[tile.pair];
+      const int64_t aoff = a.pair_aoff[tile.pair];
+      const int u = tile.u0 + rr;
+      const bool own = part == 0 && u < M;
+      double2* Crow = a.C + (int64_t)split * a.cstride + a.pair_coff[tile.pair] + (int64_t)u * M;
+      int t = k0;
+      while (t < k1) {
+        const int c = kchunk[t];
+        const int te = min(k1, kstart[c + 1]);
+        if (ep == 0) *epi_ok = mbar_wait(accfull, d & 1u, abort_flag, a.err, 4) ? 1 : 0;
+        epi_sync();
+        ok = *epi_ok != 0;
+        epi_sync();
+        if (!ok) break;
+        tc_fence_after();
+        const int64_t erow = (int64_t)c * a.ld + aoff;
+        const int ea = own ? a.EA[erow + u] : 0;
 #pragma unroll 1
-      for (int q = 0; q < kSplitColsB / 8; ++q) {
-        double vr[8], vi[8];
+        for (int q = 0; q < kSplitColsB / 8; ++q) {
+          const int vq = tile.v0 + 8 * q;
+          double2 cv[8];
+          int eb[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) vr[k] = vi[k] = 0.0;
+          for (int k = 0; k < 8; ++k) {
+            cv[k] = make_double2(0.0, 0.0);
+            eb[k] = 0;
+            if (own && vq + k < M) {
+              cv[k] = Crow[vq + k];
+              eb[k] = a.EB[erow + vq + k];
+            }
+          }
+          uint32_t x[kLevels][8], y[kLevels][8];
 #pragma unroll
-        for (int l = 0; l < kLevels; ++l) {
-          uint32_t x[8], y[8];
-          const uint32_t ta = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(l * kMmaN + 8 * q);
-          tmem_ld8(ta, x);
-          tmem_ld8(ta + kSplitColsB, y);
+          for (int l = 0; l < kLevels; ++l) {
+            const uint32_t ta = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(l * kMmaN + 8 * q);
+            tmem_ld8(ta, x[l]);
+            tmem_ld8(ta + kSplitColsB, y[l]);
+          }
           tmem_wait_ld();
-          const double w = ldexp(1.0, 4 - 8 * (l + 2));   // level L = l + 2 weighs 2^(4 - 8L)
+          double vr[8], vi[8];
 #pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            vr[k] = fma((double)(int)x[k], w, vr[k]);
-            vi[k] = fma((double)(int)y[k], w, vi[k]);
+          for (int k = 0; k < 8; ++k) vr[k] = vi[k] = 0.0;
+#pragma unroll
+          for (int l = 0; l < kLevels; ++l) {
+            const double w = __hiloint2double((1023 + 4 - 8 * (l + 2)) << 20, 0);   // 2^(4 - 8L), L = l + 2
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              vr[k] = fma((double)(int)x[l][k], w, vr[k]);
+              vi[k] = fma((double)(int)y[l][k], w, vi[k]);
+            }
           }
-        }
-        // part 0 rows hold (Ar Br, Ar Bi), part 1 rows (Ai Br, Ai Bi) of the same complex row
-        if (part == 1) {
+          // rows of part 0 hold (Ar Br, Ar Bi), rows of part 1 (Ai Br, Ai Bi) of the same complex row
+          if (part == 1) {
 #pragma unroll
-          for (int k = 0; k < 8; ++k) xch[rr * 8 + k] = make_double2(vr[k], vi[k]);
-        }
-        epi_sync();
-        if (part == 0 && u < M) {
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const int v = tile.v0 + 8 * q + k;
-            if (v >= M) continue;
-            const double2 y = xch[rr * 8 + k];
-            const int e = ea + a.EB[erow + v];
-            double2* cp = Cbase + (int64_t)u * M + v;
-            double2 cv = *cp;
-            cv.x += ldexp(vr[k] - y.y, e);
-            cv.y += ldexp(vi[k] + y.x, e);
-            *cp = cv;
+            for (int k = 0; k < 8; ++k) xch[rr * 8 + k] = make_double2(vr[k], vi[k]);
           }
+          epi_sync();
+          if (own) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              if (vq + k >= M) continue;
+              const double2 yy = xch[rr * 8 + k];
+              const int e = ea + eb[k];
+              cv[k].x += ldexp(vr[k] - yy.y, e);
+              cv[k].y += ldexp(vi[k] + yy.x, e);
+              Crow[vq + k] = cv[k];
+            }
+          }
+          epi_sync();
         }
-        epi_sync();
+        tc_fence_before();
+        mbar_arrive(accempty);
+        ++d;
+        t = te;
       }
-      tc_fence_before();
-      mbar_arrive(accempty);
-      ++d;
-      t = te;
     }
   }
   tc_fence_before();
@@ -469,7 +501,7 @@ int split_nsplit(int ntiles, int num_sms, int64_t ksteps_hint) {
   for (int s = 1; s <= 64; ++s) {
     const int64_t units = (int64_t)ntiles * s;
     const int64_t waves = (units + num_sms - 1) / num_sms;
-    const double cost = (double)waves * ((double)ksteps_hint / s + 24.0);
+    const double cost = (double)waves * ((double)ksteps_hint / s + 12.0);
     if (cost < best_cost * 0.999) {
       best_cost = cost;
       best = s;
@@ -506,7 +538,8 @@ cudaError_t split_contract(const SplitContractArgs& a, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
-  split_contract_kernel<<<a.ntiles * a.nsplit, kThreads, kSplitSmem, s>>>(a);
+  const int grid = std::min(a.ntiles * a.nsplit, a.num_ctas > 0 ? a.num_ctas : 148);
+  split_contract_kernel<<<grid, kThreads, kSplitSmem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -100,6 +100,7 @@ struct SplitContractArgs {
   double2* C = nullptr;        // partial accumulators, split s at C + s * cstride
   int64_t cstride = 0;
   int* err = nullptr;          // receives a non-zero code if a bounded wait gave up
+  int num_ctas = 148;          // persistent CTAs (one per SM)
 };
 
 cudaError_t split_contract(const SplitContractArgs& a, cudaStream_t s);
