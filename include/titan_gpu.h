@@ -107,6 +107,42 @@ int tg_gg_tensor(tg_ctx* ctx, double Ef, double eta, int orbital_resolved, const
  *   over realBZ, sigma_a = (1, x, y, z). */
 int tg_fermi_column(tg_ctx* ctx, double Ef, double eta, double* D);
 
+/* Jacobian of the self-consistency equations: replaces
+ * calcJacobian_greenfunction(jacobian, N) (source/mod_self_consistency.F90:795-1205).
+ * Unknowns per site i (set_hamiltonian_variables, :1754-1780): the occupation of each
+ * d orbital when Un(i) != 0, then (mx, my, mz) of the d shell when Um(i) != 0, and
+ * E_F last unless fixEf.  dmask(norb_max, n_atoms) flags the d orbitals (Types%dOrbs),
+ * Un/Um(n_atoms) the Hubbard parameters; jac(neq, neq) column-major real.
+ * J = (1/pi) sum_{k,E} w Re Tr_d[sigma_a G_ij M_b G_ji] (+ the E_F column from the
+ * real-axis BZ at E_F + i eta) minus the identity on the first neq - 1 entries. */
+int tg_jacobian(tg_ctx* ctx, double Ef, double eta, const int* dmask, const double* Un,
+                const double* Um, int fixEf, int neq, double* jac);
+
+/* Number of unknowns (the N of calcJacobian_greenfunction) and, when per is not
+ * null, the first unknown of each site: per(n_atoms + 1).  Host only. */
+int tg_jacobian_layout(int n_atoms, const int* norb, int norb_max, const int* dmask,
+                       const double* Un, const double* Um, int fixEf, int* per);
+
+/* Host-only assembly of the Jacobian from the GG tensor T (tg_gg_tensor with
+ * orbital_resolved = 1, shape (16, ncol, nrow, n_atoms, n_atoms)) and the
+ * Fermi column D (tg_fermi_column; ignored when fixEf).  No GPU work. */
+int tg_jacobian_assemble(int n_atoms, const int* norb, int norb_max, const int* dmask,
+                         const double* Un, const double* Um, int fixEf, int nrow, int ncol,
+                         const double* T, const double* D, int neq, double* jac);
+
+/* Adjoint of the site occupations and moments with respect to an on-site
+ * potential V_i and exchange field B_i added to every orbital of site i,
+ * h0 -> h0 + sum_i P_i (V_i sigma_0 + B_i . sigma).  A(4 n_atoms, 4 n_atoms) column-major,
+ * A(a + 4 i, b + 4 j) = d x_{i,a} / d p_{j,b} with x = (n, mx, my, mz) of
+ * expectation_values_greenfunction (mod_expectation.F90:28-149) summed over the
+ * site's orbitals and p = (V, Bx, By, Bz): (1/pi) sum w Re Tr[P_i sigma_a G P_j sigma_b G].
+ * No counterpart in the reference (its Jacobian uses the d-shell variables above). */
+int tg_adjoint_vb(tg_ctx* ctx, double Ef, double eta, double* A);
+
+/* n_atoms, norb_max and (when norb is not null) norb(n_atoms) of the system set by
+ * tg_set_system. */
+int tg_system_shape(const tg_ctx* ctx, int* n_atoms, int* norb_max, int* norb);
+
 /* RPA Dyson solve chi = (1 + chi_hf U)^-1 chi_hf in FP64 on the GPU
  * (calculate_chi.F90:85-89).  All matrices (dimens, dimens) complex. */
 int tg_dyson(tg_ctx* ctx, int dimens, const double* chi_hf, const double* umat, double* chi);

@@ -419,6 +419,16 @@ int tg_destroy(tg_ctx* c) {
 
 const char* tg_last_error(const tg_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
+int tg_system_shape(const tg_ctx* c, int* n_atoms, int* norb_max, int* norb) {
+  if (!c || !n_atoms || !norb_max) return TG_ERR_ARG;
+  if (!c->sys_set) return TG_ERR_STATE;
+  *n_atoms = c->n_atoms;
+  *norb_max = c->nmax;
+  if (norb)
+    for (int i = 0; i < c->n_atoms; ++i) norb[i] = c->norb[i];
+  return TG_OK;
+}
+
 int tg_set_system(tg_ctx* c, int n_atoms, const int* norb, int norb_max, int n_neigh, const double* cell_vec,
                   const int* basis_idx, const int* is_hopping, const double* t0i) {
   if (!c) return TG_ERR_ARG;

@@ -48,6 +48,12 @@ SIGNATURES = {
     "tg_hamiltk_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp]),
     "tg_last_timing": (C.c_int, [C.c_void_p, _dp]),
     "tg_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "tg_jacobian": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _ip, _dp, _dp, C.c_int, C.c_int, _dp]),
+    "tg_jacobian_layout": (C.c_int, [C.c_int, _ip, C.c_int, _ip, _dp, _dp, C.c_int, _ip]),
+    "tg_jacobian_assemble": (C.c_int, [C.c_int, _ip, C.c_int, _ip, _dp, _dp, C.c_int, C.c_int, C.c_int, _dp, _dp,
+                                       C.c_int, _dp]),
+    "tg_adjoint_vb": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
+    "tg_system_shape": (C.c_int, [C.c_void_p, _ip, _ip, _ip]),
 }
 
 
@@ -75,6 +81,46 @@ def load_library(path: str = LIB_PATH):
 
 def _p(a, ctype=C.c_double):
     return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def jacobian_inputs(system):
+    """dmask(norb_max, n_atoms), Un, Um and norb arrays of a system for the Jacobian entry points."""
+    nat = system.n_atoms
+    nmax = max(system.norbs)
+    dmask = np.zeros((nat, nmax), np.int32)
+    for i, dl in enumerate(system.dorbs):
+        dmask[i, list(dl)] = 1
+    return (dmask, np.ascontiguousarray(system.Un(), np.float64), np.ascontiguousarray(system.Um(), np.float64),
+            np.ascontiguousarray(system.norbs, np.int32))
+
+
+def jacobian_layout(system, fixEf=False):
+    """(neq, per) of tg_jacobian_layout: unknown count and first unknown of each site."""
+    lib = load_library()
+    dmask, Un, Um, norb = jacobian_inputs(system)
+    per = np.zeros(system.n_atoms + 1, np.int32)
+    neq = lib.tg_jacobian_layout(system.n_atoms, _p(norb, C.c_int), dmask.shape[1], _p(dmask, C.c_int), _p(Un),
+                                 _p(Um), 1 if fixEf else 0, _p(per, C.c_int))
+    if neq < 0:
+        raise TitanGPUError(neq, "tg_jacobian_layout: bad arguments")
+    return neq, per
+
+
+def jacobian_assemble(system, T, D, fixEf=False):
+    """Host-only tg_jacobian_assemble: T[i, j, g, h, 16] (orbital resolved), D[i, mu, 4]."""
+    lib = load_library()
+    dmask, Un, Um, norb = jacobian_inputs(system)
+    neq, _ = jacobian_layout(system, fixEf)
+    T = np.ascontiguousarray(T, np.complex128)
+    nrow, ncol = T.shape[2], T.shape[3]
+    Dp = _p(np.ascontiguousarray(D, np.complex128).view(np.float64)) if D is not None else None
+    J = np.zeros((neq, neq), np.float64, order="F")
+    rc = lib.tg_jacobian_assemble(system.n_atoms, _p(norb, C.c_int), dmask.shape[1], _p(dmask, C.c_int), _p(Un),
+                                  _p(Um), 1 if fixEf else 0, nrow, ncol, _p(T.view(np.float64)), Dp, neq,
+                                  J.ctypes.data_as(_dp))
+    if rc != 0:
+        raise TitanGPUError(rc, "tg_jacobian_assemble: bad arguments")
+    return np.ascontiguousarray(J)
 
 
 def _fortran_complex(m):
@@ -225,6 +271,22 @@ class GreenGPU:
         D = np.zeros((nat, self.nmax, 4), np.complex128)
         self._check(self.lib.tg_fermi_column(self.h, Ef, eta, _p(D.view(np.float64))))
         return D
+
+    def jacobian(self, Ef, eta, fixEf=False):
+        """calcJacobian_greenfunction on the GPU: J[neq, neq] (row = equation, column = unknown)."""
+        dmask, Un, Um, _ = jacobian_inputs(self.system)
+        neq, _ = jacobian_layout(self.system, fixEf)
+        J = np.zeros((neq, neq), np.float64, order="F")
+        self._check(self.lib.tg_jacobian(self.h, Ef, eta, _p(dmask, C.c_int), _p(Un), _p(Um), 1 if fixEf else 0, neq,
+                                         J.ctypes.data_as(_dp)))
+        return np.ascontiguousarray(J)
+
+    def adjoint_vb(self, Ef, eta):
+        """A[4 n_atoms, 4 n_atoms] = d(n, mx, my, mz)_i / d(V, Bx, By, Bz)_j (tg_adjoint_vb)."""
+        m = 4 * self.system.n_atoms
+        A = np.zeros((m, m), np.float64, order="F")
+        self._check(self.lib.tg_adjoint_vb(self.h, Ef, eta, A.ctypes.data_as(_dp)))
+        return np.ascontiguousarray(A)
 
     def dyson(self, chi_hf, U):
         n = chi_hf.shape[0]
