@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--compare-fp64", action="store_true", help="also time the FP64 path and report the ratio")
+    ap.add_argument("--small", action="store_true",
+                    help="30 x 30 k mesh, 64 + 16 energies: a few-second case for profiler captures")
     return ap.parse_args()
 
 
@@ -104,10 +106,11 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- workload
-def workload(config: str):
+def workload(config: str, small: bool = False):
     from titan_b200.host import synthetic
     from titan_b200.host.system import initial_state
-    deck = synthetic.make_deck(config)
+    deck = synthetic.make_deck(config, nk=(30, 30, 30), n1gl=32, parts=2, n3gl=16) if small else \
+        synthetic.make_deck(config)
     s = deck.system
     h0 = s.h0(initial_state(s))
     omegas = deck.frequencies()
@@ -121,6 +124,22 @@ def units_of(deck, omegas_idx, reals):
     return sum(nimag + len(reals[i][0]) * nk for i in omegas_idx)
 
 
+def inversions_of(deck, per, reals, first):
+    """Matrix inversions in one step: G2 once per imaginary point (shared by the step's
+    frequencies), G1 per imaginary point and frequency (G1 = G2 at e = 0, q = 0), and
+    two per real-axis point."""
+    n_om = len(reals)
+    idx = [(first + j) % n_om for j in range(per)]
+    nimag = deck.ek.n_points
+    nk = deck.real_kp.shape[0]
+    inv = nimag
+    for i in idx:
+        if len(reals[i][0]) == 0 and i == idx[0]:
+            continue
+        inv += nimag + 2 * len(reals[i][0]) * nk
+    return inv
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -130,7 +149,12 @@ def peaks():
 
 
 def cpu_baseline(deck, h0, reals, omegas, seconds_target=15.0):
-    """The oracle (numpy/LAPACK, all host threads) on a bounded sample of the workload."""
+    """The oracle (numpy/LAPACK, all host threads) on a bounded sample of the workload.
+
+    A 200-point calibration run sizes the sample so that it takes about
+    seconds_target: two thirds imaginary-axis points (in mesh order), one
+    third real-axis points (all real energies of omega_1 x the first k points).
+    """
     from oracle import titan_oracle as O
     from titan_b200.host.mesh import EKMesh
     s = deck.system
@@ -138,14 +162,20 @@ def cpu_baseline(deck, h0, reals, omegas, seconds_target=15.0):
     w_idx = 1 if len(omegas) > 1 else 0
     e = float(omegas[w_idx])
     x2, p2 = reals[w_idx]
-    n_imag_s = 1500
     ek = deck.ek
-    sub = EKMesh(ek.y, ek.wght, ek.energy_index[:n_imag_s], ek.kp[:n_imag_s], ek.weight[:n_imag_s])
-    nk_s = 24 if len(x2) else 0
-    rk = (deck.real_kp[:max(nk_s, 1)], deck.real_w[:max(nk_s, 1)])
-    t0 = time.perf_counter()
-    O.eintshechi(m, sub, rk, np.zeros(3), e, s.Ef, s.eta, s.etap, x2 if nk_s else None, p2 if nk_s else None)
-    dt = time.perf_counter() - t0
+
+    def run(n_imag_s, nk_s):
+        sub = EKMesh(ek.y, ek.wght, ek.energy_index[:n_imag_s], ek.kp[:n_imag_s], ek.weight[:n_imag_s])
+        rk = (deck.real_kp[:max(nk_s, 1)], deck.real_w[:max(nk_s, 1)])
+        t0 = time.perf_counter()
+        O.eintshechi(m, sub, rk, np.zeros(3), e, s.Ef, s.eta, s.etap, x2 if nk_s else None, p2 if nk_s else None)
+        return time.perf_counter() - t0
+
+    cal = min(200, ek.n_points)
+    rate = cal / max(run(cal, 0), 1e-6)
+    n_imag_s = int(min(ek.n_points, max(500, rate * seconds_target * 2 / 3)))
+    nk_s = int(min(deck.real_kp.shape[0], max(1, rate * seconds_target / 3 / max(len(x2), 1)))) if len(x2) else 0
+    dt = run(n_imag_s, nk_s)
     units = n_imag_s + len(x2) * nk_s
     cores = os.cpu_count()
     return {"value": units / dt, "unit": UNIT, "cores": cores, "kind": "port",
@@ -158,7 +188,7 @@ def cpu_baseline(deck, h0, reals, omegas, seconds_target=15.0):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    deck, h0, omegas, reals = workload(args.config)
+    deck, h0, omegas, reals = workload(args.config, args.small)
     cb = None
     vals = []
     for _ in range(args.warmup if args.warmup < 1 else 1):
@@ -198,7 +228,7 @@ def run_ours(args, rank, world, local_rank):
     import torch
     from titan_b200.native import GreenGPU
     torch.cuda.set_device(local_rank)
-    deck, h0, omegas, reals = workload(args.config)
+    deck, h0, omegas, reals = workload(args.config, args.small)
     s = deck.system
     gpu = GreenGPU(local_rank)
     gpu.setup(deck, h0)
@@ -220,22 +250,39 @@ def run_ours(args, rank, world, local_rank):
     total_ms_max = allreduce_max(total_ms, world)
     units_all = allreduce_sum(units, world)
     value = units_all / (total_ms_max / 1e3)
-    # dominant kernel: the chi0 contraction (kind 1), algorithmic flops 8 * dimens^2 per unit
+    # roofline of the chi0 contraction kernel (kind 1: the tcgen05 kernel alone on the split
+    # path, the FP64 GEMM on the fp64 path): algorithmic 8 * dimens^2 flops per unit
     con_ms, con_n = last[6], last[7]
     grn_ms, grn_n = last[4], last[5]
+    q_ms, q_n = last[11], last[12]
     last_units = units_of(deck, [(start + args.warmup * per + (args.steps - 1) * per + j) % len(omegas)
                                  for j in range(per)], reals)
     pk, pk_kind = peaks()
     flops_con = 8.0 * s.dimens ** 2 * last_units
     achieved = flops_con / (con_ms / 1e3) / 1e12 if con_ms > 0 else None
-    peak = pk.get("bf16_tflops_sustained" if False else "bf16_tflops")
+    peak = pk.get("bf16_tflops")
+    # DRAM traffic per contraction launch from the ncu capture in
+    # profiles/split_contract_sq2_small.md (3.999 GB over 1984 K-steps of 32 points),
+    # scaled by the K-steps one launch of this run processes
+    kstep_bytes = 3.999e9 / 1984
+    traffic = kstep_bytes * (last_units / 32.0) / con_n if (con_n and args.precision == "split") else None
     roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": (achieved / peak) if achieved else None, "traffic": None,
-            "kernel": "chi0 contraction (" + ("tcgen05 int8-sliced" if args.precision == "split" else "fp64 SIMT") + ")",
-            "peak_source": f"{pk_kind} bf16 dense (MEASURED_PEAKS.json)" if pk_kind == "measured" else "fallback 1.59 PF",
+            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+            "kernel": "chi0 contraction (" + ("tcgen05 int8-sliced split_contract_kernel" if args.precision == "split"
+                                              else "fp64 SIMT gemm64_kernel") + ")",
+            "peak_source": ("of measured bf16 dense burst (MEASURED_PEAKS.json)" if pk_kind == "measured"
+                            else "of fallback 1.59 PF"),
+            "flops_per_unit": 8.0 * s.dimens ** 2,
             "launches_in_last_step": int(con_n), "avg_launch_ms": (con_ms / con_n) if con_n else None,
-            "inversion_ms_last_step": grn_ms, "inversion_launches_last_step": int(grn_n),
-            "inversion_fp64_tflops": (8.0 * s.dimH ** 3 * (2 * last_units)) / (grn_ms / 1e3) / 1e12 if grn_ms else None}
+            "quantize_ms_last_step": q_ms if args.precision == "split" else None}
+    fp64_nominal = 37.0
+    roof_inv = {"bound": "fp64", "achieved": (8.0 * s.dimH ** 3 * inversions_of(deck, per, reals, start + args.warmup
+                                                                               * per + (args.steps - 1) * per))
+                / (grn_ms / 1e3) / 1e12 if grn_ms else None,
+                "peak": fp64_nominal, "unit": "TFLOP/s", "peak_source": "nominal B200 FP64 (not measured)",
+                "kernel": "green_team_kernel (fused H(k) + Gauss-Jordan)", "flops_per_inversion": 8.0 * s.dimH ** 3,
+                "ms_last_step": grn_ms, "launches_in_last_step": int(grn_n)}
+    roof_inv["frac"] = roof_inv["achieved"] / fp64_nominal if roof_inv["achieved"] else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
@@ -245,7 +292,7 @@ def run_ours(args, rank, world, local_rank):
                                    f"points, {deck.real_kp.shape[0]} real-axis k x 64 energies, 32 omega in [0,0.5], q=0",
                        "omegas_per_step": per, "precision": args.precision,
                        "l2": "inputs larger than L2 (mesh 200+ MB, operands GBs per pass)"},
-            "roofline": roof, "gpu_launches": launches, "clocks": clocks}
+            "roofline": roof, "roofline_inversion": roof_inv, "gpu_launches": launches, "clocks": clocks}
     if args.compare_fp64 and args.precision != "fp64":
         ms64, u64, _, _ = timed_steps(gpu, deck, h0, omegas, reals, 1, start + args.warmup * per, per, "fp64")
         line["fp64_path"] = {"value": u64 / (sum(ms64) / 1e3), "unit": UNIT, "ms_per_step": sum(ms64)}
@@ -311,7 +358,7 @@ def allreduce_max(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    t = torch.tensor([float(x)], device="cuda" if dist.get_backend() == "nccl" else "cpu", dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -321,7 +368,7 @@ def allreduce_sum(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    t = torch.tensor([float(x)], device="cuda" if dist.get_backend() == "nccl" else "cpu", dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
@@ -331,6 +378,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        # the CPU reference arm: rank 0 alone works; no process group, no GPU
+        run_reference(args, rank, world)
+        return
     if world > 1:
         import datetime
         import torch
@@ -338,10 +389,7 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        if args.impl == "reference":
-            run_reference(args, rank, world)
-        else:
-            run_ours(args, rank, world, local_rank)
+        run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -155,9 +155,10 @@ int tg_hamiltk_batch(tg_ctx* ctx, int64_t nk, const double* kp, double* H);
 /* Device timing of the last tg_chi0/tg_chi0_batch call (CUDA events on the
  * context's stream): ms[0] imaginary-axis G2 inversions, ms[1] contraction and
  * the other inversions, ms[2] epilogue, ms[3] whole call; when per-launch
- * profiling is on (tg_profile), ms[4..9] = (total ms, launches) of the
- * inversion, contraction and epilogue kernels; ms[10] = kernels launched.
- * ms must hold 11 doubles. */
+ * profiling is on (tg_profile), ms[4..9] = (total ms, timed regions) of the
+ * inversion, contraction and epilogue kernels, ms[11..12] the same for the
+ * split-precision quantisation (row maxima + digit planes); ms[10] = kernels
+ * launched.  ms must hold 13 doubles. */
 int tg_last_timing(const tg_ctx* ctx, double* ms);
 int tg_profile(tg_ctx* ctx, int enable);
 

@@ -108,7 +108,7 @@ struct tg_ctx {
   bool profile = false;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_used;
-  double kind_ms[4] = {0, 0, 0, 0};
+  double kind_ms[4] = {0, 0, 0, 0};   // 0 inversion, 1 contraction, 2 epilogue, 3 split quantisation
   int kind_n[4] = {0, 0, 0, 0};
   int64_t launches = 0;   // kernels launched by the last chi0 call
   int64_t pass_points = 0;     // points per pass (bounded workspace)
@@ -140,7 +140,7 @@ struct KindTimer {
     cudaEventRecord(a, c->stream);
   }
   ~KindTimer() {
-    if (kind != 1) c->launches += 1;   // contraction launches are counted by contract()
+    if (kind == 0 || kind == 2) c->launches += 1;   // contraction / quantize launches are counted where issued
     if (!c->profile) return;
     cudaEventRecord(b, c->stream);
     c->ev_used.push_back({kind, {a, b}});
@@ -712,17 +712,21 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     float ms = 0;
     SplitPassDev pd;
     if (split) {
-      KindTimer kt(c, 1);
+      KindTimer kt(c, 3);
       const double* yv = c->h_y.data() + p0;
       if ((rc = split_prepare(c, make_chunks(np, [&](int64_t i) { return yv[i]; }), pd))) return rc;
       if ((rc = split_quantize_operand(c, 1, c->d_B.p, pd))) return rc;
     }
     if (w_start == 1) {
-      KindTimer kt(c, 1);
       if (split) {
-        if ((rc = split_quantize_operand(c, 0, c->d_A.p, pd))) return rc;
+        {
+          KindTimer kq(c, 3);
+          if ((rc = split_quantize_operand(c, 0, c->d_A.p, pd))) return rc;
+        }
+        KindTimer kt(c, 1);
         rc = split_contract_pass(c, pd, c->d_C.p, nsplit, cstride);
       } else {
+        KindTimer kt(c, 1);
         rc = contract(c, c->d_A.p, c->d_B.p, np, c->d_C.p, nsplit, cstride);
       }
       if (rc) return rc;
@@ -744,12 +748,16 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
         TG_CHECK(c, launch_green(g1, c->num_sms, s, nullptr), "green (imag, G1)");
       }
       {
-        KindTimer kt(c, 1);
         double2* Cw = c->d_C.p + (size_t)w * nsplit * cstride;
         if (split) {
-          rc = split_quantize_operand(c, 0, c->d_A.p, pd);
+          {
+            KindTimer kq(c, 3);
+            rc = split_quantize_operand(c, 0, c->d_A.p, pd);
+          }
+          KindTimer kt(c, 1);
           if (!rc) rc = split_contract_pass(c, pd, Cw, nsplit, cstride);
         } else {
+          KindTimer kt(c, 1);
           rc = contract(c, c->d_A.p, c->d_B.p, np, Cw, nsplit, cstride);
         }
       }
@@ -802,16 +810,20 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
         TG_CHECK(c, launch_green(gr, c->num_sms, s, nullptr), "green (real, G1)");
       }
       {
-        KindTimer kt(c, 1);
         double2* Dw = c->d_D.p + (size_t)w * nsplit * cstride;
         if (split) {
           SplitPassDev pr;
           const int64_t nrk = c->n_realk, pbase = p0;
-          rc = split_prepare(c, make_chunks(np, [&](int64_t i) { return (pbase + i) / nrk; }), pr);
-          if (!rc) rc = split_quantize_operand(c, 1, c->d_B.p, pr);
-          if (!rc) rc = split_quantize_operand(c, 0, c->d_A.p, pr);
+          {
+            KindTimer kq(c, 3);
+            rc = split_prepare(c, make_chunks(np, [&](int64_t i) { return (pbase + i) / nrk; }), pr);
+            if (!rc) rc = split_quantize_operand(c, 1, c->d_B.p, pr);
+            if (!rc) rc = split_quantize_operand(c, 0, c->d_A.p, pr);
+          }
+          KindTimer kt(c, 1);
           if (!rc) rc = split_contract_pass(c, pr, Dw, nsplit, cstride);
         } else {
+          KindTimer kt(c, 1);
           rc = contract(c, c->d_A.p, c->d_B.p, np, Dw, nsplit, cstride);
         }
       }
@@ -869,6 +881,8 @@ int tg_last_timing(const tg_ctx* c, double* ms) {
     ms[5 + 2 * i] = c->kind_n[i];
   }
   ms[10] = (double)c->launches;
+  ms[11] = c->kind_ms[3];
+  ms[12] = c->kind_n[3];
   return TG_OK;
 }
 

@@ -232,7 +232,7 @@ class GreenGPU:
 
     def last_timing(self):
         """Device ms of the last chi0 call (see tg_last_timing)."""
-        ms = np.zeros(11)
+        ms = np.zeros(13)
         self._check(self.lib.tg_last_timing(self.h, _p(ms)))
         return ms
 
