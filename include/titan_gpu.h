@@ -88,6 +88,17 @@ int tg_chi0_batch(tg_ctx* ctx, const double* q, int n_omega, const double* e, do
 int tg_expectation(tg_ctx* ctx, double Ef, double eta, double* rho, double* mx, double* my,
                    double* mz, double* mp);
 
+/* tg_expectation without device allocation, for callers that cannot let a
+ * library call allocate (a fixed HBM budget, or work recorded into a stream
+ * capture).  No counterpart in the reference.  Same outputs as tg_expectation;
+ * H(k) is summed inside the kernel and the partial sums live in a fixed 8 MiB
+ * device array of the library: (16 x SMs + 1) x 2 dimH complex must fit, else
+ * TG_ERR_ARG.  The first call on a device looks the array up (make it before any
+ * stream capture); nothing has to start at zero; calls that overlap in time on
+ * one device race on the shared array. */
+int tg_expectation_noalloc(tg_ctx* ctx, double Ef, double eta, double* rho, double* mx, double* my,
+                           double* mz, double* mp);
+
 /* Orbital-diagonal GG tensor for the Jacobian and its adjoint:
  *   T(16, ncol, nrow, n_atoms(j), n_atoms(i)) complex with
  *   T[s',t,t',s; i,g; j,h] = sum_p w_p sum_{mu in g} sum_{nu in h}

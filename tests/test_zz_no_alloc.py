@@ -1,0 +1,45 @@
+"""tg_expectation_noalloc through the C ABI against tg_expectation (needs a B200).
+
+Collected last (file name), so it runs both alone and after the other GPU tests;
+each system is checked on a fresh context with the no-alloc call first (the call
+that performs the per-device scratch lookup), twice in a row.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from titan_b200.host import synthetic
+from titan_b200.host.system import initial_state
+
+pytestmark = pytest.mark.gpu
+
+
+def _call_noalloc(gpu, Ef, eta):
+    nat, nmax = gpu.system.n_atoms, gpu.nmax
+    out = [np.zeros((nat, nmax)) for _ in range(4)]
+    mp = np.zeros((nat, nmax), np.complex128)
+    dp = C.POINTER(C.c_double)
+    rc = gpu.lib.tg_expectation_noalloc(gpu.h, Ef, eta, *[o.ctypes.data_as(dp) for o in out],
+                                        mp.view(np.float64).ctypes.data_as(dp))
+    assert rc == 0, gpu.lib.tg_last_error(gpu.h)
+    return out + [mp]
+
+
+@pytest.mark.parametrize("shape,nk", [("bcc1", (4, 4, 4)), ("sq2", (6, 6, 1))])
+def test_noalloc_expectation_matches_tg_expectation(shape, nk):
+    from titan_b200.native import GreenGPU
+    deck = synthetic.make_deck(shape, nk=nk, n1gl=8, parts=1, n3gl=4)
+    s = deck.system
+    h0 = s.h0(initial_state(s))
+    gpu = GreenGPU(0)
+    try:
+        gpu.setup(deck, h0)
+        first = _call_noalloc(gpu, s.Ef, s.eta)
+        second = _call_noalloc(gpu, s.Ef, s.eta)
+        ref = list(gpu.expectation(s.Ef, s.eta))
+        for got in (first, second):
+            for a, b in zip(got, ref):
+                assert np.max(np.abs(a - b)) < 1e-12
+    finally:
+        gpu.close()

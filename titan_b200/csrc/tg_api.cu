@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1209,3 +1210,121 @@ int tg_dyson(tg_ctx* c, int dimens, const double* chi_hf, const double* umat, do
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// tg_expectation_noalloc: occupations and moments without device allocation.
+//
+// For callers that cannot let a library call allocate device memory: a host
+// that budgets every byte of HBM up front, or code that records its work into
+// a stream capture, where cudaMalloc is not allowed.  tg_expectation allocates
+// its per-team partial sums (and an H(k) table) on first use; this variant keeps
+// the partial sums in a fixed 8 MiB device array compiled into the library and
+// sums H(k) inside the inversion kernel instead of tabulating it.
+//
+// * Size limit: (16 x SMs + 1) x 2 dimH complex doubles must fit in 8 MiB
+//   (dimH <= 90 on a 148-SM B200 needs 6.8 MB); larger requests return
+//   TG_ERR_ARG before any work.
+// * Setup: the first call on each device looks up the array's device address
+//   (cudaGetSymbolAddress, which also loads this module on that device if it is
+//   not loaded yet); make one call before beginning any stream capture.
+// * Nothing in the scratch has to start at zero: every partial slot the
+//   reduction reads is written by the kernel of the same call.
+// * One array serves every context and stream of a device: calls that overlap
+//   in time on the same device race on it.  A call returns only after its
+//   results are on the host, so calls made one after another are safe.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kNoAllocScratchBytes = (size_t)8 << 20;
+constexpr int kNoAllocMaxDevices = 64;
+constexpr int kNoAllocMaxLen = 512;   // 2 dimH complex sums per partial slot
+std::atomic<double2*> g_noalloc_ptr[kNoAllocMaxDevices];
+}  // namespace
+
+static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double2)];
+
+namespace {
+// device address of the scratch on the current device (looked up once per device)
+int noalloc_scratch(tg_ctx* c, double2** out) {
+  if (c->device < 0 || c->device >= kNoAllocMaxDevices)
+    return set_err(c, TG_ERR_ARG, "tg_expectation_noalloc: device index beyond the scratch table");
+  double2* p = g_noalloc_ptr[c->device].load(std::memory_order_acquire);
+  if (!p) {
+    void* q = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&q, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_err(c, e, "tg_expectation_noalloc: scratch address");
+    p = static_cast<double2*>(q);
+    g_noalloc_ptr[c->device].store(p, std::memory_order_release);
+  }
+  *out = p;
+  return TG_OK;
+}
+}  // namespace
+
+extern "C" int tg_expectation_noalloc(tg_ctx* c, double Ef, double eta, double* rho, double* mx, double* my,
+                                      double* mz, double* mp) {
+  int rc = check_ready(c, true, false);
+  if (rc) return rc;
+  if (!rho || !mx || !my || !mz || !mp) return set_err(c, TG_ERR_ARG, "tg_expectation_noalloc: null output");
+  const int n = c->dimH;
+  const int len = 2 * n;
+  // partial slots: the team kernel runs at most 15 teams per SM (per-SM CTAs x teams <= 8 + teams - 1)
+  const size_t slots = (size_t)c->num_sms * 16;
+  const size_t need = (slots + 1) * (size_t)len * sizeof(double2);
+  if (len > kNoAllocMaxLen || need > kNoAllocScratchBytes) {
+    char b[160];
+    snprintf(b, sizeof b, "tg_expectation_noalloc: needs %zu bytes of scratch, the fixed scratch holds %zu",
+             need, kNoAllocScratchBytes);
+    return set_err(c, TG_ERR_ARG, b);
+  }
+  cudaSetDevice(c->device);
+  double2* scratch = nullptr;
+  if ((rc = noalloc_scratch(c, &scratch))) return rc;
+  double2* partial = scratch;
+  double2* reduced = scratch + slots * len;
+  cudaStream_t s = c->stream;
+  GreenArgs a = base_args(c);
+  a.pts.kind = 0;
+  a.pts.y = c->d_y.p;
+  a.pts.kp = c->d_kp.p;
+  a.pts.w = c->d_w.p;
+  a.p0 = 0;
+  a.np = c->n_imag;
+  a.zr = Ef;
+  a.zi = eta;
+  a.mode = MODE_EXPECT;
+  a.gg_desc = c->d_exp_rows.p;
+  a.acc = partial;
+  a.acc_len = 0;
+  rc = reset_status(c);
+  if (rc) return rc;
+  int grid = 0;
+  TG_CHECK(c, launch_green(a, c->num_sms, s, &grid), "green (expectation, no-alloc)");
+  TG_CHECK(c, launch_reduce_blocks(partial, grid, len, reduced, s), "reduce");
+  double2 h[kNoAllocMaxLen];
+  TG_CHECK(c, cudaMemcpyAsync(h, reduced, sizeof(double2) * len, cudaMemcpyDeviceToHost, s), "copy");
+  rc = read_status(c);
+  if (rc) return rc;
+  // mod_expectation.F90:121-147
+  int o = 0;
+  for (int i = 0; i < c->n_atoms; ++i) {
+    for (int mu = 0; mu < c->nmax; ++mu) {
+      const size_t idx = (size_t)i * c->nmax + mu;
+      if (mu >= c->norb[i]) {
+        rho[idx] = mx[idx] = my[idx] = mz[idx] = 0.0;
+        mp[2 * idx] = mp[2 * idx + 1] = 0.0;
+        continue;
+      }
+      const double2 uu = h[4 * o], dd = h[4 * o + 1], ud = h[4 * o + 2], du = h[4 * o + 3];
+      const double nu_ = 0.5 + uu.x / kPi, nd_ = 0.5 + dd.x / kPi;
+      rho[idx] = nu_ + nd_;
+      mz[idx] = nu_ - nd_;
+      const double mpr = (du.x + ud.x) / kPi, mpi = (du.y - ud.y) / kPi;
+      mx[idx] = mpr;
+      my[idx] = mpi;
+      mp[2 * idx] = mpr;
+      mp[2 * idx + 1] = mpi;
+      ++o;
+    }
+  }
+  return TG_OK;
+}

@@ -54,6 +54,7 @@ SIGNATURES = {
                                        C.c_int, _dp]),
     "tg_adjoint_vb": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
     "tg_system_shape": (C.c_int, [C.c_void_p, _ip, _ip, _ip]),
+    "tg_expectation_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp]),
 }
 
 
@@ -245,6 +246,15 @@ class GreenGPU:
         out = [np.zeros((nat, self.nmax)) for _ in range(4)]
         mp = np.zeros((nat, self.nmax), np.complex128)
         rc = self.lib.tg_expectation(self.h, Ef, eta, *[_p(o) for o in out], _p(mp.view(np.float64)))
+        self._check(rc)
+        return out[0], out[1], out[2], out[3], mp
+
+    def expectation_noalloc(self, Ef, eta):
+        """expectation() without device allocation during the call (tg_expectation_noalloc)."""
+        nat = self.system.n_atoms
+        out = [np.zeros((nat, self.nmax)) for _ in range(4)]
+        mp = np.zeros((nat, self.nmax), np.complex128)
+        rc = self.lib.tg_expectation_noalloc(self.h, Ef, eta, *[_p(o) for o in out], _p(mp.view(np.float64)))
         self._check(rc)
         return out[0], out[1], out[2], out[3], mp
 
