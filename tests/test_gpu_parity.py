@@ -209,3 +209,33 @@ def test_chi0_split_fe_golden(gpu, fe_deck, fe_chi_golden):
         for a, b in zip(hf_row, ghf[idx]):
             if abs(b) > 1e-6:
                 assert abs(a - b) <= 1e-8 * abs(b), (idx, a, b)
+
+
+@pytest.mark.parametrize("shape,nk", [("bcc4", (2, 2, 2)), ("slab5", (3, 3, 1))])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("split", 1e-9)])
+def test_chi0_larger_cells_match_oracle(gpu, shape, nk, precision, tol):
+    """4-atom bcc (dimH 72) and 5-layer slab (dimH 90): 16 and 25 site pairs."""
+    deck = synthetic.make_deck(shape, nk=nk, n1gl=4, parts=1, n3gl=4)
+    s, h0 = _setup(gpu, deck)
+    e = 0.05
+    x2, p2 = deck.real_points(e, s.Ef)
+    q = np.array([0.03, 0.0, 0.0])
+    chi = gpu.chi0(q, e, s.Ef, s.eta, s.etap, x2, p2, precision=precision)
+    ref = O.eintshechi(O.Model(s, h0), deck.ek, (deck.real_kp, deck.real_w), q, e, s.Ef, s.eta, s.etap, x2, p2)
+    assert rel(chi, ref) < tol
+
+
+def test_chi0_sharded_mesh_sums_to_full(gpu):
+    """Two mesh shares (as two ranks would hold them) add up to the full chi0."""
+    from titan_b200.host.sharding import shard_imag_mesh, shard_real_bz
+    deck = synthetic.make_deck("sq2", nk=(6, 6, 1), n1gl=8, parts=1, n3gl=6)
+    s, h0 = _setup(gpu, deck)
+    e = 0.05
+    x2, p2 = deck.real_points(e, s.Ef)
+    full = gpu.chi0(np.zeros(3), e, s.Ef, s.eta, s.etap, x2, p2, precision="fp64")
+    parts = []
+    for r in range(2):
+        gpu.set_imag_mesh(shard_imag_mesh(deck.ek, r, 2))
+        gpu.set_real_mesh(*shard_real_bz(deck.real_kp, deck.real_w, r, 2))
+        parts.append(gpu.chi0(np.zeros(3), e, s.Ef, s.eta, s.etap, x2, p2, precision="fp64"))
+    assert rel(parts[0] + parts[1], full) < 1e-13

@@ -494,6 +494,7 @@ int green_acc_ctas(int n, int64_t np, int num_sms) {
 }
 
 cudaError_t launch_green(const GreenArgs& a, int num_sms, cudaStream_t s, int* grid_used) {
+  if (green_w1_supported(a.n, a.mode)) return launch_green_w1(a, num_sms, s, grid_used);
   if (green_warp_supported(a.n, a.mode)) return launch_green_warp(a, num_sms, s, grid_used);
   const Cfg* c = find_cfg(a.n);
   if (!c) return cudaErrorInvalidValue;

@@ -141,6 +141,8 @@ cudaError_t launch_green(const GreenArgs& a, int num_sms, cudaStream_t s, int* g
 int green_supported(int n);
 int green_warp_supported(int n, int mode);
 cudaError_t launch_green_warp(const GreenArgs& a, int num_sms, cudaStream_t s, int* grid_used);
+int green_w1_supported(int n, int mode);
+cudaError_t launch_green_w1(const GreenArgs& a, int num_sms, cudaStream_t s, int* grid_used);
 int green_acc_ctas(int n, int64_t np, int num_sms);
 
 // FP64 pair-block contraction: Cpart[split][cpair_off + u*M + v] += sum_p A[p][off+u] B[p][off+v]
