@@ -148,14 +148,18 @@ def eintshechi(model: Model, mesh, real_bz, q, e, Ef, eta, etap, x2=None, p2=Non
                     t2 = np.conj(np.einsum("pmx,pgv->mvgx", c, d, optimize=True))
                     scatter(chi, i, j, s1, s2, t1 + t2)
     if x2 is not None and len(x2) > 0:
+        # every (energy, k) pair of the real-axis loops (eintshechi.F90:112-170) as one flat list
         kpr, wr = real_bz
         nkr = kpr.shape[0]
-        for nep in range(len(x2)):
-            for sl in _chunks(nkr, chunk):
-                kp = kpr[sl]
-                w = p2[nep] * wr[sl]
-                g1 = model.green(x2[nep] + e + 1j * eta, kp + q[None, :])
-                g2 = model.green(x2[nep] + 1j * etap, kp)
+        xs = np.repeat(np.asarray(x2, float), nkr)
+        ws = np.repeat(np.asarray(p2, float), nkr) * np.tile(wr, len(x2))
+        ks = np.tile(kpr, (len(x2), 1))
+        for sl in _chunks(xs.shape[0], chunk):
+            if True:
+                kp = ks[sl]
+                w = ws[sl]
+                g1 = model.green(xs[sl] + e + 1j * eta, kp + q[None, :])
+                g2 = model.green(xs[sl] + 1j * etap, kp)
                 for j in range(nat):
                     for i in range(nat):
                         for (s1, s2), (a1, a2, b1) in REAL.items():

@@ -2,7 +2,7 @@
 
 The reference tests this path only through example runs compared against
 ``results_correct`` files (its CI: .gitlab-ci.yml, jobs Fe_bulk, Fe_bulk:susc,
-graphene_pz).  This script copies those example input decks and golden
+graphene_pz, nanoribbon).  This script copies those example input decks and golden
 outputs, unchanged, into ``tests/golden/<example>/`` so the tests can run
 without the reference tree.  Run it from the repository root:
 
@@ -24,7 +24,12 @@ FILES = {
         "input", "basis", "Gr",
         "results_correct/scResult",
     ],
+    "nanoribbon": [
+        "input", "basis", "A2", "A3",
+        "results_correct/scResult",
+    ],
 }
+NANO_SUFFIX = "parts=2_parts3=1_norb=2_nkpt=1000_eta=1.0E-03_ev_fixEf_Ef=-0.25_SOC=0.10_Vab=0.15_pxpy.dat"
 
 # golden files are stored flat under short names
 SHORT = {
@@ -43,6 +48,18 @@ def main(ref_root: str) -> None:
         for f in files:
             src = os.path.join(ref_root, "examples", ex, f)
             shutil.copyfile(src, os.path.join(dst, SHORT.get(f, os.path.basename(f))))
+        # nanoribbon: the self-consistent state and the 10 x 10 site pairs of chi_HF / chi_RPA
+        if ex == "nanoribbon":
+            base = os.path.join(ref_root, "examples", ex, "results_correct", "TSOC")
+            sc = "selfconsistency_10Sites_dfttype=S_" + NANO_SUFFIX.replace("parts3=1_", "")
+            shutil.copyfile(os.path.join(base, "selfconsistency", sc),
+                            os.path.join(dst, "selfconsistency.dat"))
+            for i in range(1, 11):
+                for j in range(1, 11):
+                    shutil.copyfile(os.path.join(base, "10Sites", "HF", f"chihf_{i}_{j}_" + NANO_SUFFIX),
+                                    os.path.join(dst, f"chihf_{i}_{j}.dat"))
+                    shutil.copyfile(os.path.join(base, "10Sites", "RPA", f"chi_{i}_{j}_" + NANO_SUFFIX),
+                                    os.path.join(dst, f"chi_{i}_{j}.dat"))
         # the graphene self-consistency file has a run-dependent name
         if ex == "graphene":
             sc_dir = os.path.join(ref_root, "examples", ex, "results_correct", "FSOC", "selfconsistency")

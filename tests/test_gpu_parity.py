@@ -239,3 +239,30 @@ def test_chi0_sharded_mesh_sums_to_full(gpu):
         gpu.set_real_mesh(*shard_real_bz(deck.real_kp, deck.real_w, r, 2))
         parts.append(gpu.chi0(np.zeros(3), e, s.Ef, s.eta, s.etap, x2, p2, precision="fp64"))
     assert rel(parts[0] + parts[1], full) < 1e-13
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_nanoribbon_golden_through_gpu(gpu, precision):
+    """The reference's 10-site px/py nanoribbon: chi_HF and chi_RPA of all 100 site
+    pairs at omega = 1e-6 through the GPU path (dimH 40, 100 pairs of 16 x 16)."""
+    from titan_b200.host.deck import Deck
+    from titan_b200.host.system import read_sc_file
+    d = Deck.from_directory(os.path.join(GOLDEN, "nanoribbon"))
+    s = d.system
+    st = read_sc_file(os.path.join(GOLDEN, "nanoribbon", "selfconsistency.dat"), s.norbs)
+    s.Ef = st.Ef
+    gpu.setup(d, s.h0(st))
+    e = float(d.frequencies()[0])
+    x2, p2 = d.real_points(e, s.Ef)
+    chi = gpu.chi0(np.zeros(3), e, s.Ef, s.eta, s.etap, x2, p2, precision=precision)
+    rpa = gpu.dyson(chi, O.umatrix(s))
+    schi, srpa = O.site_reduce(s, chi), O.site_reduce(s, rpa)
+    for i in range(1, s.n_atoms + 1):
+        for j in range(1, s.n_atoms + 1):
+            for kind, sc in (("chihf", schi), ("chi", srpa)):
+                f = os.path.join(GOLDEN, "nanoribbon", f"{kind}_{i}_{j}.dat")
+                g = [[float(x) for x in l.split()] for l in open(f) if not l.strip().startswith("#")][0]
+                r = O.golden_row(s, e, 0.0, sc, i - 1, j - 1)
+                for a, b in zip(r, g):
+                    if abs(b) > 1e-6:
+                        assert abs(a - b) <= 1e-8 * abs(b), (kind, i, j, a, b)

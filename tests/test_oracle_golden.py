@@ -81,3 +81,28 @@ def test_compare_output_rule():
     assert C.compare_rows([[-10.0]], [[-20.0]], 1e-5) == []
     assert C.compare_rows([[10.0]], [[20.0]], 1e-5) != []
     assert C.compare_rows([[1e-9]], [[2e-9]], 1e-7) == []
+
+
+def _golden_rows(name, kind, i, j):
+    f = os.path.join(GOLDEN, name, f"{kind}_{i}_{j}.dat")
+    return [[float(x) for x in l.split()] for l in open(f) if not l.strip().startswith("#")]
+
+
+def test_nanoribbon_chi_matches_golden():
+    """10-site px/py nanoribbon (100 site pairs): chi_HF and chi_RPA at omega = 1e-6
+    against the reference's results_correct files (CI TOL 1e-7, here 1e-8)."""
+    from oracle_pool import _load, chi_parallel
+    d, st = _load("nanoribbon")
+    s = d.system
+    e = float(d.frequencies()[0])
+    chi = chi_parallel("nanoribbon")
+    schi = O.site_reduce(s, chi)
+    rpa = O.site_reduce(s, O.dyson(chi, O.umatrix(s)))
+    for i in range(1, s.n_atoms + 1):
+        for j in range(1, s.n_atoms + 1):
+            for kind, sc in (("chihf", schi), ("chi", rpa)):
+                g = _golden_rows("nanoribbon", kind, i, j)[0]
+                r = O.golden_row(s, e, 0.0, sc, i - 1, j - 1)
+                for a, b in zip(r, g):
+                    if abs(b) > 1e-6:
+                        assert abs(a - b) <= 1e-8 * abs(b), (kind, i, j, a, b)
