@@ -484,3 +484,198 @@ def self_consistency(system, model_factory, mesh, real_bz, state0, fixEf=False, 
             break
     f, out, model = sc_residual(system, model_factory, mesh, x, template, fixEf)
     return x, out, f, it + 1
+
+
+# ---------------------------------------------------------------------------
+# Disturbance response (eintshe + calculate_all), source/eintshe.F90:2-309,
+# source/dtdksub.F90:2-28, source/calculate_all.F90:72-420.
+# Imaginary axis (eintshe.F90:104-179): for (sigma, sigma') the spin blocks
+# (X, Y, Z, W) of G1^X(nu,gama;i,j) G2^Y(xi,mu;l,i) + conj(G2^Z(mu,xi;i,l) G1^W(gama,nu;j,i)),
+# both terms times dtdk(gama,xi;j,l).
+# ---------------------------------------------------------------------------
+SHE_IMAG = {(1, 1): ("dd", "uu", "uu", "dd"), (1, 2): ("du", "uu", "uu", "ud"), (1, 3): ("dd", "du", "ud", "dd"),
+            (1, 4): ("du", "du", "ud", "ud"),
+            (2, 1): ("ud", "uu", "uu", "du"), (2, 2): ("uu", "uu", "uu", "uu"), (2, 3): ("ud", "du", "ud", "du"),
+            (2, 4): ("uu", "du", "ud", "uu"),
+            (3, 1): ("dd", "ud", "du", "dd"), (3, 2): ("du", "ud", "du", "ud"), (3, 3): ("dd", "dd", "dd", "dd"),
+            (3, 4): ("du", "dd", "dd", "ud"),
+            (4, 1): ("ud", "ud", "du", "du"), (4, 2): ("uu", "ud", "du", "uu"), (4, 3): ("ud", "dd", "dd", "du"),
+            (4, 4): ("uu", "dd", "dd", "uu")}
+# Real axis (eintshe.F90:226-249): -i (G1^X(nu,gama;i,j) - conj(G1^X'(gama,nu;j,i))) conj(G2^Y(mu,xi;i,l)) dtdk
+SHE_REAL = {(1, 1): ("dd", "dd", "uu"), (1, 2): ("du", "ud", "uu"), (1, 3): ("dd", "dd", "ud"), (1, 4): ("du", "ud", "ud"),
+            (2, 1): ("ud", "du", "uu"), (2, 2): ("uu", "uu", "uu"), (2, 3): ("ud", "du", "ud"), (2, 4): ("uu", "uu", "ud"),
+            (3, 1): ("dd", "dd", "du"), (3, 2): ("du", "ud", "du"), (3, 3): ("dd", "dd", "dd"), (3, 4): ("du", "ud", "dd"),
+            (4, 1): ("ud", "du", "du"), (4, 2): ("uu", "uu", "du"), (4, 3): ("ud", "du", "dd"), (4, 4): ("uu", "uu", "dd")}
+
+
+def _orbital_offsets(norbs):
+    off = [0]
+    for n in norbs:
+        off.append(off[-1] + n)
+    return off
+
+
+def dtdk(system, kp, ue):
+    """dtdksub: sum_neigh i (ue . R) t0i exp(i k . R), spinless orbital space (rows site j, cols site i)."""
+    cv, bi, ish, t = system.neighbor_table()
+    off = _orbital_offsets(system.norbs)
+    kp = np.atleast_2d(kp)
+    D = np.zeros((kp.shape[0], off[-1], off[-1]), dtype=complex)
+    ph = 1j * (cv @ np.asarray(ue, float))[None, :] * np.exp(1j * kp @ cv.T)
+    for k in range(cv.shape[0]):
+        j = int(bi[k])
+        for i in range(system.n_atoms):
+            if ish[k, i]:
+                nj, ni = system.norbs[j], system.norbs[i]
+                D[:, off[j]:off[j] + nj, off[i]:off[i] + ni] += ph[:, k, None, None] * t[k, i, :nj, :ni][None]
+    return D
+
+
+def _spin_blocks(G, system):
+    """{ab: G^{ab}} over all sites in the spinless orbital index space."""
+    ia = system.ia()
+    out = {}
+    for a in "ud":
+        for b in "ud":
+            rows = [ia[i][0] + _SPIN[a] * system.norbs[i] + m for i in range(system.n_atoms) for m in range(system.norbs[i])]
+            cols = [ia[i][0] + _SPIN[b] * system.norbs[i] + m for i in range(system.n_atoms) for m in range(system.norbs[i])]
+            out[a + b] = G[:, rows][:, :, cols]
+    return out
+
+
+def eintshe(model: Model, mesh, real_bz, q, e, Ef, eta, etap, x2, p2, efield, chunk=2048):
+    """Sum over (k, E) of the disturbance integrand df1iikl (dimens x 4) over 2 pi, before the
+    prefactor (eintshe.F90:2-309; the reference multiplies every point by the constant
+    prefactor, which is applied once to the sum here)."""
+    s = model.system
+    sidx = s.sigmaimunu2i()
+    off = _orbital_offsets(s.norbs)
+    df = np.zeros((s.dimens, 4), dtype=complex)
+    q = np.asarray(q, float)
+
+    def accumulate(sig, sigp, blk_num, w, transpose):
+        # blk_num[p, (i a), (i b)]: rows nu / cols mu (transpose=False) or rows mu / cols nu
+        for i in range(s.n_atoms):
+            n = s.norbs[i]
+            b = blk_num[:, off[i]:off[i] + n, off[i]:off[i] + n]
+            c = np.einsum("p,pab->ab", w, b)
+            c = c if transpose else c.T     # -> [mu, nu]
+            df[sidx[sig - 1, i, :n, :n].reshape(-1), sigp - 1] += c.reshape(-1)
+
+    y = mesh.point_energy()
+    for sl in _chunks(mesh.n_points, chunk):
+        kp = mesh.kp[sl]
+        w = mesh.weight[sl]
+        g1 = _spin_blocks(model.green(Ef + e + 1j * (y[sl] + eta), kp + q[None, :]), s)
+        g2 = _spin_blocks(model.green(Ef + 1j * (y[sl] + etap), kp), s)
+        D = dtdk(s, kp, efield)
+        DT = np.swapaxes(D, 1, 2)
+        for (sig, sigp), (X, Y, Z, W) in SHE_IMAG.items():
+            t1 = g1[X] @ D @ g2[Y]                                  # [(i nu), (i mu)]
+            t2 = np.conj(g2[Z]) @ DT @ np.conj(g1[W])               # [(i mu), (i nu)]
+            accumulate(sig, sigp, t1, w, False)
+            accumulate(sig, sigp, t2, w, True)
+    if x2 is not None and len(x2) > 0:
+        kpr, wr = real_bz
+        nkr = kpr.shape[0]
+        xs = np.repeat(np.asarray(x2, float), nkr)
+        ws = np.repeat(np.asarray(p2, float), nkr) * np.tile(wr, len(x2))
+        ks = np.tile(kpr, (len(x2), 1))
+        for sl in _chunks(xs.shape[0], chunk):
+            kp = ks[sl]
+            g1 = _spin_blocks(model.green(xs[sl] + e + 1j * eta, kp + q[None, :]), s)
+            g2 = _spin_blocks(model.green(xs[sl] + 1j * etap, kp), s)
+            D = dtdk(s, kp, efield)
+            for (sig, sigp), (X, Xp, Y) in SHE_REAL.items():
+                A = g1[X] - np.conj(np.swapaxes(g1[Xp], 1, 2))
+                t = -1j * (A @ D @ np.conj(np.swapaxes(g2[Y], 1, 2)))   # [(i nu), (i mu)]
+                accumulate(sig, sigp, t, ws[sl], False)
+    return df / TPI
+
+
+def type_lvec(orbs):
+    """Types%lvec: L_x, L_y, L_z restricted to a type's orbitals (mod_magnet.F90:295-345)."""
+    from titan_b200.host.onsite import l_matrices
+    L = l_matrices()
+    idx = [o - 1 for o in orbs]
+    return L[:, idx][:, :, idx]
+
+
+def disturbance_outputs(system, chi_hf, tchi_raw, U, lvec, lambda_p, lambda_d, porbs, dorbs, mvec=None, hhw=None):
+    """calculate_all.F90:126-420: prefactor, tchiorbiikl, disturbances(7, site), torques(3, 3, site),
+    Beff_cart(4, site) and their site sums.  lvec[i] = L (3, nOrb, nOrb) of site i (lpvec at
+    theta = phi = 0); porbs/dorbs = local p / d orbital indices per site."""
+    nat = system.n_atoms
+    D = system.dimens
+    sidx = system.sigmaimunu2i()
+    prefactor = np.linalg.inv(np.eye(D) + chi_hf @ U)
+    T = prefactor @ tchi_raw
+    chiorb = prefactor @ chi_hf
+
+    def s2i(sig, i):
+        return (sig - 1) * nat + i
+
+    chiinv = np.zeros((4 * nat, 4 * nat), dtype=complex)
+    for i in range(nat):
+        for j in range(nat):
+            for sig in range(1, 5):
+                for sigp in range(1, 5):
+                    for mu in range(system.norbs[i]):
+                        for nu in range(system.norbs[j]):
+                            chiinv[s2i(sig, i), s2i(sigp, j)] += chiorb[sidx[sig - 1, i, mu, mu], sidx[sigp - 1, j, nu, nu]]
+    chiinv = np.linalg.inv(chiinv)
+    dist = np.zeros((7, nat), dtype=complex)
+    torq = np.zeros((3, 3, nat), dtype=complex)
+    sdmat = np.zeros(4 * nat, dtype=complex)
+
+    def tt(sig, i, mu, nu, col):
+        return T[sidx[sig - 1, i, mu, nu], col - 1]
+
+    for i in range(nat):
+        for mu in range(system.norbs[i]):
+            dist[0, i] += tt(2, i, mu, mu, 2) + tt(2, i, mu, mu, 3) + tt(3, i, mu, mu, 2) + tt(3, i, mu, mu, 3)
+            dist[1, i] += tt(1, i, mu, mu, 2) + tt(1, i, mu, mu, 3) + tt(4, i, mu, mu, 2) + tt(4, i, mu, mu, 3)
+            dist[2, i] += (tt(1, i, mu, mu, 2) + tt(1, i, mu, mu, 3) - tt(4, i, mu, mu, 2) - tt(4, i, mu, mu, 3)) / 1j
+            dist[3, i] += tt(2, i, mu, mu, 2) + tt(2, i, mu, mu, 3) - tt(3, i, mu, mu, 2) - tt(3, i, mu, mu, 3)
+        sdmat[s2i(1, i)] = dist[1, i] + 1j * dist[2, i]
+        sdmat[s2i(2, i)] = dist[0, i] + dist[3, i]
+        sdmat[s2i(3, i)] = dist[0, i] - dist[3, i]
+        sdmat[s2i(4, i)] = dist[1, i] - 1j * dist[2, i]
+        n = system.norbs[i]
+        for mu in range(n):
+            for nu in range(n):
+                ld = tt(2, i, mu, nu, 2) + tt(2, i, mu, nu, 3) + tt(3, i, mu, nu, 2) + tt(3, i, mu, nu, 3)
+                for c in range(3):
+                    dist[4 + c, i] += lvec[i][c, mu, nu] * ld
+        for lam, orbl in ((lambda_p, porbs[i]), (lambda_d, dorbs[i])):
+            for nu in orbl:
+                for mu in orbl:
+                    lp = lvec[i][:, mu, nu]
+                    a = tt(2, i, mu, nu, 2) + tt(2, i, mu, nu, 3) - tt(3, i, mu, nu, 2) - tt(3, i, mu, nu, 3)
+                    b = tt(1, i, mu, nu, 2) + tt(1, i, mu, nu, 3) - tt(4, i, mu, nu, 2) - tt(4, i, mu, nu, 3)
+                    c = tt(1, i, mu, nu, 2) + tt(1, i, mu, nu, 3) + tt(4, i, mu, nu, 2) + tt(4, i, mu, nu, 3)
+                    torq[0, 0, i] += lam * (lp[1] * a) + lam * (1j * lp[2] * b)
+                    torq[0, 1, i] += lam * (lp[2] * c) - lam * (lp[0] * a)
+                    torq[0, 2, i] += -lam * (1j * lp[0] * b) - lam * (lp[1] * c)
+        torq[0, :, i] *= 0.5
+        um = system.Um()[i]
+        m = np.zeros(3) if mvec is None else mvec[i]
+        torq[1, 0, i] = um * (m[2] * dist[2, i] - m[1] * dist[3, i])
+        torq[1, 1, i] = um * (m[0] * dist[3, i] - m[2] * dist[1, i])
+        torq[1, 2, i] = um * (m[1] * dist[1, i] - m[0] * dist[2, i])
+        if hhw is not None:
+            h = hhw[i]
+            torq[2, 0, i] = 2 * (h[1] * dist[3, i] - h[2] * dist[2, i])
+            torq[2, 1, i] = 2 * (h[2] * dist[1, i] - h[0] * dist[3, i])
+            torq[2, 2, i] = 2 * (h[0] * dist[2, i] - h[1] * dist[1, i])
+    dist[1:4] *= 0.5
+    sdmat *= 0.5
+    beff = chiinv @ sdmat
+    bc = np.zeros((4, nat), dtype=complex)
+    for i in range(nat):
+        bc[0, i] = beff[s2i(2, i)] + beff[s2i(3, i)]
+        bc[1, i] = 0.5 * (beff[s2i(1, i)] + beff[s2i(4, i)])
+        bc[2, i] = -0.5j * (beff[s2i(1, i)] - beff[s2i(4, i)])
+        bc[3, i] = 0.5 * (beff[s2i(2, i)] - beff[s2i(3, i)])
+    return {"tchiorbiikl": T, "disturbances": dist, "torques": torq, "beff": bc,
+            "total_disturbances": dist.sum(axis=1), "total_torques": torq.sum(axis=2), "total_beff": bc.sum(axis=1)}

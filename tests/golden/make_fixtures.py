@@ -60,6 +60,13 @@ def main(ref_root: str) -> None:
                                     os.path.join(dst, f"chihf_{i}_{j}.dat"))
                     shutil.copyfile(os.path.join(base, "10Sites", "RPA", f"chi_{i}_{j}_" + NANO_SUFFIX),
                                     os.path.join(dst, f"chi_{i}_{j}.dat"))
+            # calculate_all responses: disturbances, torques and effective fields per site and total
+            for folder in ("SD", "CD", "LD", "SOT", "Beff"):
+                src_dir = os.path.join(base, "10Sites", folder)
+                os.makedirs(os.path.join(dst, "resp"), exist_ok=True)
+                for f in sorted(os.listdir(src_dir)):
+                    short = f.split("_parts=")[0] + ".dat"
+                    shutil.copyfile(os.path.join(src_dir, f), os.path.join(dst, "resp", short))
         # the graphene self-consistency file has a run-dependent name
         if ex == "graphene":
             sc_dir = os.path.join(ref_root, "examples", ex, "results_correct", "FSOC", "selfconsistency")

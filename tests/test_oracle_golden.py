@@ -13,6 +13,7 @@ import pytest
 
 from oracle import compare_output as C
 from oracle import titan_oracle as O
+from golden_resp import check_responses
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -88,14 +89,24 @@ def _golden_rows(name, kind, i, j):
     return [[float(x) for x in l.split()] for l in open(f) if not l.strip().startswith("#")]
 
 
+_NR_CHI = {}
+
+
+def _nanoribbon_chi():
+    from oracle_pool import chi_parallel
+    if "chi" not in _NR_CHI:
+        _NR_CHI["chi"] = chi_parallel("nanoribbon")
+    return _NR_CHI["chi"]
+
+
 def test_nanoribbon_chi_matches_golden():
     """10-site px/py nanoribbon (100 site pairs): chi_HF and chi_RPA at omega = 1e-6
     against the reference's results_correct files (CI TOL 1e-7, here 1e-8)."""
-    from oracle_pool import _load, chi_parallel
+    from oracle_pool import _load
     d, st = _load("nanoribbon")
     s = d.system
     e = float(d.frequencies()[0])
-    chi = chi_parallel("nanoribbon")
+    chi = _nanoribbon_chi()
     schi = O.site_reduce(s, chi)
     rpa = O.site_reduce(s, O.dyson(chi, O.umatrix(s)))
     for i in range(1, s.n_atoms + 1):
@@ -106,3 +117,26 @@ def test_nanoribbon_chi_matches_golden():
                 for a, b in zip(r, g):
                     if abs(b) > 1e-6:
                         assert abs(a - b) <= 1e-8 * abs(b), (kind, i, j, a, b)
+
+
+def test_nanoribbon_disturbances_match_golden():
+    """eintshe + calculate_all on the nanoribbon with E along x: charge, spin and orbital
+    disturbances, torques and effective fields of every site and their sums against the
+    reference's results_correct files (10 significant digits; here 1e-8 of the largest site value)."""
+    from oracle_pool import _load, she_parallel
+    from titan_b200.host import response as R
+    d, st = _load("nanoribbon")
+    s = d.system
+    chi = _nanoribbon_chi()
+    tchi = she_parallel("nanoribbon")
+    U = O.umatrix(s)
+    lvec, lpvec, lam_p, lam_d, porbs, dorbs, Um = R.site_parameters(s)
+    out = O.disturbance_outputs(s, chi, tchi, U, lvec, lam_p[0], lam_d[0], porbs, dorbs)
+    check_responses("nanoribbon", out, s.n_atoms)
+    # the host post-processing agrees with the oracle's restatement on the same integral
+    pref = R.prefactor(chi, U)
+    host = R.responses(s, pref @ tchi, pref @ chi, lvec, lpvec, lam_p, lam_d, porbs, dorbs, Um)
+    for key in ("disturbances", "torques", "beff"):
+        scale = np.abs(out[key]).max()
+        assert np.abs(host[key] - out[key]).max() <= 1e-12 * scale, key
+    np.testing.assert_allclose(out["tchiorbiikl"], pref @ tchi, rtol=0, atol=1e-14 * np.abs(tchi).max())

@@ -15,7 +15,7 @@ import numpy as np
 
 from . import lattice as L
 from . import mesh as M
-from .system import TBSystem, build_system, params_from_input, read_input
+from .system import TBSystem, build_system, electric_field_vector, params_from_input, read_input
 
 
 @dataclass
@@ -35,6 +35,7 @@ class Deck:
         basis = L.read_basis(os.path.join(d, "basis"))
         elements = {nm: os.path.join(d, nm) for nm in basis.type_names}
         sysm = build_system(basis, elements, p)
+        p["efield"] = electric_field_vector(inp, sysm.a1, sysm.a2, sysm.a3)
         return cls.from_system(sysm, p, mesh)
 
     @classmethod

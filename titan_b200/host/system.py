@@ -213,6 +213,24 @@ def build_system(basis: L.Basis, element_paths: dict, params: dict) -> TBSystem:
                     neighbors, t0i, Ef, eta, etap)
 
 
+def electric_field_vector(inp: dict, a1, a2, a3) -> np.ndarray:
+    """ElectricFieldVector of a deck, unit length (mod_io.F90:296-325,
+    ElectricField.F90:16-54): ebasis cartesian (3 components), bravais (2 integer
+    coefficients of a1, a2) or spherical (theta, phi in degrees, the default)."""
+    basis = inp.get("ebasis", "spherical").strip().lower()
+    v = [_fnum(x) for x in inp.get("dirEfield", "90 0").split()]
+    if basis == "cartesian":
+        e = np.array(v[:3], float)
+    elif basis == "bravais":
+        e = v[0] * np.asarray(a1, float) + v[1] * np.asarray(a2, float)
+    elif basis == "spherical":
+        t, ph = math.radians(v[0]), math.radians(v[1])
+        e = np.array([math.cos(ph) * math.sin(t), math.sin(ph) * math.sin(t), math.cos(t)])
+    else:
+        raise ValueError(f"ebasis = {basis}: field along atom directions is not implemented (as in the reference)")
+    return e / np.linalg.norm(e)
+
+
 def params_from_input(inp: dict) -> dict:
     """Translate a parsed reference input deck into build/mesh parameters (mod_io.F90:85-140)."""
     p = {}
