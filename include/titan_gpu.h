@@ -158,6 +158,20 @@ int tg_system_shape(const tg_ctx* ctx, int* n_atoms, int* norb_max, int* norb);
  * (calculate_chi.F90:85-89).  All matrices (dimens, dimens) complex. */
 int tg_dyson(tg_ctx* ctx, int dimens, const double* chi_hf, const double* umat, double* chi);
 
+/* Disturbance response to an electric field: replaces eintshe(q, e)
+ * (source/eintshe.F90:2-309) for one frequency e.
+ *   tchi(dimens, 4) complex = prefactor . (1/2pi) sum_{k,E} w df1iikl(k, E)
+ * with df1iikl the vertex sandwich of G(k + q, E + e), dtdk(k) (dtdksub.F90:2-28,
+ * efield(3) the unit field vector u of ElectricFieldVector) and G(k, E) on the
+ * diagonal site blocks, summed over the imaginary-axis mesh of tg_set_imag_mesh and,
+ * when |e| >= 1e-15, over n_real real-axis energies x2/p2 (generate_real_epoints)
+ * times the real-axis BZ of tg_set_real_mesh.  prefactor(dimens, dimens) complex is
+ * the reference's (1 + chi_hf U)^-1 (calculate_all.F90:117-120); null = identity,
+ * which returns the bare integral.  Row order of tchi: sigmaimunu2i. */
+int tg_she(tg_ctx* ctx, const double* q, double e, double Ef, double eta, double etap, int n_real,
+           const double* x2, const double* p2, const double* efield, const double* prefactor,
+           int dimens, double* tchi);
+
 /* Test hooks.  G(dimH, dimH, nz) = (z - h0 - H(k))^-1 for nz (k, z) pairs,
  * and H(dimH, dimH, nk) = h0 + calchk(k). */
 int tg_green_batch(tg_ctx* ctx, int64_t nz, const double* z, const double* kp, double* G);

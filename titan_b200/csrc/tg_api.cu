@@ -114,6 +114,9 @@ struct tg_ctx {
   int64_t launches = 0;   // kernels launched by the last chi0 call
   int64_t pass_points = 0;     // points per pass (bounded workspace)
   int gg_blocks = 0, gg_nrow = 0, gg_ncol = 0, gg_mode = -1;
+  // disturbance response (eintshe)
+  DevArray<int> d_she_tab, d_ia;
+  DevArray<double2> d_she_part, d_she_sum, d_she_pref, d_she_out;
 };
 
 namespace {
@@ -1210,6 +1213,185 @@ int tg_dyson(tg_ctx* c, int dimens, const double* chi_hf, const double* umat, do
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// tg_she: disturbance response to an electric field (eintshe.F90:2-309)
+// ---------------------------------------------------------------------------
+namespace {
+
+// (sigma, sigma') -> spin blocks (X, Y, Z, W) of the imaginary-axis integrand
+//   G1^X V G2^Y + conj(G2^Z) V^T conj(G1^W)          (eintshe.F90:104-179)
+// 'u' = up, 'd' = down; the first letter is the row spin.  sigma-major order.
+const char* const kSheImag[16][4] = {
+    {"dd", "uu", "uu", "dd"}, {"du", "uu", "uu", "ud"}, {"dd", "du", "ud", "dd"}, {"du", "du", "ud", "ud"},
+    {"ud", "uu", "uu", "du"}, {"uu", "uu", "uu", "uu"}, {"ud", "du", "ud", "du"}, {"uu", "du", "ud", "uu"},
+    {"dd", "ud", "du", "dd"}, {"du", "ud", "du", "ud"}, {"dd", "dd", "dd", "dd"}, {"du", "dd", "dd", "ud"},
+    {"ud", "ud", "du", "du"}, {"uu", "ud", "du", "uu"}, {"ud", "dd", "dd", "du"}, {"uu", "dd", "dd", "uu"}};
+// (sigma, sigma') -> (X, X', Y) of the real-axis integrand
+//   -i (G1^X - (G1^{X'})^+) V (G2^Y)^+               (eintshe.F90:226-249)
+// X' is always X with its two spins exchanged, so the first factor is the
+// X block of G1 - G1^+.
+const char* const kSheReal[16][3] = {
+    {"dd", "dd", "uu"}, {"du", "ud", "uu"}, {"dd", "dd", "ud"}, {"du", "ud", "ud"},
+    {"ud", "du", "uu"}, {"uu", "uu", "uu"}, {"ud", "du", "ud"}, {"uu", "uu", "ud"},
+    {"dd", "dd", "du"}, {"du", "ud", "du"}, {"dd", "dd", "dd"}, {"du", "ud", "dd"},
+    {"ud", "du", "du"}, {"uu", "uu", "du"}, {"ud", "du", "dd"}, {"uu", "uu", "dd"}};
+
+int spin_bit(char x) { return x == 'd' ? 1 : 0; }
+unsigned char spin_code(char a, char b, char c, char d) {
+  return (unsigned char)(spin_bit(a) << 3 | spin_bit(b) << 2 | spin_bit(c) << 1 | spin_bit(d));
+}
+
+// kernel spin codes (outer row spin, inner spin of L, inner spin of R, outer column spin)
+void she_spin_codes(unsigned char spins[3][16]) {
+  for (int t = 0; t < 16; ++t) {
+    const char *X = kSheImag[t][0], *Y = kSheImag[t][1], *Z = kSheImag[t][2], *W = kSheImag[t][3];
+    spins[0][t] = spin_code(X[0], X[1], Y[0], Y[1]);
+    spins[1][t] = spin_code(Z[0], Z[1], W[0], W[1]);
+    const char *XR = kSheReal[t][0], *YR = kSheReal[t][2];
+    spins[2][t] = spin_code(XR[0], XR[1], YR[1], YR[0]);
+  }
+}
+
+}  // namespace
+
+extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double eta, double etap, int n_real,
+                      const double* x2, const double* p2, const double* efield, const double* prefactor, int dimens,
+                      double* tchi) {
+  int rc = check_ready(c, true, false);
+  if (rc) return rc;
+  if (!q || !efield || !tchi) return set_err(c, TG_ERR_ARG, "tg_she: null argument");
+  if (dimens != c->dimens) return set_err(c, TG_ERR_ARG, "tg_she: dimens mismatch");
+  const bool real = std::fabs(e) >= 1e-15;
+  if (real && (n_real <= 0 || !x2 || !p2)) return set_err(c, TG_ERR_ARG, "tg_she: real-axis points missing");
+  if (real && !c->real_set) return set_err(c, TG_ERR_STATE, "tg_set_real_mesh has not been called");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int n = c->dimH, no = n / 2, D = c->dimens;
+  const int64_t nn = (int64_t)n * n;
+  const int grid = she_grid(n, D, c->n_neigh, c->num_sms);
+  if (grid <= 0) return set_err(c, TG_ERR_ARG, "tg_she: dimH / dimens too large for the shared-memory vertex kernel");
+  // orbital tables of the kernel
+  std::vector<int> tab((size_t)4 * no);
+  {
+    int o = 0;
+    for (int i = 0; i < c->n_atoms; ++i)
+      for (int m = 0; m < c->norb[i]; ++m, ++o) {
+        tab[o] = c->ia[i] + m;
+        tab[no + o] = c->ia[i] + c->norb[i] + m;
+        tab[2 * no + o] = i;
+        tab[3 * no + o] = m;
+      }
+  }
+  TG_CHECK(c, c->d_she_tab.upload(tab.data(), tab.size(), s), "upload tables");
+  TG_CHECK(c, c->d_ia.upload(c->ia.data(), c->ia.size(), s), "upload ia");
+  TG_CHECK(c, c->d_she_part.ensure((size_t)grid * 4 * D), "alloc partials");
+  TG_CHECK(c, c->d_she_sum.ensure((size_t)4 * D), "alloc");
+  TG_CHECK(c, c->d_she_out.ensure((size_t)4 * D), "alloc");
+  TG_CHECK(c, cudaMemsetAsync(c->d_she_part.p, 0, sizeof(double2) * grid * 4 * D, s), "memset");
+  if (prefactor) TG_CHECK(c, c->d_she_pref.upload(reinterpret_cast<const double2*>(prefactor), (size_t)D * D, s), "upload");
+  const int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, real ? (int64_t)n_real * c->n_realk : 0));
+  TG_CHECK(c, c->d_A.ensure((size_t)P * nn), "alloc G1");
+  TG_CHECK(c, c->d_B.ensure((size_t)P * nn), "alloc G2");
+  if (real) {
+    TG_CHECK(c, c->d_x2.upload(x2, n_real, s), "upload x2");
+    TG_CHECK(c, c->d_p2.upload(p2, n_real, s), "upload p2");
+  }
+  rc = reset_status(c);
+  if (rc) return rc;
+  profile_begin(c);
+  TG_CHECK(c, cudaEventRecord(c->ev[0], s), "event");
+  GreenArgs base = base_args(c);
+  SheLaunch l;
+  l.g = &base;
+  l.dimens = D;
+  l.tab = c->d_she_tab.p;
+  l.ia = c->d_ia.p;
+  l.norb = c->d_norb.p;
+  l.decode = c->d_decode.p;
+  for (int i = 0; i < 3; ++i) l.ue[i] = efield[i];
+  she_spin_codes(l.spins);
+  l.partial = c->d_she_part.p;
+  l.grid = grid;
+  auto pass = [&](GreenArgs g, int real_axis) -> int {
+    // G2 = G(k, E), G1 = G(k + q, E + e), both column-major per point
+    g.mode = MODE_RAW;
+    g.out = c->d_B.p;
+    {
+      KindTimer kt(c, 0);
+      TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), "green (G2)");
+    }
+    g.zr += e;
+    g.zi = eta;
+    g.q[0] = q[0];
+    g.q[1] = q[1];
+    g.q[2] = q[2];
+    g.out = c->d_A.p;
+    {
+      KindTimer kt(c, 0);
+      TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), "green (G1)");
+    }
+    l.G1 = c->d_A.p;
+    l.G2 = c->d_B.p;
+    l.p0 = g.p0;
+    l.np = g.np;
+    l.pts = g.pts;
+    l.real_axis = real_axis;
+    {
+      KindTimer kt(c, 1);
+      c->launches += 1;
+      TG_CHECK(c, launch_she(l, s), "disturbance vertex");
+    }
+    return TG_OK;
+  };
+  for (int64_t p0 = 0; p0 < c->n_imag; p0 += P) {
+    GreenArgs g = base;
+    g.pts.kind = 0;
+    g.pts.y = c->d_y.p;
+    g.pts.kp = c->d_kp.p;
+    g.pts.w = c->d_w.p;
+    g.p0 = p0;
+    g.np = std::min<int64_t>(P, c->n_imag - p0);
+    g.zr = Ef;
+    g.zi = etap;
+    if ((rc = pass(g, 0))) return rc;
+  }
+  if (real) {
+    const int64_t ntot = (int64_t)n_real * c->n_realk;
+    for (int64_t p0 = 0; p0 < ntot; p0 += P) {
+      GreenArgs g = base;
+      g.pts.kind = 1;
+      g.pts.kp = c->d_rkp.p;
+      g.pts.w = c->d_rw.p;
+      g.pts.x2 = c->d_x2.p;
+      g.pts.p2 = c->d_p2.p;
+      g.pts.nk = c->n_realk;
+      g.p0 = p0;
+      g.np = std::min<int64_t>(P, ntot - p0);
+      g.zr = 0.0;
+      g.zi = etap;
+      if ((rc = pass(g, 1))) return rc;
+    }
+  }
+  {
+    KindTimer kt(c, 2);
+    TG_CHECK(c, launch_reduce_blocks(c->d_she_part.p, grid, 4 * D, c->d_she_sum.p, s), "reduce");
+  }
+  {
+    KindTimer kt(c, 2);
+    TG_CHECK(c, launch_she_prefactor(prefactor ? c->d_she_pref.p : nullptr, c->d_she_sum.p, D, 1.0 / (2.0 * kPi),
+                                     c->d_she_out.p, s),
+             "prefactor");
+  }
+  TG_CHECK(c, cudaMemcpyAsync(tchi, c->d_she_out.p, sizeof(double2) * 4 * D, cudaMemcpyDeviceToHost, s), "copy");
+  TG_CHECK(c, cudaEventRecord(c->ev[6], s), "event");
+  TG_CHECK(c, cudaEventSynchronize(c->ev[6]), "sync");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev[0], c->ev[6]);
+  c->last_ms[3] = ms;
+  profile_end(c);
+  return read_status(c);
+}
 
 // ---------------------------------------------------------------------------
 // tg_expectation_noalloc: occupations and moments without device allocation.

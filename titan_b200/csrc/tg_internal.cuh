@@ -162,4 +162,29 @@ cudaError_t launch_hk_table(const GreenArgs& a, const double* kp, int64_t nk, co
                             double2* H, cudaStream_t s);
 cudaError_t launch_reduce_blocks(const double2* part, int nblocks, int len, double2* out, cudaStream_t s);
 
+// Disturbance-response vertex (eintshe): one launch per pass over RAW G1 / G2
+struct SheLaunch {
+  const GreenArgs* g = nullptr;   // system tables (n, neighbours, hopping blocks)
+  const double2* G1 = nullptr;
+  const double2* G2 = nullptr;
+  int64_t p0 = 0, np = 0;
+  PointSet pts;
+  int real_axis = 0;
+  int dimens = 0;
+  const int* tab = nullptr;       // [4][n / 2]
+  const int* ia = nullptr;
+  const int* norb = nullptr;
+  const int* decode = nullptr;
+  double ue[3] = {0, 0, 0};
+  unsigned char spins[3][16] = {};
+  double2* partial = nullptr;     // [grid][4 dimens]
+  int grid = 0;
+};
+size_t she_smem_bytes(int n, int dimens, int n_neigh);
+// CTAs of one vertex launch (SMs x resident CTAs); 0 when the shared memory does not fit
+int she_grid(int n, int dimens, int n_neigh, int num_sms);
+cudaError_t launch_she(const SheLaunch& l, cudaStream_t s);
+cudaError_t launch_she_prefactor(const double2* P, const double2* df, int dimens, double scale, double2* out,
+                                 cudaStream_t s);
+
 }  // namespace tg

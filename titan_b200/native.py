@@ -44,6 +44,8 @@ SIGNATURES = {
     "tg_gg_tensor": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int, _ip, _dp]),
     "tg_fermi_column": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
     "tg_dyson": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),
+    "tg_she": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp,
+                         _dp, C.c_int, _dp]),
     "tg_green_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp]),
     "tg_hamiltk_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp]),
     "tg_last_timing": (C.c_int, [C.c_void_p, _dp]),
@@ -230,6 +232,22 @@ class GreenGPU:
                                     _PREC[precision], D, _p(buf.view(np.float64)))
         self._check(rc)
         return np.swapaxes(buf, 1, 2)      # Fortran (row, col) -> numpy [row, col]
+
+    def she(self, q, e, Ef, eta, etap, x2, p2, efield, prefactor=None):
+        """tchiorbiikl(q, e) as a [dimens, 4] numpy array (eintshe): prefactor . (1/2 pi) sum w df1iikl;
+        prefactor None gives the bare integral."""
+        qa = np.ascontiguousarray(q, np.float64)
+        ue = np.ascontiguousarray(efield, np.float64)
+        x2 = np.ascontiguousarray(x2 if x2 is not None else np.zeros(0), np.float64)
+        p2 = np.ascontiguousarray(p2 if p2 is not None else np.zeros(0), np.float64)
+        D = self.dimens
+        pref = None if prefactor is None else _fortran_complex(prefactor)
+        out = np.zeros((4, D), np.complex128)      # Fortran (dimens, 4)
+        rc = self.lib.tg_she(self.h, _p(qa), e, Ef, eta, etap, x2.shape[0], _p(x2) if x2.shape[0] else None,
+                             _p(p2) if p2.shape[0] else None, _p(ue),
+                             None if pref is None else _p(pref.view(np.float64)), D, _p(out.view(np.float64)))
+        self._check(rc)
+        return out.T
 
     def last_timing(self):
         """Device ms of the last chi0 call (see tg_last_timing)."""
