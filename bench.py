@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--compare-fp64", action="store_true", help="also time the FP64 path and report the ratio")
+    ap.add_argument("--workload", default="chi0", choices=["chi0", "she"],
+                    help="chi0: the susceptibility integral (headline); she: the disturbance integral "
+                         "(eintshe) of the same mesh, one frequency per step")
     ap.add_argument("--small", action="store_true",
                     help="30 x 30 k mesh, 64 + 16 energies: a few-second case for profiler captures")
     return ap.parse_args()
@@ -346,6 +349,119 @@ def run_e2e(gpu, deck, h0, omegas, reals, args, start, per, world):
             "d2h_bytes_per_step": int(out.nbytes), "timer": "host wall clock around the public API calls"}
 
 
+# --------------------------------------------------------------------------- disturbance integral
+SHE_METRIC = "eintshe disturbance integral (k,E)-points/s on 1 B200 (FP64)"
+SHE_UE = (1.0, 0.0, 0.0)
+
+
+def she_vertex_flops(s, real_axis):
+    """Algorithmic FP64 flops of the vertex sandwiches of one point: per term Y^b = L V
+    (2 n no^2 complex FMA) and the 4 dimens output entries (no complex FMA each); two terms
+    on the imaginary axis, one on the real axis; 8 flops per complex FMA."""
+    n, no = s.dimH, s.dimH // 2
+    per_term = 8.0 * (2 * n * no * no + 4 * s.dimens * no)
+    return per_term * (1 if real_axis else 2)
+
+
+def she_cpu_baseline(deck, h0, reals, omegas, seconds_target=15.0):
+    """The oracle's eintshe (numpy, all host threads) on a bounded sample of the workload."""
+    from oracle import titan_oracle as O
+    from titan_b200.host.mesh import EKMesh
+    s = deck.system
+    m = O.Model(s, h0)
+    w_idx = 1 if len(omegas) > 1 else 0
+    e = float(omegas[w_idx])
+    x2, p2 = reals[w_idx]
+    ek = deck.ek
+
+    def run(n_imag_s, nk_s):
+        sub = EKMesh(ek.y, ek.wght, ek.energy_index[:n_imag_s], ek.kp[:n_imag_s], ek.weight[:n_imag_s])
+        rk = (deck.real_kp[:max(nk_s, 1)], deck.real_w[:max(nk_s, 1)])
+        t0 = time.perf_counter()
+        O.eintshe(m, sub, rk, np.zeros(3), e, s.Ef, s.eta, s.etap, x2 if nk_s else None, p2 if nk_s else None,
+                  SHE_UE)
+        return time.perf_counter() - t0
+
+    cal = min(100, ek.n_points)
+    rate = cal / max(run(cal, 0), 1e-6)
+    n_imag_s = int(min(ek.n_points, max(200, rate * seconds_target * 2 / 3)))
+    nk_s = int(min(deck.real_kp.shape[0], max(1, rate * seconds_target / 3 / max(len(x2), 1)))) if len(x2) else 0
+    dt = run(n_imag_s, nk_s)
+    units = n_imag_s + len(x2) * nk_s
+    cores = os.cpu_count()
+    return {"value": units / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle eintshe (numpy, {cores} threads) on {n_imag_s} imaginary-axis points + "
+                      f"{len(x2)} real-axis energies x {nk_s} k of the {deck.system.name} workload at omega={e:.4g} "
+                      f"({units} units, {dt:.1f} s)"}
+
+
+def run_she(args, rank, world, local_rank):
+    """One tg_she call per step (one frequency, q = 0, E along x), frequencies walked per rank."""
+    import torch
+    from titan_b200.native import GreenGPU
+    torch.cuda.set_device(local_rank)
+    deck, h0, omegas, reals = workload(args.config, args.small)
+    s = deck.system
+    gpu = GreenGPU(local_rank)
+    gpu.setup(deck, h0)
+    gpu.profile(True)
+    n_om = len(omegas)
+    start = 1 + rank * (args.steps + args.warmup)   # omega_0 = 0 has no real axis; start at omega_1
+
+    def steps(k, first):
+        ms, units, launches, vert = [], 0, 0, 0.0
+        flops = 0.0
+        for st in range(k):
+            i = (first + st) % n_om
+            if i == 0:
+                i = 1
+            x2, p2 = reals[i]
+            gpu.she(np.zeros(3), float(omegas[i]), s.Ef, s.eta, s.etap, x2, p2, SHE_UE)
+            t = gpu.last_timing()
+            ms.append(t[3])
+            launches += int(t[10])
+            vert = (t[6], t[7])
+            nreal = len(x2) * deck.real_kp.shape[0]
+            units += deck.ek.n_points + nreal
+            flops = she_vertex_flops(s, False) * deck.ek.n_points + she_vertex_flops(s, True) * nreal
+        return ms, units, launches, vert, flops, t
+
+    steps(args.warmup, start)
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local_rank)
+    clk.start()
+    ms, units, launches, vert, flops_last, last = steps(args.steps, start + args.warmup)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier(world)
+    total_ms_max = allreduce_max(sum(ms), world)
+    value = allreduce_sum(units, world) / (total_ms_max / 1e3)
+    v_ms, v_n = vert
+    fp64_nominal = 37.0
+    achieved = flops_last / (v_ms / 1e3) / 1e12 if v_ms else None
+    roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_nominal, "unit": "TFLOP/s",
+            "frac": achieved / fp64_nominal if achieved else None, "traffic": None,
+            "peak_source": "nominal B200 FP64 (not measured)", "kernel": "she_kernel (vertex sandwiches)",
+            "flops_per_unit": {"imag": she_vertex_flops(s, False), "real": she_vertex_flops(s, True)},
+            "launches_in_last_step": int(v_n), "ms_last_step": v_ms,
+            "inversion_ms_last_step": last[4], "reduce_prefactor_ms_last_step": last[8]}
+    line = {"metric": SHE_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Slater-Koster model, no external data)",
+            "config": {"workload": f"{args.config}: dimH={s.dimH}, dimens={s.dimens}, {deck.ek.n_points} imag (E,k) "
+                                   f"points + {deck.real_kp.shape[0]} real-axis k x 64 energies per omega, q=0, "
+                                   f"E along x, one omega per step",
+                       "l2": "inputs larger than L2 (G1/G2 buffers GBs per pass)"},
+            "roofline": roof, "gpu_launches": launches, "clocks": clocks}
+    if rank == 0 and not args.no_cpu and world == 1:
+        line["cpu_baseline"] = she_cpu_baseline(deck, h0, reals, omegas)
+    gpu.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # --------------------------------------------------------------------------- distributed helpers
 def barrier(world):
     if world > 1:
@@ -389,7 +505,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload == "she":
+            run_she(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
