@@ -30,6 +30,7 @@ extern "C" {
 #define TG_ERR_STATE    (-3)   /* call order: system / h0 / mesh not set */
 #define TG_ERR_TIMEOUT  (-4)   /* a bounded device wait gave up */
 #define TG_ERR_NOMEM    (-5)   /* device allocation failed */
+#define TG_ERR_NUMERIC  (-6)   /* an iterative device solver did not converge */
 
 /* Precision of the chi0 contraction (tg_chi0). */
 #define TG_PREC_FP64     0     /* FP64 SIMT contraction */
@@ -171,6 +172,23 @@ int tg_dyson(tg_ctx* ctx, int dimens, const double* chi_hf, const double* umat, 
 int tg_she(tg_ctx* ctx, const double* q, double e, double Ef, double eta, double etap, int n_real,
            const double* x2, const double* p2, const double* efield, const double* prefactor,
            int dimens, double* tchi);
+
+/* How G(k, z) is computed.  TG_GREEN_AUTO (default): on meshes where every energy
+ * uses the same k list (uniform imaginary axis, the real-axis BZ) H(k) is
+ * diagonalised once per k (Jacobi, FP64) and G(k, z) = U diag(1/(z - lambda)) U^+
+ * is formed for all energies with FP64 tensor-core GEMMs; other meshes and
+ * dimensions use Gauss-Jordan.  TG_GREEN_GAUSS_JORDAN: Gauss-Jordan everywhere
+ * (the reference's invers, mod_tools.F90:796-829, per point).  No counterpart in
+ * the reference; both agree to roundoff. */
+#define TG_GREEN_AUTO          0
+#define TG_GREEN_GAUSS_JORDAN  1
+int tg_set_green_method(tg_ctx* ctx, int method);
+
+/* Test hook: eigenvalues lam(dimH, nk) and eigenvectors of h0 + H(k) from the Jacobi
+ * kernel behind TG_GREEN_AUTO, U(dimH, dimH, nk) with U(a, :, k) = eigenvector a (the
+ * device's row-major [k][r][a] layout); TG_ERR_NUMERIC if a matrix did not converge in
+ * 30 sweeps. */
+int tg_eig_batch(tg_ctx* ctx, int64_t nk, const double* kp, double* lam, double* U);
 
 /* Test hooks.  G(dimH, dimH, nz) = (z - h0 - H(k))^-1 for nz (k, z) pairs,
  * and H(dimH, dimH, nk) = h0 + calchk(k). */

@@ -266,3 +266,48 @@ def test_nanoribbon_golden_through_gpu(gpu, precision):
                 for a, b in zip(r, g):
                     if abs(b) > 1e-6:
                         assert abs(a - b) <= 1e-8 * abs(b), (kind, i, j, a, b)
+
+
+@pytest.mark.parametrize("shape", ["bcc1", "sq2", "bcc4"])
+def test_eig_batch_matches_eigh(gpu, shape):
+    """Jacobi eigendecomposition of H(k) behind the spectral Green functions."""
+    deck = synthetic.make_deck(shape, mesh=False)
+    s = deck.system
+    h0 = s.h0(initial_state(s))
+    gpu.set_system(s)
+    gpu.set_h0(h0)
+    kp = np.random.default_rng(3).uniform(-2, 2, size=(25, 3))
+    lam, U = gpu.eig_batch(kp)
+    H = O.Model(s, h0).hk(kp)
+    for k in range(kp.shape[0]):
+        ref = np.linalg.eigvalsh(H[k])
+        scale = np.max(np.abs(ref))
+        assert np.max(np.abs(np.sort(lam[k]) - ref)) < 1e-13 * scale * s.dimH
+        assert np.max(np.abs(U[k].conj().T @ U[k] - np.eye(s.dimH))) < 1e-13 * s.dimH
+        rec = U[k] @ np.diag(lam[k]) @ U[k].conj().T
+        assert np.max(np.abs(rec - H[k])) < 1e-14 * scale * s.dimH
+
+
+@pytest.mark.parametrize("shape,nk,e,q,precision", [
+    ("bcc1", (4, 4, 4), 0.0, (0, 0, 0), "fp64"),
+    ("bcc1", (3, 3, 3), 0.03, (0.1, 0.0, 0.2), "fp64"),
+    ("sq2", (5, 5, 1), 0.1, (0.05, 0.02, 0.0), "fp64"),
+    ("sq2", (5, 5, 1), 0.1, (0.0, 0.0, 0.0), "split"),
+    ("bcc4", (2, 2, 2), 0.05, (0.0, 0.1, 0.0), "fp64"),
+])
+def test_spectral_green_equals_gauss_jordan(gpu, shape, nk, e, q, precision):
+    """chi0 with G from the eigendecomposition (default on uniform meshes) and from
+    Gauss-Jordan per point agree to roundoff; both match the oracle."""
+    deck = synthetic.make_deck(shape, nk=nk, n1gl=8, parts=1, n3gl=6)
+    s, h0 = _setup(gpu, deck)
+    x2, p2 = deck.real_points(e, s.Ef)
+    q = np.array(q, float)
+    try:
+        gpu.set_green_method("gauss-jordan")
+        gj = gpu.chi0(q, e, s.Ef, s.eta, s.etap, x2, p2, precision=precision)
+    finally:
+        gpu.set_green_method("auto")
+    sp = gpu.chi0(q, e, s.Ef, s.eta, s.etap, x2, p2, precision=precision)
+    assert rel(sp, gj) < (1e-12 if precision == "fp64" else 1e-10)
+    ref = O.eintshechi(O.Model(s, h0), deck.ek, (deck.real_kp, deck.real_w), q, e, s.Ef, s.eta, s.etap, x2, p2)
+    assert rel(sp, ref) < (1e-10 if precision == "fp64" else 1e-9)

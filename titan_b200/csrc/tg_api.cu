@@ -114,6 +114,11 @@ struct tg_ctx {
   int64_t launches = 0;   // kernels launched by the last chi0 call
   int64_t pass_points = 0;     // points per pass (bounded workspace)
   int gg_blocks = 0, gg_nrow = 0, gg_ncol = 0, gg_mode = -1;
+  // spectral Green functions: eigendecomposition of each H(k) table, inverse output map
+  int green_method = 0;   // 0: spectral on tabulated meshes, 1: Gauss-Jordan everywhere
+  DevArray<double2> d_eigU[4];
+  DevArray<double> d_eigL[4];
+  DevArray<int> d_outinv, d_eig_status;
   // disturbance response (eintshe)
   DevArray<int> d_she_tab, d_ia;
   DevArray<double2> d_she_part, d_she_sum, d_she_pref, d_she_out;
@@ -263,6 +268,39 @@ int build_htab(tg_ctx* c, int slot, const double* d_k, int64_t nk, const double*
   GreenArgs a = base_args(c);
   TG_CHECK(c, launch_hk_table(a, d_k, nk, c->d_qvec.p, c->d_hphase.p, c->d_htab[slot].p, c->stream), "H table");
   c->launches += 2;
+  return TG_OK;
+}
+
+// eigendecomposition of every row of H table `slot` (spectral Green functions)
+bool spectral_on(tg_ctx* c) { return c->green_method == 0 && eig_supported(c->dimH); }
+
+int build_eig(tg_ctx* c, int slot, int64_t nk) {
+  const size_t nn = (size_t)c->dimH * c->dimH;
+  TG_CHECK(c, c->d_eigU[slot].ensure((size_t)nk * nn), "alloc eigenvectors");
+  TG_CHECK(c, c->d_eigL[slot].ensure((size_t)nk * c->dimH), "alloc eigenvalues");
+  KindTimer kt(c, 0);
+  TG_CHECK(c, launch_eig(c->d_htab[slot].p, nk, c->dimH, c->d_eigU[slot].p, c->d_eigL[slot].p, c->d_eig_status.p,
+                         c->num_sms, c->stream),
+           "eigendecomposition");
+  return TG_OK;
+}
+
+int reset_eig_status(tg_ctx* c) {
+  const int big = 0x7fffffff;
+  TG_CHECK(c, c->d_eig_status.ensure(1), "alloc");
+  TG_CHECK(c, cudaMemcpyAsync(c->d_eig_status.p, &big, sizeof(int), cudaMemcpyHostToDevice, c->stream), "status");
+  return TG_OK;
+}
+
+int read_eig_status(tg_ctx* c) {
+  int v = 0x7fffffff;
+  TG_CHECK(c, cudaMemcpyAsync(&v, c->d_eig_status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status");
+  TG_CHECK(c, cudaStreamSynchronize(c->stream), "sync");
+  if (v != 0x7fffffff) {
+    char b[128];
+    snprintf(b, sizeof b, "Jacobi eigensolver did not converge for table row %d", v - 1);
+    return set_err(c, TG_ERR_NUMERIC, b);
+  }
   return TG_OK;
 }
 
@@ -546,6 +584,11 @@ int tg_set_system(tg_ctx* c, int n_atoms, const int* norb, int norb_max, int n_n
   TG_CHECK(c, c->d_row_orb.upload(rorb.data(), n, s), "upload");
   TG_CHECK(c, c->d_row_spin.upload(rspin.data(), n, s), "upload");
   TG_CHECK(c, c->d_outmap.upload(outmap.data(), outmap.size(), s), "upload");
+  {
+    std::vector<int> outinv((size_t)n * n);
+    for (size_t o = 0; o < outmap.size(); ++o) outinv[outmap[o]] = (int)o;
+    TG_CHECK(c, c->d_outinv.upload(outinv.data(), outinv.size(), s), "upload");
+  }
   TG_CHECK(c, c->d_decode.upload(decode.data(), decode.size(), s), "upload");
   TG_CHECK(c, c->d_norb.upload(c->norb.data(), n_atoms, s), "upload");
   TG_CHECK(c, c->d_pair_M.upload(c->pair_M.data(), np2, s), "upload");
@@ -671,19 +714,30 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   const double zero3[3] = {0.0, 0.0, 0.0};
   const bool tab_imag = c->imag_uniform && (int64_t)c->nk_u * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
   const bool tab_real = any_real && (int64_t)c->n_realk * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
+  const bool spec = spectral_on(c);
+  if (spec && (rc = reset_eig_status(c))) return rc;
   if (tab_imag) {
     if ((rc = build_htab(c, 0, c->d_klist_u.p, c->nk_u, zero3))) return rc;
+    if (spec && (rc = build_eig(c, 0, c->nk_u))) return rc;
     if (!q_zero && (rc = build_htab(c, 1, c->d_klist_u.p, c->nk_u, q))) return rc;
+    if (!q_zero && spec && (rc = build_eig(c, 1, c->nk_u))) return rc;
   }
   if (tab_real) {
     if ((rc = build_htab(c, 2, c->d_rkp.p, c->n_realk, zero3))) return rc;
+    if (spec && (rc = build_eig(c, 2, c->n_realk))) return rc;
     if (!q_zero && (rc = build_htab(c, 3, c->d_rkp.p, c->n_realk, q))) return rc;
+    if (!q_zero && spec && (rc = build_eig(c, 3, c->n_realk))) return rc;
   }
   auto use_table = [&](GreenArgs& g, int slot, int64_t n_e, int64_t nk, const double* ylist) {
     g.htab = c->d_htab[slot].p;
     g.n_e = n_e;
     g.nk_tab = nk;
     g.ylist = ylist;
+    if (spec) {
+      g.eigU = c->d_eigU[slot].p;
+      g.eigL = c->d_eigL[slot].p;
+      g.outinv = c->d_outinv.p;
+    }
   };
   // ---------------- imaginary axis ----------------
   for (int64_t p0 = 0; p0 < c->n_imag; p0 += P) {
@@ -860,6 +914,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   profile_end(c);
   rc = read_status(c);
   if (rc) return rc;
+  if (spec && (rc = read_eig_status(c))) return rc;
   if (split) {
     int err = 0;
     TG_CHECK(c, cudaMemcpy(&err, c->d_split_err.p, sizeof(int), cudaMemcpyDeviceToHost), "split status");
@@ -1188,6 +1243,33 @@ int tg_hamiltk_batch(tg_ctx* c, int64_t nk, const double* kp, double* H) {
   TG_CHECK(c, cudaMemcpyAsync(H, c->d_gout.p, sizeof(double2) * nk * nn, cudaMemcpyDeviceToHost, s), "copy H");
   TG_CHECK(c, cudaStreamSynchronize(s), "sync");
   return TG_OK;
+}
+
+int tg_set_green_method(tg_ctx* c, int method) {
+  if (!c) return TG_ERR_ARG;
+  if (method != TG_GREEN_AUTO && method != TG_GREEN_GAUSS_JORDAN)
+    return set_err(c, TG_ERR_ARG, "tg_set_green_method: unknown method");
+  c->green_method = method;
+  return TG_OK;
+}
+
+int tg_eig_batch(tg_ctx* c, int64_t nk, const double* kp, double* lam, double* U) {
+  int rc = check_ready(c, false, false);
+  if (rc) return rc;
+  if (nk < 0 || (nk > 0 && (!kp || !lam || !U))) return set_err(c, TG_ERR_ARG, "tg_eig_batch: bad args");
+  if (nk == 0) return TG_OK;
+  if (!eig_supported(c->dimH)) return set_err(c, TG_ERR_ARG, "tg_eig_batch: dimH too large for the Jacobi kernel");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const double zero3[3] = {0.0, 0.0, 0.0};
+  TG_CHECK(c, c->d_klist.upload(kp, 3 * nk, s), "upload k");
+  if ((rc = build_htab(c, 0, c->d_klist.p, nk, zero3))) return rc;
+  if ((rc = reset_eig_status(c))) return rc;
+  if ((rc = build_eig(c, 0, nk))) return rc;
+  const size_t nn = (size_t)c->dimH * c->dimH;
+  TG_CHECK(c, cudaMemcpyAsync(lam, c->d_eigL[0].p, sizeof(double) * nk * c->dimH, cudaMemcpyDeviceToHost, s), "copy");
+  TG_CHECK(c, cudaMemcpyAsync(U, c->d_eigU[0].p, sizeof(double2) * nk * nn, cudaMemcpyDeviceToHost, s), "copy");
+  return read_eig_status(c);
 }
 
 int tg_dyson(tg_ctx* c, int dimens, const double* chi_hf, const double* umat, double* chi) {

@@ -133,6 +133,11 @@ struct GreenArgs {
   int64_t n_e = 0;
   int64_t nk_tab = 0;
   const double* ylist = nullptr;     // imaginary parts of the energies (structured imaginary axis)
+  // optional eigendecomposition of every table row (spectral Green functions):
+  // eigU[k][r][a] row-major, eigL[k][a]; outinv[r*n + c] = pair-block slot of (r, c)
+  const double2* eigU = nullptr;
+  const double* eigL = nullptr;
+  const int* outinv = nullptr;
 };
 
 // Launch the fused H(k) + Gauss-Jordan kernel for any supported n.
@@ -161,6 +166,15 @@ int gemm64_tile();
 cudaError_t launch_hk_table(const GreenArgs& a, const double* kp, int64_t nk, const double* d_q, double2* phase_ws,
                             double2* H, cudaStream_t s);
 cudaError_t launch_reduce_blocks(const double2* part, int nblocks, int len, double2* out, cudaStream_t s);
+
+// Spectral Green functions: Jacobi eigendecomposition of an H(k) table and G from (U, lambda)
+size_t eig_smem_bytes(int n);
+int eig_supported(int n);
+cudaError_t launch_eig(const double2* H, int64_t nk, int n, double2* U, double* lam, int* status, int num_sms,
+                       cudaStream_t s);
+int spectral_supported(int mode, int mode2, bool has_out2);
+cudaError_t launch_green_spectral(const GreenArgs& g, const double2* U, const double* lam, const int* outinv,
+                                  int num_sms, cudaStream_t s);
 
 // Disturbance-response vertex (eintshe): one launch per pass over RAW G1 / G2
 struct SheLaunch {

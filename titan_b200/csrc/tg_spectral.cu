@@ -1,0 +1,414 @@
+// Spectral Green functions on tabulated k meshes.
+//
+// When every energy of a pass uses the same k list (uniform imaginary-axis
+// meshes, the real-axis BZ), one H(k) serves every (E, k) point of that k.
+// H(k) is Hermitian, H = U diag(lambda) U^+, so for every z at once
+//   G(k, z) = (z - H(k))^-1 = U diag(1 / (z - lambda)) U^+,
+// which for a block of energies is one GEMM with K = dimH:
+//   G[z][(r, c)] = sum_a D[z][a] P[a][(r, c)],   D[z][a] = 1 / (z - lambda_a),
+//   P[a][(r, c)] = U[r][a] conj(U[c][a]).
+// The GEMM runs on the FP64 tensor cores (mma.sync m8n8k4 .f64; tcgen05 has no
+// FP64 kind); P is formed on the fly from U in shared memory.  The same form
+// gives G - G^+ with D = 2 i Im(1 / (z - lambda)).
+//
+// The eigendecomposition is a cyclic two-sided Jacobi iteration, one CTA per
+// matrix, n / 2 disjoint rotations per step in round-robin order, sweeps until
+// the off-diagonal Frobenius norm is below 1e-15 of the matrix norm (couplings
+// under 1e-16 of it are zeroed without a rotation, see below).  A is kept
+// exactly Hermitian (only the upper 2 x 2 blocks are rotated, the lower ones are
+// their conjugates): a rounding-level anti-Hermitian part would survive every
+// unitary rotation and stall the off-diagonal norm near eps.  Its
+// backward error (H + dH = U Lambda U^+, |dH| ~ eps |H|, U unitary to eps) is of
+// the same order as Gauss-Jordan's, so G agrees with the inverse to roundoff
+// times |H| / dist(z, spectrum).  It costs a few inversions per k and is shared
+// by all energies and frequencies of the k.
+#include "tg_internal.cuh"
+
+#include <algorithm>
+
+namespace tg {
+
+namespace {
+
+constexpr int kEigThreads = 256;
+constexpr int kEigMaxSweeps = 30;
+constexpr int kSpecZ = 16;          // energies per task (two m8 fragments)
+constexpr int kSpecThreads = 256;
+
+// --------------------------------------------------------------------------- Jacobi
+struct Rot {
+  double c, s;
+  double2 e;   // b / |b| of the rotated pair (1 when b = 0)
+};
+
+// pair k of round s of the circle schedule on n (even) indices: every pair once per n - 1 rounds
+__device__ __forceinline__ void rr_pair(int s, int k, int n, int& p, int& q) {
+  const int m = n - 1;
+  if (k == 0) {
+    p = s;
+    q = m;
+  } else {
+    p = (s + k) % m;
+    q = (s - k + m) % m;
+  }
+}
+
+__device__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  return t;
+}
+
+// H: [nk][n][n] row-major (the H(k) table); U: [nk][n][n] row-major U[r][a]; lam: [nk][n]
+__global__ void __launch_bounds__(kEigThreads) eig_jacobi_kernel(const double2* __restrict__ H, int64_t nk, int n,
+                                                                 double2* __restrict__ Uout, double* __restrict__ lam,
+                                                                 int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int np = n / 2;
+  double2* A = reinterpret_cast<double2*>(smem);
+  double2* U = A + n * n;
+  Rot* rot = reinterpret_cast<Rot*>(U + n * n);
+  double* red = reinterpret_cast<double*>(rot + np);
+  for (int64_t k = blockIdx.x; k < nk; k += gridDim.x) {
+    // A = (H + H^+) / 2: the table's H(k) is Hermitian up to rounding; the iteration keeps
+    // A exactly Hermitian (upper blocks computed, lower blocks their conjugates)
+    const double2* Hk = H + k * (int64_t)n * n;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int r = e / n, c = e % n;
+      const double2 x = Hk[e], y = Hk[c * n + r];
+      A[e] = r == c ? make_double2(x.x, 0.0) : make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+      U[e] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    bool converged = false;
+    for (int sweep = 0; sweep < kEigMaxSweeps; ++sweep) {
+      double off = 0.0, tot = 0.0;
+      for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const double m2 = A[e].x * A[e].x + A[e].y * A[e].y;
+        tot += m2;
+        if (e / n != e % n) off += m2;
+      }
+      off = block_sum(off, red);
+      tot = block_sum(tot, red);
+      if (off <= 1e-30 * tot) {
+        converged = true;
+        break;
+      }
+      // couplings below 1e-16 |A|_F are set to zero without a rotation (a backward error
+      // below rounding): rotating them would turn the rounding noise inside a cluster of
+      // degenerate eigenvalues into large random angles that undo the annihilation of the
+      // couplings between clusters (linear instead of quadratic convergence)
+      const double thr_b = 1e-16 * sqrt(tot);
+      for (int s = 0; s < n - 1; ++s) {
+        for (int kk = threadIdx.x; kk < np; kk += blockDim.x) {
+          int p, q;
+          rr_pair(s, kk, n, p, q);
+          const double a = A[p * n + p].x, d = A[q * n + q].x;
+          const double2 b = A[p * n + q];
+          const double ab = hypot(b.x, b.y);
+          Rot r;
+          if (ab <= thr_b) {
+            r.c = 1.0;
+            r.s = 0.0;
+            r.e = make_double2(1.0, 0.0);
+          } else {
+            const double tau = (d - a) / (2.0 * ab);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + hypot(1.0, tau));
+            r.c = 1.0 / sqrt(1.0 + t * t);
+            r.s = t * r.c;
+            r.e = make_double2(b.x / ab, b.y / ab);
+          }
+          rot[kk] = r;
+        }
+        __syncthreads();
+        // A <- J^+ A J on 2 x 2 blocks (rows of pair k1, columns of pair k2), in place:
+        // J = [[c, s], [-s conj(e), c conj(e)]] on (p, q); block (k2, k1) is the conjugate
+        // transpose of block (k1, k2), written by the same thread
+        for (int blk = threadIdx.x; blk < np * np; blk += blockDim.x) {
+          const int k1 = blk / np, k2 = blk % np;
+          if (k1 > k2) continue;
+          int p1, q1, p2, q2;
+          rr_pair(s, k1, n, p1, q1);
+          rr_pair(s, k2, n, p2, q2);
+          const Rot r1 = rot[k1], r2 = rot[k2];
+          if (k1 == k2) {
+            const double a = A[p1 * n + p1].x, d = A[q1 * n + q1].x;
+            const double2 b = A[p1 * n + q1];
+            const double ab = hypot(b.x, b.y);
+            const double t = r1.s / r1.c;
+            A[p1 * n + p1] = make_double2(a - t * ab, 0.0);
+            A[q1 * n + q1] = make_double2(d + t * ab, 0.0);
+            A[p1 * n + q1] = make_double2(0.0, 0.0);
+            A[q1 * n + p1] = make_double2(0.0, 0.0);
+            continue;
+          }
+          const double2 xpp = A[p1 * n + p2], xpq = A[p1 * n + q2], xqp = A[q1 * n + p2], xqq = A[q1 * n + q2];
+          const double2 e2c = cconj(r2.e);
+          // X = A_blk J2
+          const double2 ypq = cmul(e2c, xpq), yqq = cmul(e2c, xqq);
+          const double2 x00 = csub(cscale(xpp, r2.c), cscale(ypq, r2.s));
+          const double2 x01 = cadd(cscale(xpp, r2.s), cscale(ypq, r2.c));
+          const double2 x10 = csub(cscale(xqp, r2.c), cscale(yqq, r2.s));
+          const double2 x11 = cadd(cscale(xqp, r2.s), cscale(yqq, r2.c));
+          // J1^+ X: rows (c x0 - s e x1, s x0 + c e x1)
+          const double2 z10 = cmul(r1.e, x10), z11 = cmul(r1.e, x11);
+          const double2 n00 = csub(cscale(x00, r1.c), cscale(z10, r1.s));
+          const double2 n01 = csub(cscale(x01, r1.c), cscale(z11, r1.s));
+          const double2 n10 = cadd(cscale(x00, r1.s), cscale(z10, r1.c));
+          const double2 n11 = cadd(cscale(x01, r1.s), cscale(z11, r1.c));
+          A[p1 * n + p2] = n00;
+          A[p1 * n + q2] = n01;
+          A[q1 * n + p2] = n10;
+          A[q1 * n + q2] = n11;
+          A[p2 * n + p1] = cconj(n00);
+          A[q2 * n + p1] = cconj(n01);
+          A[p2 * n + q1] = cconj(n10);
+          A[q2 * n + q1] = cconj(n11);
+        }
+        // U <- U J (columns p, q of every row)
+        for (int e = threadIdx.x; e < n * np; e += blockDim.x) {
+          const int r = e / np, kk = e % np;
+          int p, q;
+          rr_pair(s, kk, n, p, q);
+          const Rot rr = rot[kk];
+          const double2 up = U[r * n + p], uq = cmul(cconj(rr.e), U[r * n + q]);
+          U[r * n + p] = csub(cscale(up, rr.c), cscale(uq, rr.s));
+          U[r * n + q] = cadd(cscale(up, rr.s), cscale(uq, rr.c));
+        }
+        __syncthreads();
+      }
+    }
+    if (!converged && threadIdx.x == 0 && status) atomicMin(status, (int)(k < 0x7ffffffe ? k + 1 : 0x7fffffff));
+    double2* Uk = Uout + k * (int64_t)n * n;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) Uk[e] = U[e];
+    for (int a = threadIdx.x; a < n; a += blockDim.x) lam[k * n + a] = A[a * n + a].x;
+    __syncthreads();
+  }
+}
+
+// --------------------------------------------------------------------------- G from (U, lambda)
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+struct SpecArgs {
+  GreenArgs g;
+  const double2* U = nullptr;   // [nk][n][n]
+  const double* lam = nullptr;  // [nk][n]
+  const int* outinv = nullptr;  // [n*n] pair-block slot of (r, c) = r * n + c
+  int kp = 0;                   // K padded to a multiple of 4
+};
+
+__host__ __device__ inline size_t spec_smem(int n, int kp) {
+  return sizeof(double2) * ((size_t)n * kp + (size_t)kSpecZ * kp) + sizeof(double) * kSpecZ + sizeof(int) * kSpecZ;
+}
+
+// (row, col) of G that lands in output slot o for a mode
+__device__ __forceinline__ void slot_rc(const SpecArgs& sa, int mode, int o, int& r, int& c) {
+  const int n = sa.g.n;
+  if (mode == MODE_RAW) {
+    r = o % n;
+    c = o / n;
+    return;
+  }
+  const int rc = sa.g.outmap[o];
+  if (mode == MODE_B_IMAG) {   // G^T
+    c = rc / n;
+    r = rc % n;
+  } else {
+    r = rc / n;
+    c = rc % n;
+  }
+}
+
+__global__ void __launch_bounds__(kSpecThreads) spec_green_kernel(SpecArgs sa) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const GreenArgs& a = sa.g;
+  const int n = a.n, kp = sa.kp, nn = n * n;
+  double2* Us = reinterpret_cast<double2*>(smem);          // [n][kp]
+  double2* Ds = Us + (size_t)n * kp;                        // [kSpecZ][kp]
+  double* ws = reinterpret_cast<double*>(Ds + (size_t)kSpecZ * kp);
+  int* item = reinterpret_cast<int*>(ws + kSpecZ);          // pass-local point of each row, -1 = none
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarp = blockDim.x >> 5;
+  const int64_t ne = a.n_e;
+  const int64_t per_k = (ne + kSpecZ - 1) / kSpecZ;
+  const int64_t ik0 = a.p0 / ne, ik1 = (a.p0 + a.np - 1) / ne;
+  const int64_t ntask = (ik1 - ik0 + 1) * per_k;
+  const bool anti = a.mode == MODE_A_REAL;
+  for (int64_t t = blockIdx.x; t < ntask; t += gridDim.x) {
+    const int64_t ik = ik0 + t / per_k;
+    const int64_t ie0 = (t % per_k) * kSpecZ;
+    // rows of this task
+    if (threadIdx.x < kSpecZ) {
+      const int64_t ie = ie0 + threadIdx.x;
+      const int64_t wi = ik * ne + ie;
+      item[threadIdx.x] = (ie < ne && wi >= a.p0 && wi < a.p0 + a.np) ? (int)(wi - a.p0) : -1;
+    }
+    const double2* Uk = sa.U + ik * (int64_t)nn;
+    for (int e = threadIdx.x; e < n * kp; e += blockDim.x) {
+      const int r = e / kp, aa = e % kp;
+      Us[e] = aa < n ? Uk[r * n + aa] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    // D[z][a] and the weights
+    const double* lk = sa.lam + ik * n;
+    for (int e = threadIdx.x; e < kSpecZ * kp; e += blockDim.x) {
+      const int zr = e / kp, aa = e % kp;
+      double2 dv = make_double2(0.0, 0.0);
+      if (item[zr] >= 0 && aa < n) {
+        const int64_t ie = ie0 + zr;
+        double x, y;
+        if (a.pts.kind == 0) {
+          x = a.zr;
+          y = a.zi + a.ylist[ie];
+        } else {
+          x = a.zr + a.pts.x2[ie];
+          y = a.zi;
+        }
+        x -= lk[aa];
+        const double s = x * x + y * y;
+        if (s == 0.0) {
+          if (a.status) {
+            const int64_t pidx = a.p0 + item[zr] + 1;
+            atomicMin(a.status, (int)(pidx < 0x7fffffff ? pidx : 0x7fffffff));
+          }
+        } else {
+          const double inv = 1.0 / s;
+          dv = anti ? make_double2(0.0, -2.0 * y * inv) : make_double2(x * inv, -y * inv);
+        }
+      }
+      Ds[e] = dv;
+    }
+    if (threadIdx.x < kSpecZ) {
+      double w = 0.0;
+      if (item[threadIdx.x] >= 0) {
+        const int64_t ie = ie0 + threadIdx.x;
+        w = a.pts.kind == 0 ? a.pts.w[ie * a.nk_tab + ik] : a.pts.p2[ie] * a.pts.w[ik];
+      }
+      ws[threadIdx.x] = w;
+    }
+    __syncthreads();
+    // G tiles: 16 energies x 8 output slots per warp step
+    const int g8 = lane >> 2, t4 = lane & 3;
+    const int nfrag = (nn + 7) / 8;
+    for (int nf = warp; nf < nfrag; nf += nwarp) {
+      int rb = 0, cb = 0;
+      const int ob = nf * 8 + g8;
+      if (ob < nn) slot_rc(sa, a.mode, ob, rb, cb);
+      const double2* ur = Us + (size_t)rb * kp;
+      const double2* uc = Us + (size_t)cb * kp;
+      double cr[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, ci[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+      for (int k0 = 0; k0 < kp; k0 += 4) {
+        const int ka = k0 + t4;
+        const double2 pv = cmul(ur[ka], cconj(uc[ka]));
+#pragma unroll
+        for (int mf = 0; mf < 2; ++mf) {
+          const double2 dv = Ds[(mf * 8 + g8) * kp + ka];
+          dmma(cr[mf][0], cr[mf][1], dv.x, pv.x);
+          dmma(cr[mf][0], cr[mf][1], -dv.y, pv.y);
+          dmma(ci[mf][0], ci[mf][1], dv.x, pv.y);
+          dmma(ci[mf][0], ci[mf][1], dv.y, pv.x);
+        }
+      }
+#pragma unroll
+      for (int mf = 0; mf < 2; ++mf) {
+        const int zr = mf * 8 + g8;
+        const int pl = item[zr];
+        if (pl < 0) continue;
+        const double w = ws[zr];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int o = nf * 8 + 2 * t4 + j;
+          if (o >= nn) continue;
+          const double2 v = make_double2(cr[mf][j], ci[mf][j]);
+          double2 v1 = v;
+          if (a.mode == MODE_A_IMAG || a.mode == MODE_A_REAL) v1 = cscale(v, w);
+          else if (a.mode == MODE_B_REAL) v1 = cconj(v);
+          a.out[(int64_t)pl * nn + o] = v1;
+          if (a.out2) {
+            // second operand of the same G: G^T in pair-block order (mode2 == MODE_B_IMAG)
+            int r, c;
+            slot_rc(sa, a.mode, o, r, c);
+            a.out2[(int64_t)pl * nn + sa.outinv[c * n + r]] = v;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------------- host side
+size_t eig_smem_bytes(int n) {
+  return sizeof(double2) * 2 * (size_t)n * n + sizeof(Rot) * (size_t)(n / 2) + sizeof(double) * 32;
+}
+
+int eig_supported(int n) {
+  if (n % 2 != 0 || n < 2) return 0;
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+  return eig_smem_bytes(n) <= (size_t)optin;
+}
+
+cudaError_t launch_eig(const double2* H, int64_t nk, int n, double2* U, double* lam, int* status, int num_sms,
+                       cudaStream_t s) {
+  if (nk <= 0) return cudaSuccess;
+  if (n % 2 != 0 || n < 2) return cudaErrorInvalidValue;
+  const size_t smem = eig_smem_bytes(n);
+  cudaError_t e = cudaFuncSetAttribute(eig_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eig_jacobi_kernel, kEigThreads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm <= 0) return cudaErrorInvalidValue;
+  const int64_t grid = std::min<int64_t>(nk, (int64_t)num_sms * per_sm);
+  eig_jacobi_kernel<<<(unsigned)grid, kEigThreads, smem, s>>>(H, nk, n, U, lam, status);
+  return cudaGetLastError();
+}
+
+int spectral_supported(int mode, int mode2, bool has_out2) {
+  const bool m = mode == MODE_RAW || mode == MODE_A_IMAG || mode == MODE_B_IMAG || mode == MODE_A_REAL ||
+                 mode == MODE_B_REAL;
+  if (!m) return 0;
+  if (has_out2) return mode == MODE_A_IMAG && mode2 == MODE_B_IMAG;
+  return 1;
+}
+
+cudaError_t launch_green_spectral(const GreenArgs& g, const double2* U, const double* lam, const int* outinv,
+                                  int num_sms, cudaStream_t s) {
+  if (g.np <= 0) return cudaSuccess;
+  if (!g.htab || g.n_e <= 0 || !U || !lam) return cudaErrorInvalidValue;
+  if (!spectral_supported(g.mode, g.mode2, g.out2 != nullptr)) return cudaErrorInvalidValue;
+  if (g.out2 && !outinv) return cudaErrorInvalidValue;
+  SpecArgs sa;
+  sa.g = g;
+  sa.U = U;
+  sa.lam = lam;
+  sa.outinv = outinv;
+  sa.kp = (g.n + 3) / 4 * 4;
+  const size_t smem = spec_smem(g.n, sa.kp);
+  cudaError_t e = cudaFuncSetAttribute(spec_green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spec_green_kernel, kSpecThreads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm <= 0) return cudaErrorInvalidValue;
+  const int64_t ne = g.n_e;
+  const int64_t ntask = ((g.p0 + g.np - 1) / ne - g.p0 / ne + 1) * ((ne + kSpecZ - 1) / kSpecZ);
+  const int64_t grid = std::min<int64_t>(ntask, (int64_t)num_sms * per_sm);
+  spec_green_kernel<<<(unsigned)grid, kSpecThreads, smem, s>>>(sa);
+  return cudaGetLastError();
+}
+
+}  // namespace tg

@@ -44,6 +44,8 @@ SIGNATURES = {
     "tg_gg_tensor": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int, _ip, _dp]),
     "tg_fermi_column": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
     "tg_dyson": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),
+    "tg_set_green_method": (C.c_int, [C.c_void_p, C.c_int]),
+    "tg_eig_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp]),
     "tg_she": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp,
                          _dp, C.c_int, _dp]),
     "tg_green_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp]),
@@ -324,6 +326,19 @@ class GreenGPU:
         self._check(self.lib.tg_dyson(self.h, n, _p(a.view(np.float64)), _p(u.view(np.float64)),
                                       _p(out.view(np.float64))))
         return out.T
+
+    def set_green_method(self, method):
+        """"auto": spectral Green functions on tabulated meshes (default); "gauss-jordan": inversion per point."""
+        self._check(self.lib.tg_set_green_method(self.h, {"auto": 0, "gauss-jordan": 1}[method]))
+
+    def eig_batch(self, kp):
+        """Eigenvalues [nk, dimH] and eigenvectors [nk, dimH, dimH] (column a = eigenvector a) of H(k)."""
+        kp = np.ascontiguousarray(kp, np.float64).reshape(-1, 3)
+        nk = kp.shape[0]
+        lam = np.zeros((nk, self.dimH))
+        U = np.zeros((nk, self.dimH, self.dimH), np.complex128)
+        self._check(self.lib.tg_eig_batch(self.h, nk, _p(kp), _p(lam), _p(U.view(np.float64))))
+        return lam, U
 
     def green_batch(self, z, kp):
         z = np.ascontiguousarray(z, np.complex128)
