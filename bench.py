@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--compare-fp64", action="store_true", help="also time the FP64 path and report the ratio")
+    ap.add_argument("--green", default="auto", choices=["auto", "gauss-jordan", "spectral"],
+                    help="Green-function method (tg_set_green_method)")
     ap.add_argument("--workload", default="chi0", choices=["chi0", "she"],
                     help="chi0: the susceptibility integral (headline); she: the disturbance integral "
                          "(eintshe) of the same mesh, one frequency per step")
@@ -235,6 +237,7 @@ def run_ours(args, rank, world, local_rank):
     s = deck.system
     gpu = GreenGPU(local_rank)
     gpu.setup(deck, h0)
+    gpu.set_green_method(args.green)
     gpu.profile(True)
     per = args.omegas_per_step
     start = rank * per * (args.steps + args.warmup)     # ranks take different frequencies
@@ -283,7 +286,9 @@ def run_ours(args, rank, world, local_rank):
                                                                                * per + (args.steps - 1) * per))
                 / (grn_ms / 1e3) / 1e12 if grn_ms else None,
                 "peak": fp64_nominal, "unit": "TFLOP/s", "peak_source": "nominal B200 FP64 (not measured)",
-                "kernel": "green_team_kernel (fused H(k) + Gauss-Jordan)", "flops_per_inversion": 8.0 * s.dimH ** 3,
+                "kernel": ("eig_jacobi_kernel + spec_green_kernel (spectral G, FP64 DMMA)" if args.green != "gauss-jordan"
+                           else "green_w1_kernel / green_team_kernel (fused H(k) + Gauss-Jordan)"),
+                "flops_per_inversion": 8.0 * s.dimH ** 3,
                 "ms_last_step": grn_ms, "launches_in_last_step": int(grn_n)}
     roof_inv["frac"] = roof_inv["achieved"] / fp64_nominal if roof_inv["achieved"] else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -293,7 +298,7 @@ def run_ours(args, rank, world, local_rank):
             "data": "synthetic (seeded Slater-Koster model, no external data)",
             "config": {"workload": f"{args.config}: dimH={s.dimH}, chi dim={s.dimens}, {deck.ek.n_points} imag (E,k) "
                                    f"points, {deck.real_kp.shape[0]} real-axis k x 64 energies, 32 omega in [0,0.5], q=0",
-                       "omegas_per_step": per, "precision": args.precision,
+                       "omegas_per_step": per, "precision": args.precision, "green": args.green,
                        "l2": "inputs larger than L2 (mesh 200+ MB, operands GBs per pass)"},
             "roofline": roof, "roofline_inversion": roof_inv, "gpu_launches": launches, "clocks": clocks}
     if args.compare_fp64 and args.precision != "fp64":
@@ -404,6 +409,7 @@ def run_she(args, rank, world, local_rank):
     s = deck.system
     gpu = GreenGPU(local_rank)
     gpu.setup(deck, h0)
+    gpu.set_green_method(args.green)
     gpu.profile(True)
     n_om = len(omegas)
     start = 1 + rank * (args.steps + args.warmup)   # omega_0 = 0 has no real axis; start at omega_1
@@ -452,7 +458,7 @@ def run_she(args, rank, world, local_rank):
             "data": "synthetic (seeded Slater-Koster model, no external data)",
             "config": {"workload": f"{args.config}: dimH={s.dimH}, dimens={s.dimens}, {deck.ek.n_points} imag (E,k) "
                                    f"points + {deck.real_kp.shape[0]} real-axis k x 64 energies per omega, q=0, "
-                                   f"E along x, one omega per step",
+                                   f"E along x, one omega per step", "green": args.green,
                        "l2": "inputs larger than L2 (G1/G2 buffers GBs per pass)"},
             "roofline": roof, "gpu_launches": launches, "clocks": clocks}
     if rank == 0 and not args.no_cpu and world == 1:

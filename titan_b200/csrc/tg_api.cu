@@ -115,7 +115,7 @@ struct tg_ctx {
   int64_t pass_points = 0;     // points per pass (bounded workspace)
   int gg_blocks = 0, gg_nrow = 0, gg_ncol = 0, gg_mode = -1;
   // spectral Green functions: eigendecomposition of each H(k) table, inverse output map
-  int green_method = 0;   // 0: spectral on tabulated meshes, 1: Gauss-Jordan everywhere
+  int green_method = 0;   // TG_GREEN_AUTO / TG_GREEN_GAUSS_JORDAN / TG_GREEN_SPECTRAL
   DevArray<double2> d_eigU[4];
   DevArray<double> d_eigL[4];
   DevArray<int> d_outinv, d_eig_status;
@@ -272,7 +272,10 @@ int build_htab(tg_ctx* c, int slot, const double* d_k, int64_t nk, const double*
 }
 
 // eigendecomposition of every row of H table `slot` (spectral Green functions)
-bool spectral_on(tg_ctx* c) { return c->green_method == 0 && eig_supported(c->dimH); }
+// chi0 uses spectral Green functions unless Gauss-Jordan is forced; the disturbance
+// integral only when TG_GREEN_SPECTRAL asks for it (see tg_set_green_method)
+bool spectral_on(tg_ctx* c) { return c->green_method != TG_GREEN_GAUSS_JORDAN && eig_supported(c->dimH); }
+bool spectral_she_on(tg_ctx* c) { return c->green_method == TG_GREEN_SPECTRAL && eig_supported(c->dimH); }
 
 int build_eig(tg_ctx* c, int slot, int64_t nk) {
   const size_t nn = (size_t)c->dimH * c->dimH;
@@ -1247,7 +1250,7 @@ int tg_hamiltk_batch(tg_ctx* c, int64_t nk, const double* kp, double* H) {
 
 int tg_set_green_method(tg_ctx* c, int method) {
   if (!c) return TG_ERR_ARG;
-  if (method != TG_GREEN_AUTO && method != TG_GREEN_GAUSS_JORDAN)
+  if (method != TG_GREEN_AUTO && method != TG_GREEN_GAUSS_JORDAN && method != TG_GREEN_SPECTRAL)
     return set_err(c, TG_ERR_ARG, "tg_set_green_method: unknown method");
   c->green_method = method;
   return TG_OK;
@@ -1383,6 +1386,41 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
   if (rc) return rc;
   profile_begin(c);
   TG_CHECK(c, cudaEventRecord(c->ev[0], s), "event");
+  // H(k) tables (k-major traversal) and, for spectral Green functions, their eigendecompositions
+  const bool q_zero = q[0] == 0.0 && q[1] == 0.0 && q[2] == 0.0;
+  const double zero3[3] = {0.0, 0.0, 0.0};
+  const bool tab_imag = c->imag_uniform && (int64_t)c->nk_u * nn * 16 <= ((int64_t)8 << 30);
+  const bool tab_real = real && (int64_t)c->n_realk * nn * 16 <= ((int64_t)8 << 30);
+  const bool spec = spectral_she_on(c);
+  if (spec && (tab_imag || tab_real) && (rc = reset_eig_status(c))) return rc;
+  auto tables = [&](int slot, const double* d_k, int64_t nk, bool shift) -> int {
+    if ((rc = build_htab(c, slot, d_k, nk, shift ? q : zero3))) return rc;
+    if (spec && (rc = build_eig(c, slot, nk))) return rc;
+    return TG_OK;
+  };
+  if (tab_imag) {
+    if ((rc = tables(0, c->d_klist_u.p, c->nk_u, false))) return rc;
+    if (!q_zero && (rc = tables(1, c->d_klist_u.p, c->nk_u, true))) return rc;
+  }
+  if (tab_real) {
+    if ((rc = tables(2, c->d_rkp.p, c->n_realk, false))) return rc;
+    if (!q_zero && (rc = tables(3, c->d_rkp.p, c->n_realk, true))) return rc;
+  }
+  auto use_table = [&](GreenArgs& g, int slot, int64_t n_e, int64_t nk, const double* ylist) {
+    g.htab = c->d_htab[slot].p;
+    g.n_e = n_e;
+    g.nk_tab = nk;
+    g.ylist = ylist;
+    g.q[0] = g.q[1] = g.q[2] = 0.0;   // q is inside the table
+    if (spec) {
+      g.eigU = c->d_eigU[slot].p;
+      g.eigL = c->d_eigL[slot].p;
+      g.outinv = c->d_outinv.p;
+    } else {
+      g.eigU = nullptr;
+      g.eigL = nullptr;
+    }
+  };
   GreenArgs base = base_args(c);
   SheLaunch l;
   l.g = &base;
@@ -1395,10 +1433,13 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
   she_spin_codes(l.spins);
   l.partial = c->d_she_part.p;
   l.grid = grid;
-  auto pass = [&](GreenArgs g, int real_axis) -> int {
-    // G2 = G(k, E), G1 = G(k + q, E + e), both column-major per point
+  // one pass: G2 = G(k, E), G1 = G(k + q, E + e), both column-major per point, then the
+  // vertex; slot2 / slot1 >= 0: H(k) tables of G2 / G1 with n_e energies per k (k-major order)
+  auto pass = [&](GreenArgs g, int real_axis, int slot2, int slot1, int64_t n_e, int64_t nk,
+                  const double* ylist, const double* klist) -> int {
     g.mode = MODE_RAW;
     g.out = c->d_B.p;
+    if (slot2 >= 0) use_table(g, slot2, n_e, nk, ylist);
     {
       KindTimer kt(c, 0);
       TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), "green (G2)");
@@ -1409,10 +1450,14 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
     g.q[1] = q[1];
     g.q[2] = q[2];
     g.out = c->d_A.p;
+    if (slot1 >= 0) use_table(g, slot1, n_e, nk, ylist);
     {
       KindTimer kt(c, 0);
       TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), "green (G1)");
     }
+    l.n_e = slot2 >= 0 ? n_e : 0;
+    l.nk_tab = nk;
+    l.klist = klist;
     l.G1 = c->d_A.p;
     l.G2 = c->d_B.p;
     l.p0 = g.p0;
@@ -1436,7 +1481,9 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
     g.np = std::min<int64_t>(P, c->n_imag - p0);
     g.zr = Ef;
     g.zi = etap;
-    if ((rc = pass(g, 0))) return rc;
+    if (tab_imag) rc = pass(g, 0, 0, q_zero ? 0 : 1, c->n_e_u, c->nk_u, c->d_ylist.p, c->d_klist_u.p);
+    else rc = pass(g, 0, -1, -1, 0, 0, nullptr, nullptr);
+    if (rc) return rc;
   }
   if (real) {
     const int64_t ntot = (int64_t)n_real * c->n_realk;
@@ -1452,7 +1499,9 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
       g.np = std::min<int64_t>(P, ntot - p0);
       g.zr = 0.0;
       g.zi = etap;
-      if ((rc = pass(g, 1))) return rc;
+      if (tab_real) rc = pass(g, 1, 2, q_zero ? 2 : 3, n_real, c->n_realk, nullptr, c->d_rkp.p);
+      else rc = pass(g, 1, -1, -1, 0, 0, nullptr, nullptr);
+      if (rc) return rc;
     }
   }
   {
@@ -1472,7 +1521,10 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
   cudaEventElapsedTime(&ms, c->ev[0], c->ev[6]);
   c->last_ms[3] = ms;
   profile_end(c);
-  return read_status(c);
+  rc = read_status(c);
+  if (rc) return rc;
+  if (spec && (tab_imag || tab_real)) return read_eig_status(c);
+  return TG_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -193,6 +193,10 @@ struct SheLaunch {
   unsigned char spins[3][16] = {};
   double2* partial = nullptr;     // [grid][4 dimens]
   int grid = 0;
+  // k-major point order of a tabulated pass (n_e > 0): point p0 + pl -> k = klist[p / n_e],
+  // energy p % n_e, as the inversion kernels walk an H(k) table
+  int64_t n_e = 0, nk_tab = 0;
+  const double* klist = nullptr;
 };
 size_t she_smem_bytes(int n, int dimens, int n_neigh);
 // CTAs of one vertex launch (SMs x resident CTAs); 0 when the shared memory does not fit

@@ -47,6 +47,8 @@ struct SheArgs {
   double ue[3] = {0, 0, 0};
   unsigned char spins[3][16] = {};   // term t, (s * 4 + s') -> a << 3 | b << 2 | c << 1 | d (0 = up)
   double2* partial = nullptr;        // [gridDim][4 dimens], df(row, s') at s' dimens + row
+  int64_t n_e = 0, nk_tab = 0;       // k-major order of a tabulated pass (n_e > 0)
+  const double* klist = nullptr;
 };
 
 struct SheSmem {
@@ -151,7 +153,13 @@ __global__ void __launch_bounds__(256) she_kernel(SheArgs a) {
   for (int64_t pl = blockIdx.x; pl < a.np; pl += gridDim.x) {
     const int64_t p = a.p0 + pl;
     double kx, ky, kz, w;
-    if (a.pts.kind == 0) {
+    if (a.n_e > 0) {
+      const int64_t ik = p / a.n_e, ie = p % a.n_e;
+      kx = a.klist[3 * ik];
+      ky = a.klist[3 * ik + 1];
+      kz = a.klist[3 * ik + 2];
+      w = a.pts.kind == 0 ? a.pts.w[ie * a.nk_tab + ik] : a.pts.p2[ie] * a.pts.w[ik];
+    } else if (a.pts.kind == 0) {
       kx = a.pts.kp[3 * p];
       ky = a.pts.kp[3 * p + 1];
       kz = a.pts.kp[3 * p + 2];
@@ -307,6 +315,9 @@ cudaError_t launch_she(const SheLaunch& l, cudaStream_t s) {
   for (int t = 0; t < 3; ++t)
     for (int i = 0; i < 16; ++i) a.spins[t][i] = l.spins[t][i];
   a.partial = l.partial;
+  a.n_e = l.n_e;
+  a.nk_tab = l.nk_tab;
+  a.klist = l.klist;
   int dev = 0, optin = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);

@@ -13,7 +13,7 @@
 //
 // The eigendecomposition is a cyclic two-sided Jacobi iteration, one CTA per
 // matrix, n / 2 disjoint rotations per step in round-robin order, sweeps until
-// the off-diagonal Frobenius norm is below 1e-15 of the matrix norm (couplings
+// the off-diagonal Frobenius norm is below 1e-17 of the matrix norm (couplings
 // under 1e-16 of it are zeroed without a rotation, see below).  A is kept
 // exactly Hermitian (only the upper 2 x 2 blocks are rotated, the lower ones are
 // their conjugates): a rounding-level anti-Hermitian part would survive every
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(kEigThreads) eig_jacobi_kernel(const double2* 
       }
       off = block_sum(off, red);
       tot = block_sum(tot, red);
-      if (off <= 1e-30 * tot) {
+      if (off <= 1e-34 * tot) {
         converged = true;
         break;
       }

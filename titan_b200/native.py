@@ -328,8 +328,10 @@ class GreenGPU:
         return out.T
 
     def set_green_method(self, method):
-        """"auto": spectral Green functions on tabulated meshes (default); "gauss-jordan": inversion per point."""
-        self._check(self.lib.tg_set_green_method(self.h, {"auto": 0, "gauss-jordan": 1}[method]))
+        """"auto" (default): spectral Green functions for chi0 on tabulated meshes, Gauss-Jordan for the
+        disturbance integral; "gauss-jordan": inversion per point everywhere; "spectral": spectral wherever
+        the mesh allows (see tg_set_green_method)."""
+        self._check(self.lib.tg_set_green_method(self.h, {"auto": 0, "gauss-jordan": 1, "spectral": 2}[method]))
 
     def eig_batch(self, kp):
         """Eigenvalues [nk, dimH] and eigenvectors [nk, dimH, dimH] (column a = eigenvector a) of H(k)."""
