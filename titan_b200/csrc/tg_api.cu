@@ -101,6 +101,7 @@ struct tg_ctx {
   DevArray<unsigned long long> d_m64A, d_m64B;
   DevArray<int> d_EA, d_EB, d_chunks, d_split_err;
   std::vector<double> h_y;   // imaginary-axis energies per point (chunk boundaries)
+  std::vector<double> h_klist_u, h_rkp;   // host copies of the uniform k list and the real-axis BZ
   DevArray<double2> d_dy;
   DevArray<int> d_piv;
   cudaEvent_t ev[8] = {};
@@ -306,6 +307,10 @@ int read_eig_status(tg_ctx* c) {
   }
   return TG_OK;
 }
+
+// the real-axis BZ is the uniform imaginary-axis k list (same points, same order): its
+// H(k) tables and eigendecompositions are those of the imaginary axis
+bool real_k_is_imag_k(tg_ctx* c) { return c->imag_uniform && c->real_set && c->h_rkp == c->h_klist_u; }
 
 // contraction of one pass into Cpart on the FP64 SIMT path
 int contract(tg_ctx* c, const double2* A, const double2* B, int64_t np, double2* Cpart, int nsplit,
@@ -648,6 +653,7 @@ int tg_set_imag_mesh(tg_ctx* c, int64_t n_points, const double* y, const double*
     if (ok && ne > 1) {
       TG_CHECK(c, c->d_ylist.upload(ylist.data(), ne, c->stream), "upload ylist");
       TG_CHECK(c, c->d_klist_u.upload(kp, 3 * nk, c->stream), "upload klist");
+      c->h_klist_u.assign(kp, kp + 3 * nk);
       c->imag_uniform = true;
       c->n_e_u = ne;
       c->nk_u = nk;
@@ -666,6 +672,7 @@ int tg_set_real_mesh(tg_ctx* c, int64_t n_k, const double* kp, const double* w) 
   TG_CHECK(c, c->d_rkp.upload(kp, 3 * n_k, c->stream), "upload kp");
   TG_CHECK(c, c->d_rw.upload(w, n_k, c->stream), "upload w");
   TG_CHECK(c, cudaStreamSynchronize(c->stream), "sync");
+  c->h_rkp.assign(kp, kp + 3 * n_k);
   c->n_realk = n_k;
   c->real_set = true;
   return TG_OK;
@@ -725,7 +732,10 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     if (!q_zero && (rc = build_htab(c, 1, c->d_klist_u.p, c->nk_u, q))) return rc;
     if (!q_zero && spec && (rc = build_eig(c, 1, c->nk_u))) return rc;
   }
-  if (tab_real) {
+  // real-axis slots 2 / 3 alias the imaginary-axis slots 0 / 1 when the k lists coincide
+  const bool alias_real = tab_imag && tab_real && real_k_is_imag_k(c);
+  const int rslot0 = alias_real ? 0 : 2, rslot1 = alias_real ? 1 : 3;
+  if (tab_real && !alias_real) {
     if ((rc = build_htab(c, 2, c->d_rkp.p, c->n_realk, zero3))) return rc;
     if (spec && (rc = build_eig(c, 2, c->n_realk))) return rc;
     if (!q_zero && (rc = build_htab(c, 3, c->d_rkp.p, c->n_realk, q))) return rc;
@@ -851,7 +861,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       gr.zi = etap;
       gr.mode = MODE_B_REAL;
       gr.out = c->d_B.p;
-      if (tab_real) use_table(gr, 2, n_real, c->n_realk, nullptr);
+      if (tab_real) use_table(gr, rslot0, n_real, c->n_realk, nullptr);
       {
         KindTimer kt(c, 0);
         TG_CHECK(c, launch_green(gr, c->num_sms, s, nullptr), "green (real, G2)");
@@ -863,7 +873,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       gr.mode = MODE_A_REAL;
       gr.out = c->d_A.p;
       if (tab_real) {
-        use_table(gr, q_zero ? 2 : 3, n_real, c->n_realk, nullptr);
+        use_table(gr, q_zero ? rslot0 : rslot1, n_real, c->n_realk, nullptr);
         gr.q[0] = gr.q[1] = gr.q[2] = 0.0;
       }
       {
@@ -1402,7 +1412,9 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
     if ((rc = tables(0, c->d_klist_u.p, c->nk_u, false))) return rc;
     if (!q_zero && (rc = tables(1, c->d_klist_u.p, c->nk_u, true))) return rc;
   }
-  if (tab_real) {
+  const bool alias_real = tab_imag && tab_real && real_k_is_imag_k(c);
+  const int rslot0 = alias_real ? 0 : 2, rslot1 = alias_real ? 1 : 3;
+  if (tab_real && !alias_real) {
     if ((rc = tables(2, c->d_rkp.p, c->n_realk, false))) return rc;
     if (!q_zero && (rc = tables(3, c->d_rkp.p, c->n_realk, true))) return rc;
   }
@@ -1499,7 +1511,7 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
       g.np = std::min<int64_t>(P, ntot - p0);
       g.zr = 0.0;
       g.zi = etap;
-      if (tab_real) rc = pass(g, 1, 2, q_zero ? 2 : 3, n_real, c->n_realk, nullptr, c->d_rkp.p);
+      if (tab_real) rc = pass(g, 1, rslot0, q_zero ? rslot0 : rslot1, n_real, c->n_realk, nullptr, c->d_rkp.p);
       else rc = pass(g, 1, -1, -1, 0, 0, nullptr, nullptr);
       if (rc) return rc;
     }

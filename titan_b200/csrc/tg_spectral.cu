@@ -334,10 +334,12 @@ __global__ void __launch_bounds__(kSpecThreads) spec_green_kernel(SpecArgs sa) {
           else if (a.mode == MODE_B_REAL) v1 = cconj(v);
           a.out[(int64_t)pl * nn + o] = v1;
           if (a.out2) {
-            // second operand of the same G: G^T in pair-block order (mode2 == MODE_B_IMAG)
+            // the other imaginary-axis operand of the same G: v = G[r][c] goes to slot
+            // (c, r) of the G^T layout (mode2 B) or, times w, to slot (r, c) of the G layout (mode2 A)
             int r, c;
             slot_rc(sa, a.mode, o, r, c);
-            a.out2[(int64_t)pl * nn + sa.outinv[c * n + r]] = v;
+            const bool tr = a.mode2 == MODE_B_IMAG;
+            a.out2[(int64_t)pl * nn + sa.outinv[tr ? c * n + r : r * n + c]] = tr ? v : cscale(v, w);
           }
         }
       }
@@ -381,7 +383,8 @@ int spectral_supported(int mode, int mode2, bool has_out2) {
   const bool m = mode == MODE_RAW || mode == MODE_A_IMAG || mode == MODE_B_IMAG || mode == MODE_A_REAL ||
                  mode == MODE_B_REAL;
   if (!m) return 0;
-  if (has_out2) return mode == MODE_A_IMAG && mode2 == MODE_B_IMAG;
+  if (has_out2)
+    return (mode == MODE_A_IMAG && mode2 == MODE_B_IMAG) || (mode == MODE_B_IMAG && mode2 == MODE_A_IMAG);
   return 1;
 }
 
