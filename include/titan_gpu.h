@@ -173,6 +173,14 @@ int tg_she(tg_ctx* ctx, const double* q, double e, double Ef, double eta, double
            const double* x2, const double* p2, const double* efield, const double* prefactor,
            int dimens, double* tchi);
 
+/* Local density of states on the real axis: replaces ldos_energy(e, ldosu, ldosd)
+ * (source/mod_LDOS.F90:95-150) for n_e energies at once:
+ *   ldosu(mu, i, ie) = -(1/pi) sum_k w_k Im G(i up mu, i up mu; k, e(ie) + i eta)
+ * (ldosd with the down block) over the real-axis BZ of tg_set_real_mesh;
+ * ldosu, ldosd(norb_max, n_atoms, n_e).  With TG_GREEN_AUTO / TG_GREEN_SPECTRAL each
+ * H(k) is diagonalised once for all energies; TG_GREEN_GAUSS_JORDAN inverts per (k, e). */
+int tg_ldos(tg_ctx* ctx, int n_e, const double* e, double eta, double* ldosu, double* ldosd);
+
 /* How G(k, z) is computed.  Spectral: on meshes where every energy uses the same
  * k list (uniform imaginary axis, the real-axis BZ) H(k) is diagonalised once per k
  * (Jacobi, FP64) and G(k, z) = U diag(1/(z - lambda)) U^+ is formed for all energies

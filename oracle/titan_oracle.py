@@ -679,3 +679,27 @@ def disturbance_outputs(system, chi_hf, tchi_raw, U, lvec, lambda_p, lambda_d, p
         bc[3, i] = 0.5 * (beff[s2i(2, i)] - beff[s2i(3, i)])
     return {"tchiorbiikl": T, "disturbances": dist, "torques": torq, "beff": bc,
             "total_disturbances": dist.sum(axis=1), "total_torques": torq.sum(axis=2), "total_beff": bc.sum(axis=1)}
+
+
+# ---------------------------------------------------------------------------
+# Local density of states on the real axis, source/mod_LDOS.F90:95-150 (ldos_energy):
+# ldosu(i, mu) = -(1/pi) sum_k w_k Im G(i up mu, i up mu; k, e + i eta), ldosd with the down block.
+# ---------------------------------------------------------------------------
+def ldos(model: Model, real_bz, energies, eta, chunk=4096):
+    """(ldosu, ldosd) [n_e, nAtoms, nOrbMax] at each energy e (absolute, as green(e, eta) is called)."""
+    s = model.system
+    kp, w = real_bz
+    ia = s.ia()
+    nmax = max(s.norbs)
+    up = np.zeros((len(energies), s.n_atoms, nmax))
+    dn = np.zeros((len(energies), s.n_atoms, nmax))
+    for ie, e in enumerate(energies):
+        for sl in _chunks(kp.shape[0], chunk):
+            G = model.green(np.full(kp[sl].shape[0], e + 1j * eta), kp[sl])
+            d = np.einsum('kii->ki', G).imag
+            for i in range(s.n_atoms):
+                n = s.norbs[i]
+                r0 = ia[i][0]
+                up[ie, i, :n] -= w[sl] @ d[:, r0:r0 + n]
+                dn[ie, i, :n] -= w[sl] @ d[:, r0 + n:r0 + 2 * n]
+    return up / PI, dn / PI

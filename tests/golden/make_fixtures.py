@@ -2,7 +2,7 @@
 
 The reference tests this path only through example runs compared against
 ``results_correct`` files (its CI: .gitlab-ci.yml, jobs Fe_bulk, Fe_bulk:susc,
-graphene_pz, nanoribbon).  This script copies those example input decks and golden
+graphene_pz, nanoribbon, Nb_100_Monolayer:ldos).  This script copies those example input decks and golden
 outputs, unchanged, into ``tests/golden/<example>/`` so the tests can run
 without the reference tree.  Run it from the repository root:
 
@@ -28,6 +28,15 @@ FILES = {
         "input", "basis", "A2", "A3",
         "results_correct/scResult",
     ],
+    "Nb_100_Monolayer": [
+        "input", "basis", "Nb",
+        "results_correct/scResult",
+        "results_correct/TSOC/selfconsistency/selfconsistency_1Sites_dfttype=S_parts=2_norb=9_nkpt=1024_eta=1.0E-03_ev.dat",
+        "results_correct/TSOC/1Sites/LDOS/ldosu_site=1_norb=9_nkpt=1024_eta=1.0E-03_ev.dat",
+        "results_correct/TSOC/1Sites/LDOS/ldosd_site=1_norb=9_nkpt=1024_eta=1.0E-03_ev.dat",
+        "results_correct/TSOC/1Sites/LDOS/lmdosu_site=1_norb=9_nkpt=1024_eta=1.0E-03_ev.dat",
+        "results_correct/TSOC/1Sites/LDOS/lmdosd_site=1_norb=9_nkpt=1024_eta=1.0E-03_ev.dat",
+    ],
 }
 NANO_SUFFIX = "parts=2_parts3=1_norb=2_nkpt=1000_eta=1.0E-03_ev_fixEf_Ef=-0.25_SOC=0.10_Vab=0.15_pxpy.dat"
 
@@ -37,6 +46,12 @@ SHORT = {
     "results_correct/TSOC/selfconsistency/selfconsistency_1Sites_dfttype=S_parts=2_norb=9_nkpt=1000_eta=1.0E-03.dat": "selfconsistency.dat",
     "results_correct/TSOC/1Sites/HF/chihf_1_1_parts=2_parts3=1_norb=9_nkpt=1000_eta=1.0E-03.dat": "chihf_1_1.dat",
     "results_correct/TSOC/1Sites/RPA/chi_1_1_parts=2_parts3=1_norb=9_nkpt=1000_eta=1.0E-03.dat": "chi_1_1.dat",
+    "results_correct/TSOC/selfconsistency/selfconsistency_1Sites_dfttype=S_parts=2_norb=9_nkpt=1024_eta=1.0E-03_ev.dat":
+        "selfconsistency.dat",
+    "results_correct/TSOC/1Sites/LDOS/ldosu_site=1_norb=9_nkpt=1024_eta=1.0E-03_ev.dat": "ldosu_site=1.dat",
+    "results_correct/TSOC/1Sites/LDOS/ldosd_site=1_norb=9_nkpt=1024_eta=1.0E-03_ev.dat": "ldosd_site=1.dat",
+    "results_correct/TSOC/1Sites/LDOS/lmdosu_site=1_norb=9_nkpt=1024_eta=1.0E-03_ev.dat": "lmdosu_site=1.dat",
+    "results_correct/TSOC/1Sites/LDOS/lmdosd_site=1_norb=9_nkpt=1024_eta=1.0E-03_ev.dat": "lmdosd_site=1.dat",
 }
 
 
@@ -67,6 +82,11 @@ def main(ref_root: str) -> None:
                 for f in sorted(os.listdir(src_dir)):
                     short = f.split("_parts=")[0] + ".dat"
                     shutil.copyfile(os.path.join(src_dir, f), os.path.join(dst, "resp", short))
+        # the bulk reference densities of Nb (Un != 0): initialrho file of the element
+        if ex == "Nb_100_Monolayer":
+            shutil.copyfile(os.path.join(ref_root, "examples", ex, "results_correct", "FSOC", "selfconsistency",
+                                         "initialrho_Nb_dfttype=S_parts=2_norb=9_nkpt=1024_eta=1.0E-03_ev.dat"),
+                            os.path.join(dst, "initialrho_Nb.dat"))
         # the graphene self-consistency file has a run-dependent name
         if ex == "graphene":
             sc_dir = os.path.join(ref_root, "examples", ex, "results_correct", "FSOC", "selfconsistency")

@@ -1,6 +1,9 @@
-"""Reader and comparator for the reference's calculate_all output files (disturbances,
-torques and effective fields per site and their totals) in tests/golden/<deck>/resp."""
+"""Readers of the reference's golden decks and outputs shared by the CPU and GPU tests: the
+calculate_all output files (disturbances, torques and effective fields per site and their
+totals) in tests/golden/<deck>/resp, and the Nb(100) monolayer deck with its LDOS files."""
 import os
+
+import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -39,3 +42,19 @@ def check_responses(name, out, n_atoms, rtol=1e-8):
             assert abs(abs(v) - g[0]) <= tol, (kind, k, abs(v), g[0])
             assert abs(v.real - g[1]) <= tol, (kind, k, v.real, g[1])
             assert abs(v.imag - g[2]) <= tol, (kind, k, v.imag, g[2])
+
+
+def nb_ldos_golden(name):
+    f = os.path.join(GOLDEN, "Nb_100_Monolayer", name)
+    return np.array([[float(x) for x in l.split()] for l in open(f) if not l.startswith("#")])
+
+
+def nb_monolayer():
+    """The reference's Nb(100) monolayer deck (9 orbitals, SOC, Un = Um != 0 with the bulk
+    reference densities of its initialrho file) at its golden self-consistent state."""
+    from titan_b200.host.deck import Deck
+    from titan_b200.host.system import read_sc_file
+    d = Deck.from_directory(os.path.join(GOLDEN, "Nb_100_Monolayer"))
+    st = read_sc_file(os.path.join(GOLDEN, "Nb_100_Monolayer", "selfconsistency.dat"), d.system.norbs)
+    d.system.Ef = st.Ef
+    return d, st

@@ -13,7 +13,7 @@ import pytest
 
 from oracle import compare_output as C
 from oracle import titan_oracle as O
-from golden_resp import check_responses
+from golden_resp import check_responses, nb_ldos_golden, nb_monolayer
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -140,3 +140,20 @@ def test_nanoribbon_disturbances_match_golden():
         scale = np.abs(out[key]).max()
         assert np.abs(host[key] - out[key]).max() <= 1e-12 * scale, key
     np.testing.assert_allclose(out["tchiorbiikl"], pref @ tchi, rtol=0, atol=1e-14 * np.abs(tchi).max())
+
+
+def test_nb_ldos_matches_golden():
+    """ldos_energy restated: spin- and orbital-resolved LDOS of the Nb(100) monolayer at the 101
+    energies of the reference's Nb_100_Monolayer:ldos CI job (10 significant digits; here 2e-9
+    relative per entry, and the s / p / d / total columns of the ldos files)."""
+    d, st = nb_monolayer()
+    s = d.system
+    lu, ld = nb_ldos_golden("ldosu_site=1.dat"), nb_ldos_golden("ldosd_site=1.dat")
+    mu, md = nb_ldos_golden("lmdosu_site=1.dat"), nb_ldos_golden("lmdosd_site=1.dat")
+    up, dn = O.ldos(O.Model(s, s.h0(st)), (d.real_kp, d.real_w), lu[:, 0], s.eta)
+    for ours, per_orb, summed in ((up[:, 0], mu, lu), (dn[:, 0], md, ld)):
+        np.testing.assert_allclose(ours, per_orb[:, 1:], rtol=2e-9, atol=0)
+        np.testing.assert_allclose(ours.sum(1), summed[:, 1], rtol=2e-9, atol=0)
+        np.testing.assert_allclose(ours[:, 0], summed[:, 2], rtol=2e-9, atol=0)
+        np.testing.assert_allclose(ours[:, 1:4].sum(1), summed[:, 3], rtol=2e-9, atol=0)
+        np.testing.assert_allclose(ours[:, 4:].sum(1), summed[:, 4], rtol=2e-9, atol=0)

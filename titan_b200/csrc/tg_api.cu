@@ -120,6 +120,7 @@ struct tg_ctx {
   DevArray<double2> d_eigU[4];
   DevArray<double> d_eigL[4];
   DevArray<int> d_outinv, d_eig_status;
+  DevArray<double> d_ldos_e, d_ldos;
   // disturbance response (eintshe)
   DevArray<int> d_she_tab, d_ia;
   DevArray<double2> d_she_part, d_she_sum, d_she_pref, d_she_out;
@@ -1283,6 +1284,56 @@ int tg_eig_batch(tg_ctx* c, int64_t nk, const double* kp, double* lam, double* U
   TG_CHECK(c, cudaMemcpyAsync(lam, c->d_eigL[0].p, sizeof(double) * nk * c->dimH, cudaMemcpyDeviceToHost, s), "copy");
   TG_CHECK(c, cudaMemcpyAsync(U, c->d_eigU[0].p, sizeof(double2) * nk * nn, cudaMemcpyDeviceToHost, s), "copy");
   return read_eig_status(c);
+}
+
+int tg_ldos(tg_ctx* c, int n_e, const double* e, double eta, double* ldosu, double* ldosd) {
+  int rc = check_ready(c, false, true);
+  if (rc) return rc;
+  if (n_e < 0 || (n_e > 0 && (!e || !ldosu || !ldosd))) return set_err(c, TG_ERR_ARG, "tg_ldos: bad args");
+  if (n_e == 0) return TG_OK;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int n = c->dimH, nat = c->n_atoms, nmax = c->nmax;
+  auto put = [&](int ie, int i, int mu, double up, double dn) {
+    const size_t o = ((size_t)ie * nat + i) * nmax + mu;
+    ldosu[o] = up;
+    ldosd[o] = dn;
+  };
+  std::fill(ldosu, ldosu + (size_t)n_e * nat * nmax, 0.0);
+  std::fill(ldosd, ldosd + (size_t)n_e * nat * nmax, 0.0);
+  if (!spectral_on(c)) {
+    // Gauss-Jordan per (k, e): the sigma_0 / sigma_z traces of G_ii of the Fermi-column kernel
+    std::vector<double> D((size_t)2 * 4 * nmax * nat);
+    const double pi = kPi;
+    for (int ie = 0; ie < n_e; ++ie) {
+      if ((rc = tg_fermi_column(c, e[ie], eta, D.data()))) return rc;
+      for (int i = 0; i < nat; ++i)
+        for (int mu = 0; mu < c->norb[i]; ++mu) {
+          const double* d = D.data() + 2 * 4 * ((size_t)i * nmax + mu);
+          put(ie, i, mu, -(d[1] + d[7]) / (2.0 * pi), -(d[1] - d[7]) / (2.0 * pi));
+        }
+    }
+    return TG_OK;
+  }
+  // spectral: one eigendecomposition per k of the real-axis BZ, every energy from it
+  const double zero3[3] = {0.0, 0.0, 0.0};
+  if ((rc = reset_eig_status(c))) return rc;
+  if ((rc = build_htab(c, 2, c->d_rkp.p, c->n_realk, zero3))) return rc;
+  if ((rc = build_eig(c, 2, c->n_realk))) return rc;
+  TG_CHECK(c, c->d_ldos_e.upload(e, n_e, s), "upload energies");
+  TG_CHECK(c, c->d_ldos.ensure((size_t)n_e * n), "alloc ldos");
+  c->launches += 1;
+  TG_CHECK(c, launch_spec_ldos(c->d_eigU[2].p, c->d_eigL[2].p, c->d_rw.p, c->n_realk, n, c->d_ldos_e.p, n_e, eta,
+                               c->d_ldos.p, c->num_sms, s),
+           "ldos");
+  std::vector<double> h((size_t)n_e * n);
+  TG_CHECK(c, cudaMemcpyAsync(h.data(), c->d_ldos.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s), "copy");
+  if ((rc = read_eig_status(c))) return rc;   // synchronises the stream
+  for (int ie = 0; ie < n_e; ++ie)
+    for (int i = 0; i < nat; ++i)
+      for (int mu = 0; mu < c->norb[i]; ++mu)
+        put(ie, i, mu, h[(size_t)ie * n + c->ia[i] + mu], h[(size_t)ie * n + c->ia[i] + c->norb[i] + mu]);
+  return TG_OK;
 }
 
 int tg_dyson(tg_ctx* c, int dimens, const double* chi_hf, const double* umat, double* chi) {

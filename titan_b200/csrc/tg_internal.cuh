@@ -173,6 +173,9 @@ int eig_supported(int n);
 cudaError_t launch_eig(const double2* H, int64_t nk, int n, double2* U, double* lam, int* status, int num_sms,
                        cudaStream_t s);
 int spectral_supported(int mode, int mode2, bool has_out2);
+// out[ie][r] = -Im G_rr(e_ie + i eta) / pi summed over the tabulated k with weights w
+cudaError_t launch_spec_ldos(const double2* U, const double* lam, const double* w, int64_t nk, int n,
+                             const double* e, int n_e, double eta, double* out, int num_sms, cudaStream_t s);
 cudaError_t launch_green_spectral(const GreenArgs& g, const double2* U, const double* lam, const int* outinv,
                                   int num_sms, cudaStream_t s);
 

@@ -348,9 +348,69 @@ __global__ void __launch_bounds__(kSpecThreads) spec_green_kernel(SpecArgs sa) {
   }
 }
 
+// --------------------------------------------------------------------------- LDOS from (U, lambda)
+constexpr int kLdosE = 32;   // energies per CTA
+
+// out[ie][r] += (eta / pi) sum_{k in this CTA's chunk} w_k sum_a |U[k][r][a]|^2 / ((e_ie - lambda_ka)^2 + eta^2),
+// i.e. -Im G_rr(k, e + i eta) / pi summed over the chunk (atomicAdd into out)
+__global__ void __launch_bounds__(256) spec_ldos_kernel(const double2* __restrict__ U, const double* __restrict__ lam,
+                                                        const double* __restrict__ w, int64_t nk, int n,
+                                                        const double* __restrict__ e, int n_e, double eta,
+                                                        int64_t k_per_cta, double* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* P = reinterpret_cast<double*>(smem);   // [n][n] |U|^2
+  double* L = P + n * n;                          // [kLdosE][n]
+  double* acc = L + kLdosE * n;                   // [kLdosE][n]
+  const int e0 = blockIdx.x * kLdosE;
+  const int ne = min(kLdosE, n_e - e0);
+  const int64_t k0 = (int64_t)blockIdx.y * k_per_cta, k1 = min(nk, k0 + k_per_cta);
+  for (int o = threadIdx.x; o < kLdosE * n; o += blockDim.x) acc[o] = 0.0;
+  for (int64_t k = k0; k < k1; ++k) {
+    __syncthreads();
+    const double2* Uk = U + k * (int64_t)n * n;
+    for (int o = threadIdx.x; o < n * n; o += blockDim.x) {
+      const double2 u = Uk[o];
+      P[o] = u.x * u.x + u.y * u.y;
+    }
+    for (int o = threadIdx.x; o < ne * n; o += blockDim.x) {
+      const double x = e[e0 + o / n] - lam[k * n + o % n];
+      L[o] = 1.0 / (x * x + eta * eta);
+    }
+    __syncthreads();
+    const double wk = w[k];
+    for (int o = threadIdx.x; o < ne * n; o += blockDim.x) {
+      const int ie = o / n, r = o % n;
+      const double* pr = P + r * n;
+      const double* le = L + ie * n;
+      double s = 0.0;
+      for (int a = 0; a < n; ++a) s = fma(pr[a], le[a], s);
+      acc[o] = fma(wk, s, acc[o]);
+    }
+  }
+  __syncthreads();
+  const double f = eta / 3.141592653589793238462643383279502884;
+  for (int o = threadIdx.x; o < ne * n; o += blockDim.x) atomicAdd(out + (int64_t)(e0 + o / n) * n + o % n, f * acc[o]);
+}
+
 }  // namespace
 
 // --------------------------------------------------------------------------- host side
+cudaError_t launch_spec_ldos(const double2* U, const double* lam, const double* w, int64_t nk, int n,
+                             const double* e, int n_e, double eta, double* out, int num_sms, cudaStream_t s) {
+  if (nk <= 0 || n_e <= 0) return cudaSuccess;
+  const size_t smem = sizeof(double) * ((size_t)n * n + 2 * (size_t)kLdosE * n);
+  cudaError_t err = cudaFuncSetAttribute(spec_ldos_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  err = cudaMemsetAsync(out, 0, sizeof(double) * (size_t)n_e * n, s);
+  if (err != cudaSuccess) return err;
+  const int eb = (n_e + kLdosE - 1) / kLdosE;
+  const int64_t kchunks = std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)4 * num_sms / eb));
+  const int64_t kper = (nk + kchunks - 1) / kchunks;
+  const dim3 grid((unsigned)eb, (unsigned)((nk + kper - 1) / kper));
+  spec_ldos_kernel<<<grid, 256, smem, s>>>(U, lam, w, nk, n, e, n_e, eta, kper, out);
+  return cudaGetLastError();
+}
+
 size_t eig_smem_bytes(int n) {
   return sizeof(double2) * 2 * (size_t)n * n + sizeof(Rot) * (size_t)(n / 2) + sizeof(double) * 32;
 }

@@ -15,7 +15,8 @@ import numpy as np
 
 from . import lattice as L
 from . import mesh as M
-from .system import TBSystem, build_system, electric_field_vector, params_from_input, read_input
+from .system import (TBSystem, build_system, electric_field_vector, params_from_input, read_initial_rho, read_input,
+                     set_reference_densities)
 
 
 @dataclass
@@ -36,6 +37,11 @@ class Deck:
         elements = {nm: os.path.join(d, nm) for nm in basis.type_names}
         sysm = build_system(basis, elements, p)
         p["efield"] = electric_field_vector(inp, sysm.a1, sysm.a2, sysm.a3)
+        # reference densities of elements with Un != 0 (the bulk run's initialrho_<element> file)
+        init = {t: os.path.join(d, f"initialrho_{nm}.dat") for t, nm in enumerate(basis.type_names)}
+        init = {t: f for t, f in init.items() if os.path.exists(f)}
+        if init:
+            set_reference_densities(sysm, {t: read_initial_rho(f, len(sysm.elements[t].orbs)) for t, f in init.items()})
         return cls.from_system(sysm, p, mesh)
 
     @classmethod

@@ -279,6 +279,34 @@ def params_from_input(inp: dict) -> dict:
     return p
 
 
+def read_initial_rho(path: str, norb: int):
+    """Reference densities of an element with Un != 0: rho0(nOrb), then rhod0, mpd0 (re, im), mzd0,
+    then Un, Um (the initialrho file of read_init_expecs, mod_initial_expectation.F90:473-534)."""
+    with open(path) as f:
+        vals = [float(x) for x in f.read().split()]
+    rho0 = np.array(vals[:norb])
+    rhod0, mpr, mpi, mzd0 = vals[norb:norb + 4]
+    return {"rho0": rho0, "rhod0": rhod0, "mpd0": complex(mpr, mpi), "mzd0": mzd0,
+            "Un": vals[norb + 4], "Um": vals[norb + 5]}
+
+
+def set_reference_densities(system: "TBSystem", per_element: dict):
+    """Per-site rho0 / rhod0 / mzd0 / mpd0 of the Hubbard term (mod_initial_expectation.F90:216-230) from
+    reference densities keyed by element (type index); elements without an entry keep zero (the
+    reference's Un = 0 case)."""
+    nat, nmax = system.n_atoms, max(system.norbs)
+    rho0 = np.zeros((nat, nmax))
+    rhod0, mzd0 = np.zeros(nat), np.zeros(nat)
+    mpd0 = np.zeros(nat, complex)
+    for i, t in enumerate(system.atom_type):
+        r = per_element.get(t)
+        if r is None:
+            continue
+        rho0[i, :len(r["rho0"])] = r["rho0"]
+        rhod0[i], mzd0[i], mpd0[i] = r["rhod0"], r["mzd0"], r["mpd0"]
+    system.rho0, system.rhod0, system.mzd0, system.mpd0 = rho0, rhod0, mzd0, mpd0
+
+
 def read_sc_file(path: str, norbs):
     """Self-consistency results file: n, mx, my, mz, delta per site, then Ef (mod_self_consistency.F90:341-389)."""
     vals = []

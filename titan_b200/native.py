@@ -45,6 +45,7 @@ SIGNATURES = {
     "tg_fermi_column": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
     "tg_dyson": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),
     "tg_set_green_method": (C.c_int, [C.c_void_p, C.c_int]),
+    "tg_ldos": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_double, _dp, _dp]),
     "tg_eig_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp]),
     "tg_she": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp,
                          _dp, C.c_int, _dp]),
@@ -326,6 +327,15 @@ class GreenGPU:
         self._check(self.lib.tg_dyson(self.h, n, _p(a.view(np.float64)), _p(u.view(np.float64)),
                                       _p(out.view(np.float64))))
         return out.T
+
+    def ldos(self, energies, eta):
+        """LDOS up / down [n_e, n_atoms, nOrbMax] on the real-axis BZ (ldos_energy, mod_LDOS.F90:95-150)."""
+        e = np.ascontiguousarray(energies, np.float64)
+        nat = self.system.n_atoms
+        up = np.zeros((e.shape[0], nat, self.nmax))
+        dn = np.zeros((e.shape[0], nat, self.nmax))
+        self._check(self.lib.tg_ldos(self.h, e.shape[0], _p(e), eta, _p(up), _p(dn)))
+        return up, dn
 
     def set_green_method(self, method):
         """"auto" (default): spectral Green functions for chi0 on tabulated meshes, Gauss-Jordan for the
