@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--compare-fp64", action="store_true", help="also time the FP64 path and report the ratio")
     ap.add_argument("--green", default="auto", choices=["auto", "gauss-jordan", "spectral"],
                     help="Green-function method (tg_set_green_method)")
-    ap.add_argument("--workload", default="chi0", choices=["chi0", "she"],
+    ap.add_argument("--workload", default="chi0", choices=["chi0", "she", "ldos"],
                     help="chi0: the susceptibility integral (headline); she: the disturbance integral "
                          "(eintshe) of the same mesh, one frequency per step")
     ap.add_argument("--small", action="store_true",
@@ -468,6 +468,79 @@ def run_she(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- local density of states
+LDOS_METRIC = "real-axis LDOS (k,E)-points/s on 1 B200 (FP64)"
+LDOS_ENERGIES = 1001
+
+
+def ldos_energies(deck):
+    s = deck.system
+    return s.Ef + np.linspace(-2.0, 1.0, LDOS_ENERGIES)
+
+
+def ldos_cpu_baseline(deck, h0, seconds_target=15.0):
+    """The oracle's ldos (numpy, all host threads) on a bounded sample: all k, the first energies."""
+    from oracle import titan_oracle as O
+    s = deck.system
+    m = O.Model(s, h0)
+    es = ldos_energies(deck)
+    t0 = time.perf_counter()
+    O.ldos(m, (deck.real_kp, deck.real_w), es[:1], s.eta)
+    rate = deck.real_kp.shape[0] / max(time.perf_counter() - t0, 1e-6)
+    ne = int(min(len(es), max(1, rate * seconds_target / deck.real_kp.shape[0])))
+    t0 = time.perf_counter()
+    O.ldos(m, (deck.real_kp, deck.real_w), es[:ne], s.eta)
+    dt = time.perf_counter() - t0
+    units = ne * deck.real_kp.shape[0]
+    cores = os.cpu_count()
+    return {"value": units / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle ldos (numpy/LAPACK, {cores} threads) on {ne} energies x {deck.real_kp.shape[0]} k of the "
+                      f"{s.name} real-axis BZ ({units} units, {dt:.1f} s)"}
+
+
+def run_ldos(args, rank, world, local_rank):
+    """One tg_ldos call per step: 1001 energies over the real-axis BZ (weak scaling over ranks)."""
+    import torch
+    from titan_b200.native import GreenGPU
+    torch.cuda.set_device(local_rank)
+    deck, h0, _, _ = workload(args.config, args.small)
+    s = deck.system
+    gpu = GreenGPU(local_rank)
+    gpu.setup(deck, h0)
+    gpu.set_green_method(args.green)
+    es = ldos_energies(deck)
+    nk = deck.real_kp.shape[0]
+    for _ in range(args.warmup):
+        gpu.ldos(es, s.eta)
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local_rank)
+    clk.start()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        gpu.ldos(es, s.eta)
+    stop.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier(world)
+    ms = allreduce_max(start.elapsed_time(stop), world)
+    units = allreduce_sum(len(es) * nk * args.steps, world)
+    line = {"metric": LDOS_METRIC, "value": units / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Slater-Koster model, no external data)",
+            "config": {"workload": f"{args.config}: dimH={s.dimH}, {nk} real-axis k x {len(es)} energies per step",
+                       "green": args.green,
+                       "timer": "CUDA events on the current stream around the blocking tg_ldos calls"},
+            "clocks": clocks}
+    if rank == 0 and not args.no_cpu and world == 1:
+        line["cpu_baseline"] = ldos_cpu_baseline(deck, h0)
+    gpu.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # --------------------------------------------------------------------------- distributed helpers
 def barrier(world):
     if world > 1:
@@ -513,6 +586,8 @@ def main():
     try:
         if args.workload == "she":
             run_she(args, rank, world, local_rank)
+        elif args.workload == "ldos":
+            run_ldos(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:
