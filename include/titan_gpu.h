@@ -173,6 +173,14 @@ int tg_she(tg_ctx* ctx, const double* q, double e, double Ef, double eta, double
            const double* x2, const double* p2, const double* efield, const double* prefactor,
            int dimens, double* tchi);
 
+/* Orbital-resolved on-site spin density of the sum rule: replaces calcSmunu
+ * (source/mod_sumrule.F90:162-245).  With A = sum_{k,E} w G(i, i) over the imaginary-axis
+ * mesh at Ef + i(y + eta) and imgXY(mu, nu) = (A(nu X, mu Y) + conj A(mu Y, nu X)) / 2 pi
+ * (+ 1/2 on the uu and dd diagonals):
+ *   S(mu, nu, 1, i) = imgud + imgdu,  S(:, :, 2, i) = i (imgud - imgdu),  S(:, :, 3, i) = imguu - imgdd,
+ * S(norb_max, norb_max, 3, n_atoms) complex (Smunuiivec).  Gauss-Jordan per point. */
+int tg_smunu(tg_ctx* ctx, double Ef, double eta, double* S);
+
 /* Local density of states on the real axis: replaces ldos_energy(e, ldosu, ldosd)
  * (source/mod_LDOS.F90:95-150) for n_e energies at once:
  *   ldosu(mu, i, ie) = -(1/pi) sum_k w_k Im G(i up mu, i up mu; k, e(ie) + i eta)

@@ -703,3 +703,85 @@ def ldos(model: Model, real_bz, energies, eta, chunk=4096):
                 up[ie, i, :n] -= w[sl] @ d[:, r0:r0 + n]
                 dn[ie, i, :n] -= w[sl] @ d[:, r0 + n:r0 + 2 * n]
     return up / PI, dn / PI
+
+
+# ---------------------------------------------------------------------------
+# Sum rule of the static transverse susceptibility, source/mod_sumrule.F90:10-245.
+# ---------------------------------------------------------------------------
+# spin (+, up, down, -) <-> cartesian (0, x, y, z) transforms, mod_constants.F90:34-44 (row index first)
+STOC = np.array([[0, 1, 1, 0], [0.5, 0, 0, 0.5], [-0.5j, 0, 0, 0.5j], [0, 0.5, -0.5, 0]], dtype=complex)
+CTOS = np.array([[0, 1, 1j, 0], [0.5, 0, 0, 1], [0.5, 0, 0, -1], [0, 1, -1j, 0]], dtype=complex)
+
+
+def _levi_civita():
+    e = np.zeros((3, 3, 3))
+    for a, b, c in ((0, 1, 2), (1, 2, 0), (2, 0, 1)):
+        e[a, b, c] = 1.0
+        e[a, c, b] = -1.0
+    return e
+
+
+def smunu(model: Model, mesh, Ef, eta, chunk=2048):
+    """calcSmunu (mod_sumrule.F90:162-245): S[i, k, mu, nu], k = x, y, z."""
+    s = model.system
+    ia = s.ia()
+    nmax = max(s.norbs)
+    blk = [np.zeros((2 * n, 2 * n), dtype=complex) for n in s.norbs]
+    y = mesh.point_energy()
+    for sl in _chunks(mesh.n_points, chunk):
+        G = model.green(Ef + 1j * (y[sl] + eta), mesh.kp[sl])
+        for i, n in enumerate(s.norbs):
+            r0 = ia[i][0]
+            blk[i] += np.einsum('p,pab->ab', mesh.weight[sl], G[:, r0:r0 + 2 * n, r0:r0 + 2 * n])
+    S = np.zeros((s.n_atoms, 3, nmax, nmax), dtype=complex)
+    for i, n in enumerate(s.norbs):
+        A = blk[i]
+
+        def img(sx, sy):
+            # img[mu, nu] = (A[nu X, mu Y] + conj(A[mu Y, nu X])) / 2 pi
+            ax = A[sx * n:(sx + 1) * n, sy * n:(sy + 1) * n]        # [nu, mu]
+            ay = A[sy * n:(sy + 1) * n, sx * n:(sx + 1) * n]        # [mu, nu]
+            return (ax.T + np.conj(ay)) / TPI
+        uu, dd, ud, du = img(0, 0), img(1, 1), img(0, 1), img(1, 0)
+        uu = uu + 0.5 * np.eye(n)
+        dd = dd + 0.5 * np.eye(n)
+        S[i, 0, :n, :n] = ud + du
+        S[i, 1, :n, :n] = (ud - du) * 1j
+        S[i, 2, :n, :n] = uu - dd
+    return S
+
+
+def beff_sumrule(system, mvec, lvec, lambda_p, lambda_d, porbs, dorbs, Um, hhw=None):
+    """Beffective (mod_sumrule.F90:111-160): Beff[dimens] on the cartesian rows sigma = x, y, z."""
+    sidx = system.sigmaimunu2i()
+    B = np.zeros(system.dimens, dtype=complex)
+    for i in range(system.n_atoms):
+        for sg in range(3):
+            for mu in dorbs[i]:
+                B[sidx[sg + 1, i, mu, mu]] -= 0.5 * Um[i] * mvec[i][sg]
+            if hhw is not None:
+                for mu in range(system.norbs[i]):
+                    B[sidx[sg + 1, i, mu, mu]] += hhw[i][sg]
+            for lam, orbl in ((lambda_p[i], porbs[i]), (lambda_d[i], dorbs[i])):
+                for nu in orbl:
+                    for mu in orbl:
+                        B[sidx[sg + 1, i, mu, nu]] += 0.5 * lam * lvec[i][sg, mu, nu]
+    return B
+
+
+def sumrule(system, chi_hf, S, B):
+    """sumrule (mod_sumrule.F90:10-107): lhs, rhs [group (i, mu, nu), m, n] and sum |lhs - rhs|;
+    groups run over the on-site orbital pairs in sigmaimunu2i order."""
+    sidx = system.sigmaimunu2i()
+    groups = [(i, mu, nu) for i in range(system.n_atoms) for mu in range(system.norbs[i])
+              for nu in range(system.norbs[i])]
+    IDX = np.array([[sidx[r, i, mu, nu] for r in range(4)] for (i, mu, nu) in groups])   # [group, spin]
+    # cart(p, q) = sum_{r, t} StoC(p, r) chi(r, t) CtoS(t, q) for every pair of groups
+    chi4 = chi_hf[IDX[:, :, None, None], IDX[None, None, :, :]]                     # [g, r, h, t]
+    cart = np.einsum('pr,grht,tq->gphq', STOC, chi4, CTOS)
+    eps = _levi_civita()
+    Sg = np.array([S[i, :, mu, nu] for (i, mu, nu) in groups])                       # [g, k]
+    lhs = np.einsum('mnk,gk->gmn', eps, Sg)
+    Bg = B[IDX]                                                                        # [h, spin]
+    rhs = 2.0 * np.einsum('nqp,gmhp,hq->gmn', eps, cart[:, 1:, :, 1:], Bg[:, 1:])
+    return lhs, rhs, float(np.sum(np.abs(lhs - rhs)))

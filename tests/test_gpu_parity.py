@@ -311,3 +311,22 @@ def test_spectral_green_equals_gauss_jordan(gpu, shape, nk, e, q, precision):
     assert rel(sp, gj) < (1e-12 if precision == "fp64" else 1e-10)
     ref = O.eintshechi(O.Model(s, h0), deck.ek, (deck.real_kp, deck.real_w), q, e, s.Ef, s.eta, s.etap, x2, p2)
     assert rel(sp, ref) < (1e-10 if precision == "fp64" else 1e-9)
+
+
+def test_smunu_and_sum_rule_on_fe_golden_state(gpu, fe_deck):
+    """calcSmunu on the GPU against the oracle, and the sum rule with the GPU's chi_HF(0, 0)."""
+    from titan_b200.host import response as R
+    from titan_b200.host import sumrule as SR
+    s = fe_deck.system
+    st = fe_deck.state
+    h0 = s.h0(st)
+    gpu.setup(fe_deck, h0)
+    S = gpu.smunu(s.Ef, s.eta)
+    ref = O.smunu(O.Model(s, h0), fe_deck.ek, s.Ef, s.eta)
+    assert np.max(np.abs(S - ref)) < 1e-12 * np.max(np.abs(ref))
+    chi = gpu.chi0(np.zeros(3), 0.0, s.Ef, s.eta, s.etap)
+    lvec, lpvec, lam_p, lam_d, porbs, dorbs, Um = R.site_parameters(s)
+    mvec = [[st.mx[i][dorbs[i]].sum(), st.my[i][dorbs[i]].sum(), st.mz[i][dorbs[i]].sum()] for i in range(s.n_atoms)]
+    B = SR.effective_field(s, mvec, lvec, lam_p, lam_d, porbs, dorbs, Um)
+    lhs, rhs, diff = SR.check(s, chi, S, B)
+    assert diff < 1e-9 * np.abs(lhs).max()

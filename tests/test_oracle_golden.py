@@ -157,3 +157,24 @@ def test_nb_ldos_matches_golden():
         np.testing.assert_allclose(ours[:, 0], summed[:, 2], rtol=2e-9, atol=0)
         np.testing.assert_allclose(ours[:, 1:4].sum(1), summed[:, 3], rtol=2e-9, atol=0)
         np.testing.assert_allclose(ours[:, 4:].sum(1), summed[:, 4], rtol=2e-9, atol=0)
+
+
+def test_fe_sum_rule_holds_and_host_matches_oracle(fe_deck):
+    """mod_sumrule restated: at the golden Fe state the static transverse chi_HF(q = 0, omega = 0)
+    and the on-site spin density satisfy the sum rule (the reference prints YES below 1e-5; here it
+    holds to roundoff), and the host-side algebra equals the oracle's."""
+    from titan_b200.host import response as R
+    from titan_b200.host import sumrule as SR
+    s = fe_deck.system
+    st = fe_deck.state
+    m = O.Model(s, s.h0(st))
+    chi = O.eintshechi(m, fe_deck.ek, (fe_deck.real_kp, fe_deck.real_w), np.zeros(3), 0.0, s.Ef, s.eta, s.etap)
+    S = O.smunu(m, fe_deck.ek, s.Ef, s.eta)
+    lvec, lpvec, lam_p, lam_d, porbs, dorbs, Um = R.site_parameters(s)
+    mvec = [[st.mx[i][dorbs[i]].sum(), st.my[i][dorbs[i]].sum(), st.mz[i][dorbs[i]].sum()] for i in range(s.n_atoms)]
+    B = O.beff_sumrule(s, mvec, lvec, lam_p, lam_d, porbs, dorbs, Um)
+    np.testing.assert_allclose(SR.effective_field(s, mvec, lvec, lam_p, lam_d, porbs, dorbs, Um), B, rtol=0, atol=1e-15)
+    lo, ro, diff = O.sumrule(s, chi, S, B)
+    assert diff < 1e-10 * np.abs(lo).max()
+    lh, rh, dh = SR.check(s, chi, S, B)
+    assert np.abs(lh - lo).max() <= 1e-14 and np.abs(rh - ro).max() <= 1e-13

@@ -1286,6 +1286,80 @@ int tg_eig_batch(tg_ctx* c, int64_t nk, const double* kp, double* lam, double* U
   return read_eig_status(c);
 }
 
+int tg_smunu(tg_ctx* c, double Ef, double eta, double* S) {
+  int rc = check_ready(c, true, false);
+  if (rc) return rc;
+  if (!S) return set_err(c, TG_ERR_ARG, "tg_smunu: null output");
+  if (!green_supported(c->dimH)) return set_err(c, TG_ERR_ARG, "tg_smunu: dimH has no accumulating kernel");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int nat = c->n_atoms, nmax = c->nmax;
+  // entries (r, c) of every on-site block, site by site, row-major inside the 2n x 2n block
+  std::vector<int> desc, site_off(nat + 1, 0);
+  for (int i = 0; i < nat; ++i) {
+    const int n2 = 2 * c->norb[i];
+    for (int x = 0; x < n2; ++x)
+      for (int y = 0; y < n2; ++y) {
+        desc.push_back(c->ia[i] + x);
+        desc.push_back(c->ia[i] + y);
+      }
+    site_off[i + 1] = site_off[i] + n2 * n2;
+  }
+  const int acc_len = site_off[nat];
+  TG_CHECK(c, c->d_gg_desc.upload(desc.data(), desc.size(), s), "upload");
+  GreenArgs a = base_args(c);
+  a.pts.kind = 0;
+  a.pts.y = c->d_y.p;
+  a.pts.kp = c->d_kp.p;
+  a.pts.w = c->d_w.p;
+  a.np = c->n_imag;
+  a.zr = Ef;
+  a.zi = eta;
+  a.mode = MODE_ENTRIES;
+  a.gg_desc = c->d_gg_desc.p;
+  a.acc_len = acc_len;
+  const int maxgrid = green_acc_ctas(c->dimH, c->n_imag, c->num_sms);
+  TG_CHECK(c, c->d_acc.ensure((size_t)maxgrid * acc_len), "alloc acc");
+  TG_CHECK(c, c->d_acc_red.ensure(acc_len), "alloc acc");
+  a.acc = c->d_acc.p;
+  c->gg_mode = -1;   // the entry list replaced the GG descriptors
+  if ((rc = reset_status(c))) return rc;
+  int grid = 0;
+  TG_CHECK(c, launch_green(a, c->num_sms, s, &grid), "green (on-site blocks)");
+  TG_CHECK(c, launch_reduce_blocks(c->d_acc.p, grid, acc_len, c->d_acc_red.p, s), "reduce");
+  std::vector<double2> h(acc_len);
+  TG_CHECK(c, cudaMemcpyAsync(h.data(), c->d_acc_red.p, sizeof(double2) * acc_len, cudaMemcpyDeviceToHost, s), "copy");
+  if ((rc = read_status(c))) return rc;
+  // calcSmunu: imgXY(mu, nu) = (A(nu X, mu Y) + conj(A(mu Y, nu X))) / 2 pi, 1/2 on the uu / dd diagonals
+  const double tpi = 2.0 * kPi;
+  std::fill(S, S + (size_t)2 * nmax * nmax * 3 * nat, 0.0);
+  for (int i = 0; i < nat; ++i) {
+    const int n = c->norb[i], n2 = 2 * n;
+    auto A = [&](int x, int y) { return h[site_off[i] + x * n2 + y]; };
+    auto img = [&](int sx, int sy, int mu, int nu) {   // spins sx (row of nu), sy (column of mu)
+      const double2 p = A(sx * n + nu, sy * n + mu), q = A(sy * n + mu, sx * n + nu);
+      return make_double2((p.x + q.x) / tpi, (p.y - q.y) / tpi);
+    };
+    for (int mu = 0; mu < n; ++mu)
+      for (int nu = 0; nu < n; ++nu) {
+        double2 uu = img(0, 0, mu, nu), dd = img(1, 1, mu, nu);
+        const double2 ud = img(0, 1, mu, nu), du = img(1, 0, mu, nu);
+        if (mu == nu) {
+          uu.x += 0.5;
+          dd.x += 0.5;
+        }
+        const double2 k1 = cadd(ud, du), k2 = cmul(make_double2(0.0, 1.0), csub(ud, du)), k3 = csub(uu, dd);
+        const double2 ks[3] = {k1, k2, k3};
+        for (int k = 0; k < 3; ++k) {
+          const size_t o = (size_t)mu + (size_t)nmax * (nu + (size_t)nmax * (k + 3 * (size_t)i));
+          S[2 * o] = ks[k].x;
+          S[2 * o + 1] = ks[k].y;
+        }
+      }
+  }
+  return TG_OK;
+}
+
 int tg_ldos(tg_ctx* c, int n_e, const double* e, double eta, double* ldosu, double* ldosd) {
   int rc = check_ready(c, false, true);
   if (rc) return rc;

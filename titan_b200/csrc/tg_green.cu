@@ -417,6 +417,18 @@ __global__ void __launch_bounds__(kMaxThreads, 1) green_gj_kernel(GreenArgs a, i
         accum[4 * o + 2] = cadd(accum[4 * o + 2], s2);
         accum[4 * o + 3] = cadd(accum[4 * o + 3], s3);
       }
+    } else if (a.mode == MODE_ENTRIES) {
+      // acc[e] += w * G(r_e, c_e) for the entry list (r_e, c_e) = gg_desc[2e], gg_desc[2e + 1]
+      for (int e = tid; e < a.acc_len; e += nthreads) {
+        const int r = a.gg_desc[2 * e], c = a.gg_desc[2 * e + 1];
+        double2 sum = make_double2(0, 0);
+        for (int mm = 0; mm < mpb; ++mm) {
+          const double* zq = zw + 8 * mm;
+          if (zq[6] == 0.0) continue;
+          sum = cfma(make_double2(zq[5], 0.0), ginv(Xs + (size_t)mm * NN, piv + mm * N, pinv + mm * N, N, r, c), sum);
+        }
+        accum[e] = cadd(accum[e], sum);
+      }
     }
     __syncthreads();
   }
@@ -430,7 +442,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) green_gj_kernel(GreenArgs a, i
       dst[4 * tid + 2] = ex_ud;
       dst[4 * tid + 3] = ex_du;
     }
-  } else if (a.mode == MODE_GG || a.mode == MODE_DIAG4) {
+  } else if (a.mode == MODE_GG || a.mode == MODE_DIAG4 || a.mode == MODE_ENTRIES) {
     double2* dst = a.acc + (size_t)blockIdx.x * a.acc_len;
     for (int e = tid; e < a.acc_len; e += nthreads) dst[e] = accum[e];
   }

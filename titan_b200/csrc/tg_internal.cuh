@@ -83,6 +83,7 @@ enum GreenMode : int {
   MODE_GG = 6,        // accumulate the orbital-diagonal GG tensor (Jacobian)
   MODE_DIAG4 = 7,     // accumulate w * sigma-traces of diagonal orbitals (Fermi column)
   MODE_HK = 8,        // H(k) only (no inversion), column-major per point
+  MODE_ENTRIES = 9,   // accumulate w * G(r_e, c_e) for a list of entries (gg_desc pairs, acc_len of them)
 };
 
 // A set of (k, z) points.  kind 0: flattened imaginary-axis list (y, kp, w per

@@ -46,6 +46,7 @@ SIGNATURES = {
     "tg_dyson": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),
     "tg_set_green_method": (C.c_int, [C.c_void_p, C.c_int]),
     "tg_ldos": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_double, _dp, _dp]),
+    "tg_smunu": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
     "tg_eig_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp]),
     "tg_she": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp,
                          _dp, C.c_int, _dp]),
@@ -327,6 +328,13 @@ class GreenGPU:
         self._check(self.lib.tg_dyson(self.h, n, _p(a.view(np.float64)), _p(u.view(np.float64)),
                                       _p(out.view(np.float64))))
         return out.T
+
+    def smunu(self, Ef, eta):
+        """Smunuiivec as [n_atoms, 3, nOrbMax(mu), nOrbMax(nu)] (calcSmunu, mod_sumrule.F90:162-245)."""
+        nat = self.system.n_atoms
+        S = np.zeros((nat, 3, self.nmax, self.nmax), np.complex128)   # Fortran (mu, nu, 3, nat) read back
+        self._check(self.lib.tg_smunu(self.h, Ef, eta, _p(S.view(np.float64))))
+        return np.swapaxes(S, 2, 3)
 
     def ldos(self, energies, eta):
         """LDOS up / down [n_e, n_atoms, nOrbMax] on the real-axis BZ (ldos_energy, mod_LDOS.F90:95-150)."""
