@@ -173,6 +173,19 @@ int tg_she(tg_ctx* ctx, const double* q, double e, double Ef, double eta, double
            const double* x2, const double* p2, const double* efield, const double* prefactor,
            int dimens, double* tchi);
 
+/* Linear-SOC susceptibility: replaces eintshechilinearsoc(q, e) (source/eintshechi.F90:182-414).
+ * The context's h0 (tg_set_h0) must be the Hamiltonian without the local spin-orbit blocks
+ * and vsoc(dimH, dimH) complex those blocks (the hk / vsoc split of hamiltklinearsoc,
+ * mod_hamiltonian.F90:304-396).  With G0 = (z - h0 - H(k))^-1:
+ *   chiorb_hf(dimens, dimens)   chi0_HF of G0 (as tg_chi0 with that h0),
+ *   chiorb_lsoc(dimens, dimens) chi(G0 V G0 (k+q, E+e), G0(k, E)) + chi(G0(k+q, E+e), G0 V G0 (k, E)),
+ * both divided by 2 pi.  The real-axis part runs over all n_real energies (the reference's
+ * loop stops after the first energy's k points, eintshechi.F90:321).  FP64, Gauss-Jordan per
+ * point; dimH up to 68 (3 dimH^2 complex of shared memory). */
+int tg_chi0_linear_soc(tg_ctx* ctx, const double* q, double e, double Ef, double eta, double etap,
+                       int n_real, const double* x2, const double* p2, const double* vsoc, int dimens,
+                       double* chiorb_hf, double* chiorb_lsoc);
+
 /* Orbital-resolved on-site spin density of the sum rule: replaces calcSmunu
  * (source/mod_sumrule.F90:162-245).  With A = sum_{k,E} w G(i, i) over the imaginary-axis
  * mesh at Ef + i(y + eta) and imgXY(mu, nu) = (A(nu X, mu Y) + conj A(mu Y, nu X)) / 2 pi

@@ -105,6 +105,60 @@ def _chunks(P, size):
         yield slice(s, min(P, s + size))
 
 
+def _scatter_fn(s):
+    sidx = s.sigmaimunu2i()
+    norbs = s.norbs
+
+    def scatter(target, i, j, s1, s2, block):
+        # block[mu, nu, gama, xi] -> target[sigmaimunu2i(s1,i,mu,nu), sigmaimunu2i(s2,j,gama,xi)]
+        ni, nj = norbs[i], norbs[j]
+        rows = sidx[s1 - 1, i, :ni, :ni].reshape(-1)
+        cols = sidx[s2 - 1, j, :nj, :nj].reshape(-1)
+        target[np.ix_(rows, cols)] += block.reshape(ni * ni, nj * nj)
+    return scatter
+
+
+def _imag_terms(s, g1, g2, w, target, scatter):
+    """Imaginary-axis integrand of eintshechi.F90:86-104 for G1 = g1, G2 = g2 (weights w), added to target."""
+    ia = s.ia()
+    norbs = s.norbs
+    for j in range(s.n_atoms):
+        for i in range(s.n_atoms):
+            for (s1, s2), (x1, y1) in TERM1.items():
+                a = _blk(g1, ia, norbs, i, j, x1) * w[:, None, None]   # [P, nu, gama]
+                b = _blk(g2, ia, norbs, j, i, y1)                      # [P, xi, mu]
+                t1 = np.einsum("pvg,pxm->mvgx", a, b, optimize=True)
+                x2s, y2s = TERM2[(s1, s2)]
+                c = _blk(g2, ia, norbs, i, j, x2s) * w[:, None, None]  # [P, mu, xi]
+                d = _blk(g1, ia, norbs, j, i, y2s)                     # [P, gama, nu]
+                t2 = np.conj(np.einsum("pmx,pgv->mvgx", c, d, optimize=True))
+                scatter(target, i, j, s1, s2, t1 + t2)
+
+
+def _real_terms(s, g1, g2, w, target, scatter):
+    """Real-axis integrand of eintshechi.F90:146-164 for G1 = g1, G2 = g2 (weights w), added to target."""
+    ia = s.ia()
+    norbs = s.norbs
+    for j in range(s.n_atoms):
+        for i in range(s.n_atoms):
+            for (s1, s2), (a1, a2, b1) in REAL.items():
+                A = _blk(g1, ia, norbs, i, j, a1) - np.conj(np.swapaxes(_blk(g1, ia, norbs, j, i, a2), 1, 2))
+                A = A * w[:, None, None]                           # [P, nu, gama]
+                B = np.conj(_blk(g2, ia, norbs, i, j, b1))          # [P, mu, xi]
+                blk = -1j * np.einsum("pvg,pmx->mvgx", A, B, optimize=True)
+                scatter(target, i, j, s1, s2, blk)
+
+
+def _real_list(real_bz, x2, p2):
+    """Every (energy, k) pair of the real-axis loops (eintshechi.F90:112-170) as one flat list."""
+    kpr, wr = real_bz
+    nkr = kpr.shape[0]
+    xs = np.repeat(np.asarray(x2, float), nkr)
+    ws = np.repeat(np.asarray(p2, float), nkr) * np.tile(wr, len(x2))
+    ks = np.tile(kpr, (len(x2), 1))
+    return xs, ws, ks
+
+
 def eintshechi(model: Model, mesh, real_bz, q, e, Ef, eta, etap, x2=None, p2=None, chunk=4096):
     """chi0_HF(q, e) of eintshechi.F90:2-178 (before the MPI reduction).
 
@@ -113,62 +167,61 @@ def eintshechi(model: Model, mesh, real_bz, q, e, Ef, eta, etap, x2=None, p2=Non
     with generate_real_epoints).  Returns chiorb_hf[dimens, dimens].
     """
     s = model.system
-    ia = s.ia()
-    norbs = s.norbs
-    nat = s.n_atoms
-    sidx = s.sigmaimunu2i()
     D = s.dimens
     chi = np.zeros((D, D), dtype=complex)
     fint = np.zeros((D, D), dtype=complex)
     q = np.asarray(q, float)
+    scatter = _scatter_fn(s)
+    y = mesh.point_energy()
+    for sl in _chunks(mesh.n_points, chunk):
+        kp = mesh.kp[sl]
+        g1 = model.green(Ef + e + 1j * (y[sl] + eta), kp + q[None, :])   # gfq
+        g2 = model.green(Ef + 1j * (y[sl] + etap), kp)                   # gf
+        _imag_terms(s, g1, g2, mesh.weight[sl], chi, scatter)
+    if x2 is not None and len(x2) > 0:
+        xs, ws, ks = _real_list(real_bz, x2, p2)
+        for sl in _chunks(xs.shape[0], chunk):
+            g1 = model.green(xs[sl] + e + 1j * eta, ks[sl] + q[None, :])
+            g2 = model.green(xs[sl] + 1j * etap, ks[sl])
+            _real_terms(s, g1, g2, ws[sl], fint, scatter)
+    return (chi + fint) / TPI
 
-    def scatter(target, i, j, s1, s2, block):
-        # block[mu, nu, gama, xi] -> target[sigmaimunu2i(s1,i,mu,nu), sigmaimunu2i(s2,j,gama,xi)]
-        ni, nj = norbs[i], norbs[j]
-        rows = sidx[s1 - 1, i, :ni, :ni].reshape(-1)
-        cols = sidx[s2 - 1, j, :nj, :nj].reshape(-1)
-        target[np.ix_(rows, cols)] += block.reshape(ni * ni, nj * nj)
 
+def eintshechi_linear_soc(model0: Model, vsoc, mesh, real_bz, q, e, Ef, eta, etap, x2=None, p2=None, chunk=2048):
+    """eintshechilinearsoc (eintshechi.F90:182-414): chi_HF of G0 = (z - H0)^-1, H0 the
+    Hamiltonian without the local SOC (hamiltklinearsoc, mod_hamiltonian.F90:304-396), and its
+    first-order SOC correction
+        chi_lsoc = chi(G0 V G0 (k+q, E+e), G0(k, E)) + chi(G0(k+q, E+e), G0 V G0 (k, E)),  V = vsoc
+    (greenlinearsoc, mod_greenfunction.F90:141-202).  Returns (chiorb_hf, chiorb_hflsoc).
+    The real-axis sum runs over every real point; the reference's loop stops after
+    realBZ%workload points (the first real energy only, eintshechi.F90:321)."""
+    s = model0.system
+    D = s.dimens
+    V = np.asarray(vsoc, complex)
+    chi = np.zeros((D, D), dtype=complex)
+    lsoc = np.zeros((D, D), dtype=complex)
+    q = np.asarray(q, float)
+    scatter = _scatter_fn(s)
     y = mesh.point_energy()
     for sl in _chunks(mesh.n_points, chunk):
         kp = mesh.kp[sl]
         w = mesh.weight[sl]
-        ep = y[sl]
-        g1 = model.green(Ef + e + 1j * (ep + eta), kp + q[None, :])   # gfq
-        g2 = model.green(Ef + 1j * (ep + etap), kp)                   # gf
-        for j in range(nat):
-            for i in range(nat):
-                for (s1, s2), (x1, y1) in TERM1.items():
-                    a = _blk(g1, ia, norbs, i, j, x1) * w[:, None, None]   # [P, nu, gama]
-                    b = _blk(g2, ia, norbs, j, i, y1)                      # [P, xi, mu]
-                    t1 = np.einsum("pvg,pxm->mvgx", a, b, optimize=True)
-                    x2s, y2s = TERM2[(s1, s2)]
-                    c = _blk(g2, ia, norbs, i, j, x2s) * w[:, None, None]  # [P, mu, xi]
-                    d = _blk(g1, ia, norbs, j, i, y2s)                     # [P, gama, nu]
-                    t2 = np.conj(np.einsum("pmx,pgv->mvgx", c, d, optimize=True))
-                    scatter(chi, i, j, s1, s2, t1 + t2)
+        g1 = model0.green(Ef + e + 1j * (y[sl] + eta), kp + q[None, :])
+        g2 = model0.green(Ef + 1j * (y[sl] + etap), kp)
+        v1, v2 = g1 @ V @ g1, g2 @ V @ g2
+        _imag_terms(s, g1, g2, w, chi, scatter)
+        _imag_terms(s, v1, g2, w, lsoc, scatter)
+        _imag_terms(s, g1, v2, w, lsoc, scatter)
     if x2 is not None and len(x2) > 0:
-        # every (energy, k) pair of the real-axis loops (eintshechi.F90:112-170) as one flat list
-        kpr, wr = real_bz
-        nkr = kpr.shape[0]
-        xs = np.repeat(np.asarray(x2, float), nkr)
-        ws = np.repeat(np.asarray(p2, float), nkr) * np.tile(wr, len(x2))
-        ks = np.tile(kpr, (len(x2), 1))
+        xs, ws, ks = _real_list(real_bz, x2, p2)
         for sl in _chunks(xs.shape[0], chunk):
-            if True:
-                kp = ks[sl]
-                w = ws[sl]
-                g1 = model.green(xs[sl] + e + 1j * eta, kp + q[None, :])
-                g2 = model.green(xs[sl] + 1j * etap, kp)
-                for j in range(nat):
-                    for i in range(nat):
-                        for (s1, s2), (a1, a2, b1) in REAL.items():
-                            A = _blk(g1, ia, norbs, i, j, a1) - np.conj(np.swapaxes(_blk(g1, ia, norbs, j, i, a2), 1, 2))
-                            A = A * w[:, None, None]                           # [P, nu, gama]
-                            B = np.conj(_blk(g2, ia, norbs, i, j, b1))          # [P, mu, xi]
-                            blk = -1j * np.einsum("pvg,pmx->mvgx", A, B, optimize=True)
-                            scatter(fint, i, j, s1, s2, blk)
-    return (chi + fint) / TPI
+            g1 = model0.green(xs[sl] + e + 1j * eta, ks[sl] + q[None, :])
+            g2 = model0.green(xs[sl] + 1j * etap, ks[sl])
+            v1, v2 = g1 @ V @ g1, g2 @ V @ g2
+            _real_terms(s, g1, g2, ws[sl], chi, scatter)
+            _real_terms(s, v1, g2, ws[sl], lsoc, scatter)
+            _real_terms(s, g1, v2, ws[sl], lsoc, scatter)
+    return chi / TPI, lsoc / TPI
 
 
 def umatrix(system):

@@ -330,3 +330,23 @@ def test_smunu_and_sum_rule_on_fe_golden_state(gpu, fe_deck):
     B = SR.effective_field(s, mvec, lvec, lam_p, lam_d, porbs, dorbs, Um)
     lhs, rhs, diff = SR.check(s, chi, S, B)
     assert diff < 1e-9 * np.abs(lhs).max()
+
+
+@pytest.mark.parametrize("shape,nk,e,q", [
+    ("bcc1", (3, 3, 3), 0.0, (0, 0, 0)),
+    ("bcc1", (3, 3, 3), 0.03, (0.1, 0.0, 0.2)),
+    ("sq2", (4, 4, 1), 0.05, (0.05, 0.02, 0.0)),
+])
+def test_chi0_linear_soc_matches_oracle(gpu, shape, nk, e, q):
+    """eintshechilinearsoc on the GPU: chi_HF of H0 and the linear-SOC correction vs the oracle."""
+    deck = synthetic.make_deck(shape, nk=nk, n1gl=6, parts=1, n3gl=4)
+    s = deck.system
+    h00, V = s.linear_soc_split(initial_state(s))
+    gpu.setup(deck, h00)
+    x2, p2 = deck.real_points(e, s.Ef)
+    q = np.array(q, float)
+    chi, lsoc = gpu.chi0_linear_soc(q, e, s.Ef, s.eta, s.etap, x2, p2, V)
+    rchi, rl = O.eintshechi_linear_soc(O.Model(s, h00), V, deck.ek, (deck.real_kp, deck.real_w), q, e, s.Ef, s.eta,
+                                       s.etap, x2, p2)
+    assert rel(chi, rchi) < 1e-10
+    assert rel(lsoc, rl) < 1e-10

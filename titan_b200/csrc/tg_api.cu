@@ -121,6 +121,8 @@ struct tg_ctx {
   DevArray<double> d_eigL[4];
   DevArray<int> d_outinv, d_eig_status;
   DevArray<double> d_ldos_e, d_ldos;
+  // linear SOC: V, G V G of both Green functions, four operands, chi_lsoc partials
+  DevArray<double2> d_vsoc, d_lsb[6], d_Cl, d_Dl;
   // disturbance response (eintshe)
   DevArray<int> d_she_tab, d_ia;
   DevArray<double2> d_she_part, d_she_sum, d_she_pref, d_she_out;
@@ -1284,6 +1286,125 @@ int tg_eig_batch(tg_ctx* c, int64_t nk, const double* kp, double* lam, double* U
   TG_CHECK(c, cudaMemcpyAsync(lam, c->d_eigL[0].p, sizeof(double) * nk * c->dimH, cudaMemcpyDeviceToHost, s), "copy");
   TG_CHECK(c, cudaMemcpyAsync(U, c->d_eigU[0].p, sizeof(double2) * nk * nn, cudaMemcpyDeviceToHost, s), "copy");
   return read_eig_status(c);
+}
+
+int tg_chi0_linear_soc(tg_ctx* c, const double* q, double e, double Ef, double eta, double etap, int n_real,
+                       const double* x2, const double* p2, const double* vsoc, int dimens, double* chiorb_hf,
+                       double* chiorb_lsoc) {
+  int rc = check_ready(c, true, false);
+  if (rc) return rc;
+  if (!q || !vsoc || !chiorb_hf || !chiorb_lsoc) return set_err(c, TG_ERR_ARG, "tg_chi0_linear_soc: null argument");
+  if (dimens != c->dimens) return set_err(c, TG_ERR_ARG, "tg_chi0_linear_soc: dimens mismatch");
+  const bool real = std::fabs(e) >= 1e-15;
+  if (real && (n_real <= 0 || !x2 || !p2)) return set_err(c, TG_ERR_ARG, "tg_chi0_linear_soc: real-axis points missing");
+  if (real && !c->real_set) return set_err(c, TG_ERR_STATE, "tg_set_real_mesh has not been called");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int n = c->dimH;
+  const int64_t nn = (int64_t)n * n;
+  {
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    if (gvg_smem_bytes(n) > (size_t)optin)
+      return set_err(c, TG_ERR_ARG, "tg_chi0_linear_soc: dimH too large for the G V G kernel (3 dimH^2 complex in shared memory)");
+  }
+  const int64_t cstride = (int64_t)c->dimens * c->dimens;
+  const int nsplit = nsplit_for(c);
+  // eight P x dimH^2 buffers per pass: P a quarter of the chi0 pass
+  int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, real ? (int64_t)n_real * c->n_realk : 0)) / 4;
+  P = std::max<int64_t>(64, (P / 64) * 64);
+  TG_CHECK(c, c->d_A.ensure((size_t)P * nn), "alloc");
+  TG_CHECK(c, c->d_B.ensure((size_t)P * nn), "alloc");
+  for (int k = 0; k < 6; ++k) TG_CHECK(c, c->d_lsb[k].ensure((size_t)P * nn), "alloc");
+  TG_CHECK(c, c->d_vsoc.upload(reinterpret_cast<const double2*>(vsoc), (size_t)nn, s), "upload V");
+  DevArray<double2>* parts[4] = {&c->d_C, &c->d_D, &c->d_Cl, &c->d_Dl};
+  for (auto* d : parts) {
+    TG_CHECK(c, d->ensure((size_t)nsplit * cstride), "alloc partials");
+    TG_CHECK(c, cudaMemsetAsync(d->p, 0, sizeof(double2) * nsplit * cstride, s), "memset");
+  }
+  TG_CHECK(c, c->d_chi.ensure((size_t)cstride), "alloc chi");
+  if (real) {
+    TG_CHECK(c, c->d_x2.upload(x2, n_real, s), "upload x2");
+    TG_CHECK(c, c->d_p2.upload(p2, n_real, s), "upload p2");
+  }
+  if ((rc = reset_status(c))) return rc;
+  profile_begin(c);
+  double2 *X1 = c->d_lsb[0].p, *X2 = c->d_lsb[1].p, *oA = c->d_lsb[2].p, *oB = c->d_lsb[3].p, *oAx = c->d_lsb[4].p,
+          *oBx = c->d_lsb[5].p;
+  auto pass = [&](GreenArgs g, bool real_axis, double2* C, double2* Cl) -> int {
+    // G2 = G0(k, E), G1 = G0(k + q, E + e) column-major; X = G V G of both
+    g.mode = MODE_RAW;
+    g.out = c->d_B.p;
+    {
+      KindTimer kt(c, 0);
+      TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), "green (G2)");
+    }
+    g.zr += e;
+    g.zi = eta;
+    g.q[0] = q[0];
+    g.q[1] = q[1];
+    g.q[2] = q[2];
+    g.out = c->d_A.p;
+    {
+      KindTimer kt(c, 0);
+      TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), "green (G1)");
+    }
+    c->launches += 6;
+    TG_CHECK(c, launch_gvg(c->d_A.p, c->d_vsoc.p, n, g.np, X1, c->num_sms, s), "G V G (1)");
+    TG_CHECK(c, launch_gvg(c->d_B.p, c->d_vsoc.p, n, g.np, X2, c->num_sms, s), "G V G (2)");
+    const int ma = real_axis ? MODE_A_REAL : MODE_A_IMAG, mb = real_axis ? MODE_B_REAL : MODE_B_IMAG;
+    TG_CHECK(c, launch_operand(c->d_A.p, n, g.np, g.p0, g.pts, ma, c->d_outmap.p, oA, c->num_sms, s), "operand");
+    TG_CHECK(c, launch_operand(c->d_B.p, n, g.np, g.p0, g.pts, mb, c->d_outmap.p, oB, c->num_sms, s), "operand");
+    TG_CHECK(c, launch_operand(X1, n, g.np, g.p0, g.pts, ma, c->d_outmap.p, oAx, c->num_sms, s), "operand");
+    TG_CHECK(c, launch_operand(X2, n, g.np, g.p0, g.pts, mb, c->d_outmap.p, oBx, c->num_sms, s), "operand");
+    KindTimer kt(c, 1);
+    if ((rc = contract(c, oA, oB, g.np, C, nsplit, cstride))) return rc;
+    if ((rc = contract(c, oAx, oB, g.np, Cl, nsplit, cstride))) return rc;
+    return contract(c, oA, oBx, g.np, Cl, nsplit, cstride);
+  };
+  const GreenArgs base = base_args(c);
+  for (int64_t p0 = 0; p0 < c->n_imag; p0 += P) {
+    GreenArgs g = base;
+    g.pts.kind = 0;
+    g.pts.y = c->d_y.p;
+    g.pts.kp = c->d_kp.p;
+    g.pts.w = c->d_w.p;
+    g.p0 = p0;
+    g.np = std::min<int64_t>(P, c->n_imag - p0);
+    g.zr = Ef;
+    g.zi = etap;
+    if ((rc = pass(g, false, c->d_C.p, c->d_Cl.p))) return rc;
+  }
+  if (real) {
+    const int64_t ntot = (int64_t)n_real * c->n_realk;
+    for (int64_t p0 = 0; p0 < ntot; p0 += P) {
+      GreenArgs g = base;
+      g.pts.kind = 1;
+      g.pts.kp = c->d_rkp.p;
+      g.pts.w = c->d_rw.p;
+      g.pts.x2 = c->d_x2.p;
+      g.pts.p2 = c->d_p2.p;
+      g.pts.nk = c->n_realk;
+      g.p0 = p0;
+      g.np = std::min<int64_t>(P, ntot - p0);
+      g.zr = 0.0;
+      g.zi = etap;
+      if ((rc = pass(g, true, c->d_D.p, c->d_Dl.p))) return rc;
+    }
+  }
+  double* outs[2] = {chiorb_hf, chiorb_lsoc};
+  DevArray<double2>* cs[2][2] = {{&c->d_C, &c->d_D}, {&c->d_Cl, &c->d_Dl}};
+  for (int k = 0; k < 2; ++k) {
+    {
+      KindTimer kt(c, 2);
+      TG_CHECK(c, launch_chi_epilogue(cs[k][0]->p, cs[k][1]->p, nsplit, cstride, c->dimens, c->d_decode.p, c->d_norb.p,
+                                      c->d_pair_coff.p, c->n_atoms, 1.0 / (2.0 * kPi), c->d_chi.p, s),
+               "epilogue");
+    }
+    TG_CHECK(c, cudaMemcpyAsync(outs[k], c->d_chi.p, sizeof(double2) * cstride, cudaMemcpyDeviceToHost, s), "copy");
+  }
+  profile_end(c);
+  return read_status(c);
 }
 
 int tg_smunu(tg_ctx* c, double Ef, double eta, double* S) {

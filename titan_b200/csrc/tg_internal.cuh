@@ -180,6 +180,13 @@ cudaError_t launch_spec_ldos(const double2* U, const double* lam, const double* 
 cudaError_t launch_green_spectral(const GreenArgs& g, const double2* U, const double* lam, const int* outinv,
                                   int num_sms, cudaStream_t s);
 
+// Linear SOC: X_p = G_p V G_p, and a column-major G_p into a pair-block operand layout
+size_t gvg_smem_bytes(int n);
+cudaError_t launch_gvg(const double2* G, const double2* V, int n, int64_t np, double2* X, int num_sms,
+                       cudaStream_t s);
+cudaError_t launch_operand(const double2* G, int n, int64_t np, int64_t p0, const PointSet& pts, int mode,
+                           const int* outmap, double2* out, int num_sms, cudaStream_t s);
+
 // Disturbance-response vertex (eintshe): one launch per pass over RAW G1 / G2
 struct SheLaunch {
   const GreenArgs* g = nullptr;   // system tables (n, neighbours, hopping blocks)

@@ -168,6 +168,18 @@ class TBSystem:
         onsite = [self.elements[t].onsite.astype(complex) for t in self.atom_type]
         return O.assemble_h0(self.norbs, onsite, self.local_blocks(state))
 
+    def linear_soc_split(self, state: MagState, soc_theta: float = 0.0, soc_phi: float = 0.0):
+        """(h0 without the local SOC, V = the SOC blocks) with h0(state) = h0_0 + V, the split of
+        hamiltklinearsoc (mod_hamiltonian.F90:304-396) for the linear-SOC susceptibility."""
+        h0 = self.h0(state)
+        V = np.zeros_like(h0)
+        ia = O.site_offsets(self.norbs)
+        for i, t in enumerate(self.atom_type):
+            el = self.elements[t]
+            b0, b3 = ia[i][0], ia[i][3]
+            V[b0:b3, b0:b3] = O.ls_matrix(el.orbs, el.lambda_p, el.lambda_d, soc_theta, soc_phi)
+        return h0 - V, V
+
     def Un(self):
         return np.array([self.elements[t].Un for t in self.atom_type])
 

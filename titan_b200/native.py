@@ -47,6 +47,8 @@ SIGNATURES = {
     "tg_set_green_method": (C.c_int, [C.c_void_p, C.c_int]),
     "tg_ldos": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_double, _dp, _dp]),
     "tg_smunu": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
+    "tg_chi0_linear_soc": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp,
+                                     _dp, _dp, C.c_int, _dp, _dp]),
     "tg_eig_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp]),
     "tg_she": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp,
                          _dp, C.c_int, _dp]),
@@ -328,6 +330,22 @@ class GreenGPU:
         self._check(self.lib.tg_dyson(self.h, n, _p(a.view(np.float64)), _p(u.view(np.float64)),
                                       _p(out.view(np.float64))))
         return out.T
+
+    def chi0_linear_soc(self, q, e, Ef, eta, etap, x2, p2, vsoc):
+        """(chiorb_hf, chiorb_hflsoc) [dimens, dimens] of eintshechilinearsoc; the context's h0 must exclude
+        the SOC blocks vsoc (see TBSystem.linear_soc_split)."""
+        qa = np.ascontiguousarray(q, np.float64)
+        x2 = np.ascontiguousarray(x2 if x2 is not None else np.zeros(0), np.float64)
+        p2 = np.ascontiguousarray(p2 if p2 is not None else np.zeros(0), np.float64)
+        V = _fortran_complex(vsoc)
+        D = self.dimens
+        chi = np.zeros((D, D), np.complex128)
+        lsoc = np.zeros((D, D), np.complex128)
+        rc = self.lib.tg_chi0_linear_soc(self.h, _p(qa), e, Ef, eta, etap, x2.shape[0], _p(x2) if x2.shape[0] else None,
+                                         _p(p2) if p2.shape[0] else None, _p(V.view(np.float64)), D,
+                                         _p(chi.view(np.float64)), _p(lsoc.view(np.float64)))
+        self._check(rc)
+        return chi.T, lsoc.T
 
     def smunu(self, Ef, eta):
         """Smunuiivec as [n_atoms, 3, nOrbMax(mu), nOrbMax(nu)] (calcSmunu, mod_sumrule.F90:162-245)."""
