@@ -186,6 +186,16 @@ int tg_chi0_linear_soc(tg_ctx* ctx, const double* q, double e, double Ef, double
                        int n_real, const double* x2, const double* p2, const double* vsoc, int dimens,
                        double* chiorb_hf, double* chiorb_lsoc);
 
+/* Exchange coupling J_ij(q): replaces jij_energy(q, Jij) (source/jij_energy.F90:6-242) in
+ * the normal state.  With dBxc/dm = -Um_i/2 (sigma^d_mu - (sigma^d . e_i) e_{i mu}) on the d
+ * orbitals (dmask(norb_max, n_atoms), the d-moment directions evec(3, n_atoms), Um(n_atoms)):
+ *   J(i, j, mu, nu) = -1/(2 pi) sum_{k,E} w [Tr(A^i_mu G_ij(k) A^j_nu G_ji(k-q))
+ *                                           + conj Tr(A^i_mu G_ij(k-q) A^j_nu G_ji(k))]
+ * over the imaginary-axis mesh at Ef + i(y + eta); J(n_atoms, n_atoms, 3, 3) complex.
+ * Gauss-Jordan per point (two inversions: k and k - q). */
+int tg_jij(tg_ctx* ctx, const double* q, double Ef, double eta, const double* evec, const double* Um,
+           const int* dmask, double* J);
+
 /* Orbital-resolved on-site spin density of the sum rule: replaces calcSmunu
  * (source/mod_sumrule.F90:162-245).  With A = sum_{k,E} w G(i, i) over the imaginary-axis
  * mesh at Ef + i(y + eta) and imgXY(mu, nu) = (A(nu X, mu Y) + conj A(mu Y, nu X)) / 2 pi

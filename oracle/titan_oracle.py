@@ -838,3 +838,48 @@ def sumrule(system, chi_hf, S, B):
     Bg = B[IDX]                                                                        # [h, spin]
     rhs = 2.0 * np.einsum('nqp,gmhp,hq->gmn', eps, cart[:, 1:, :, 1:], Bg[:, 1:])
     return lhs, rhs, float(np.sum(np.abs(lhs - rhs)))
+
+
+# ---------------------------------------------------------------------------
+# Exchange coupling J_ij(q), source/jij_energy.F90:6-242 (normal state).
+# ---------------------------------------------------------------------------
+def dbxc_dm(system, evec, Um, dorbs):
+    """dBxc_dm[i][mu] (2 nOrb x 2 nOrb): -Um/2 (sigma^d_mu - (sigma^d . e) e_mu), jij_energy.F90:55-64."""
+    sig = [np.array([[0, 1], [1, 0]], complex), np.array([[0, -1j], [1j, 0]]), np.array([[1, 0], [0, -1]], complex)]
+    out = []
+    for i, n in enumerate(system.norbs):
+        P = np.zeros((3, 2 * n, 2 * n), dtype=complex)
+        for a in range(3):
+            for d in dorbs[i]:
+                P[a][np.ix_([d, d + n], [d, d + n])] = sig[a]
+        e = np.asarray(evec[i], float)
+        pe = P[0] * e[0] + P[1] * e[1] + P[2] * e[2]
+        out.append([-0.5 * Um[i] * (P[mu] - pe * e[mu]) for mu in range(3)])
+    return out
+
+
+def jij(model: Model, mesh, q, Ef, eta, evec, Um, dorbs, chunk=1024):
+    """J[i, j, mu, nu] = -1/(2 pi) sum w [Tr(A G_ij(k) B G_ji(k-q)) + conj Tr(A G_ij(k-q) B G_ji(k))]."""
+    s = model.system
+    ia = s.ia()
+    nat = s.n_atoms
+    A = dbxc_dm(s, evec, Um, dorbs)
+    q = np.asarray(q, float)
+    J = np.zeros((nat, nat, 3, 3), dtype=complex)
+    y = mesh.point_energy()
+    blk = [slice(ia[i][0], ia[i][0] + 2 * s.norbs[i]) for i in range(nat)]
+    for sl in _chunks(mesh.n_points, chunk):
+        z = Ef + 1j * (y[sl] + eta)
+        G = model.green(z, mesh.kp[sl])
+        Gm = model.green(z, mesh.kp[sl] - q[None, :])
+        w = mesh.weight[sl]
+        for j in range(nat):
+            for i in range(nat):
+                gij, gji = G[:, blk[i], blk[j]], G[:, blk[j], blk[i]]
+                gijm, gjim = Gm[:, blk[i], blk[j]], Gm[:, blk[j], blk[i]]
+                for nu in range(3):
+                    for mu in range(3):
+                        t1 = np.einsum("ab,pbc,cd,pda->p", A[i][mu], gij, A[j][nu], gjim, optimize=True)
+                        t2 = np.einsum("ab,pbc,cd,pda->p", A[i][mu], gijm, A[j][nu], gji, optimize=True)
+                        J[i, j, mu, nu] += np.sum(w * (t1 + np.conj(t2)))
+    return -J / TPI

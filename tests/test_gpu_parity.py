@@ -350,3 +350,34 @@ def test_chi0_linear_soc_matches_oracle(gpu, shape, nk, e, q):
                                        s.etap, x2, p2)
     assert rel(chi, rchi) < 1e-10
     assert rel(lsoc, rl) < 1e-10
+
+
+def _moment_directions(state, dorbs):
+    m = np.array([[state.mx[i][d].sum(), state.my[i][d].sum(), state.mz[i][d].sum()] for i, d in enumerate(dorbs)])
+    return m / np.linalg.norm(m, axis=1)[:, None]
+
+
+@pytest.mark.parametrize("q", [(0.0, 0.0, 0.0), (0.2, 0.1, 0.0)])
+def test_jij_on_fe_golden_state(gpu, fe_deck, q):
+    """jij_energy on the GPU against the oracle at the golden Fe state, q = 0 and q != 0."""
+    s = fe_deck.system
+    st = fe_deck.state
+    h0 = s.h0(st)
+    gpu.setup(fe_deck, h0)
+    evec = _moment_directions(st, s.dorbs)
+    J = gpu.jij(np.array(q), s.Ef, s.eta, evec, s.Um())
+    ref = O.jij(O.Model(s, h0), fe_deck.ek, np.array(q), s.Ef, s.eta, evec, s.Um(), s.dorbs)
+    assert np.max(np.abs(J - ref)) < 1e-11 * np.max(np.abs(ref))
+
+
+def test_jij_two_sites_tilted_moments(gpu):
+    """Two-site cell with non-collinear moment directions (all 9 tensor components nonzero)."""
+    deck = synthetic.make_deck("sq2", nk=(5, 5, 1), n1gl=6, parts=1)
+    s = deck.system
+    h0 = s.h0(initial_state(s))
+    gpu.setup(deck, h0)
+    evec = np.array([[0.0, 0.6, 0.8], [0.6, 0.0, 0.8]])
+    q = np.array([0.1, 0.05, 0.0])
+    J = gpu.jij(q, s.Ef, s.eta, evec, s.Um())
+    ref = O.jij(O.Model(s, h0), deck.ek, q, s.Ef, s.eta, evec, s.Um(), s.dorbs)
+    assert np.max(np.abs(J - ref)) < 1e-11 * np.max(np.abs(ref))

@@ -123,6 +123,9 @@ struct tg_ctx {
   DevArray<double> d_ldos_e, d_ldos;
   // linear SOC: V, G V G of both Green functions, four operands, chi_lsoc partials
   DevArray<double2> d_vsoc, d_lsb[6], d_Cl, d_Dl;
+  // exchange coupling: d-orbital tables and per-CTA tensor slices
+  DevArray<int> d_jij_tab;
+  DevArray<double2> d_jij_part, d_jij_sum;
   // disturbance response (eintshe)
   DevArray<int> d_she_tab, d_ia;
   DevArray<double2> d_she_part, d_she_sum, d_she_pref, d_she_out;
@@ -1405,6 +1408,118 @@ int tg_chi0_linear_soc(tg_ctx* c, const double* q, double e, double Ef, double e
   }
   profile_end(c);
   return read_status(c);
+}
+
+int tg_jij(tg_ctx* c, const double* q, double Ef, double eta, const double* evec, const double* Um, const int* dmask,
+           double* J) {
+  int rc = check_ready(c, true, false);
+  if (rc) return rc;
+  if (!q || !evec || !Um || !dmask || !J) return set_err(c, TG_ERR_ARG, "tg_jij: null argument");
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  const int n = c->dimH, nat = c->n_atoms, nmax = c->nmax;
+  const int64_t nn = (int64_t)n * n;
+  // d-orbital lists: tab = [dstart (nat + 1) | dlist]
+  std::vector<int> tab(nat + 1, 0);
+  for (int i = 0; i < nat; ++i) {
+    int cnt = 0;
+    for (int o = 0; o < c->norb[i]; ++o)
+      if (dmask[(size_t)i * nmax + o]) {
+        tab.push_back(o);
+        ++cnt;
+      }
+    tab[i + 1] = tab[i] + cnt;
+  }
+  TG_CHECK(c, c->d_jij_tab.upload(tab.data(), tab.size(), s), "upload d orbitals");
+  TG_CHECK(c, c->d_ia.upload(c->ia.data(), c->ia.size(), s), "upload ia");
+  const int len = nat * nat * 32;
+  const int grid = c->num_sms * 4;
+  TG_CHECK(c, c->d_jij_part.ensure((size_t)grid * len), "alloc partials");
+  TG_CHECK(c, c->d_jij_sum.ensure((size_t)len), "alloc");
+  TG_CHECK(c, cudaMemsetAsync(c->d_jij_part.p, 0, sizeof(double2) * (size_t)grid * len, s), "memset");
+  const int64_t P = pass_size(c, c->n_imag);
+  TG_CHECK(c, c->d_A.ensure((size_t)P * nn), "alloc");
+  TG_CHECK(c, c->d_B.ensure((size_t)P * nn), "alloc");
+  if ((rc = reset_status(c))) return rc;
+  profile_begin(c);
+  for (int64_t p0 = 0; p0 < c->n_imag; p0 += P) {
+    GreenArgs g = base_args(c);
+    g.pts.kind = 0;
+    g.pts.y = c->d_y.p;
+    g.pts.kp = c->d_kp.p;
+    g.pts.w = c->d_w.p;
+    g.p0 = p0;
+    g.np = std::min<int64_t>(P, c->n_imag - p0);
+    g.zr = Ef;
+    g.zi = eta;
+    g.mode = MODE_RAW;
+    g.out = c->d_A.p;
+    {
+      KindTimer kt(c, 0);
+      TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), "green (k)");
+    }
+    g.q[0] = -q[0];
+    g.q[1] = -q[1];
+    g.q[2] = -q[2];
+    g.out = c->d_B.p;
+    {
+      KindTimer kt(c, 0);
+      TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), "green (k - q)");
+    }
+    KindTimer kt(c, 1);
+    c->launches += 1;
+    TG_CHECK(c, launch_jij(c->d_A.p, c->d_B.p, p0, g.np, c->d_w.p, n, nat, c->d_ia.p, c->d_norb.p, c->d_jij_tab.p,
+                           c->d_jij_tab.p + (nat + 1), c->d_jij_part.p, grid, s),
+             "jij tensors");
+  }
+  {
+    KindTimer kt(c, 2);
+    TG_CHECK(c, launch_reduce_blocks(c->d_jij_part.p, grid, len, c->d_jij_sum.p, s), "reduce");
+  }
+  std::vector<double2> h(len);
+  TG_CHECK(c, cudaMemcpyAsync(h.data(), c->d_jij_sum.p, sizeof(double2) * len, cudaMemcpyDeviceToHost, s), "copy");
+  profile_end(c);
+  if ((rc = read_status(c))) return rc;
+  // sigma_a[s][s'] (0 = up), a = x, y, z
+  const double2 sig[3][2][2] = {{{{0, 0}, {1, 0}}, {{1, 0}, {0, 0}}},
+                                {{{0, 0}, {0, -1}}, {{0, 1}, {0, 0}}},
+                                {{{1, 0}, {0, 0}}, {{0, 0}, {-1, 0}}}};
+  // V(T16, a, b) = sum sigma_a[s][s'] sigma_b[t][t'] T[s' + 2t + 4t' + 8s]
+  auto vertex = [&](const double2* T16, int a, int b) {
+    double2 v = make_double2(0.0, 0.0);
+    for (int ss = 0; ss < 2; ++ss)
+      for (int sp = 0; sp < 2; ++sp)
+        for (int t = 0; t < 2; ++t)
+          for (int tp = 0; tp < 2; ++tp)
+            v = cadd(v, cmul(cmul(sig[a][ss][sp], sig[b][t][tp]), T16[sp + 2 * t + 4 * tp + 8 * ss]));
+    return v;
+  };
+  const double f = -1.0 / (2.0 * kPi);
+  for (int i = 0; i < nat; ++i)
+    for (int j = 0; j < nat; ++j) {
+      const double2* T = h.data() + (size_t)(i * nat + j) * 32;
+      double2 V[3][3], Vs[3][3];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          V[a][b] = vertex(T, a, b);
+          Vs[a][b] = cconj(vertex(T + 16, a, b));
+        }
+      for (int mu = 0; mu < 3; ++mu)
+        for (int nu = 0; nu < 3; ++nu) {
+          double2 acc = make_double2(0.0, 0.0);
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+              // c^i_{mu a} = -Um_i / 2 (delta_{mu a} - e_{i mu} e_{i a})
+              const double ci = -0.5 * Um[i] * ((mu == a ? 1.0 : 0.0) - evec[3 * i + mu] * evec[3 * i + a]);
+              const double cj = -0.5 * Um[j] * ((nu == b ? 1.0 : 0.0) - evec[3 * j + nu] * evec[3 * j + b]);
+              acc = cadd(acc, cscale(cadd(V[a][b], Vs[a][b]), ci * cj));
+            }
+          const size_t o = (size_t)i + (size_t)nat * (j + (size_t)nat * (mu + 3 * (size_t)nu));
+          J[2 * o] = f * acc.x;
+          J[2 * o + 1] = f * acc.y;
+        }
+    }
+  return TG_OK;
 }
 
 int tg_smunu(tg_ctx* c, double Ef, double eta, double* S) {

@@ -187,6 +187,11 @@ cudaError_t launch_gvg(const double2* G, const double2* V, int n, int64_t np, do
 cudaError_t launch_operand(const double2* G, int n, int64_t np, int64_t p0, const PointSet& pts, int mode,
                            const int* outmap, double2* out, int num_sms, cudaStream_t s);
 
+// Exchange coupling: d-orbital GG tensors T(G(k), G(k - q)) and T(G(k - q), G(k)) per site pair
+cudaError_t launch_jij(const double2* Ga, const double2* Gb, int64_t p0, int64_t np, const double* w, int n,
+                       int n_atoms, const int* ia, const int* norb, const int* dstart, const int* dlist,
+                       double2* partial, int grid, cudaStream_t s);
+
 // Disturbance-response vertex (eintshe): one launch per pass over RAW G1 / G2
 struct SheLaunch {
   const GreenArgs* g = nullptr;   // system tables (n, neighbours, hopping blocks)

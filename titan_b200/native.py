@@ -47,6 +47,7 @@ SIGNATURES = {
     "tg_set_green_method": (C.c_int, [C.c_void_p, C.c_int]),
     "tg_ldos": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_double, _dp, _dp]),
     "tg_smunu": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
+    "tg_jij": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double, _dp, _dp, _ip, _dp]),
     "tg_chi0_linear_soc": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp,
                                      _dp, _dp, C.c_int, _dp, _dp]),
     "tg_eig_batch": (C.c_int, [C.c_void_p, C.c_int64, _dp, _dp, _dp]),
@@ -346,6 +347,20 @@ class GreenGPU:
                                          _p(chi.view(np.float64)), _p(lsoc.view(np.float64)))
         self._check(rc)
         return chi.T, lsoc.T
+
+    def jij(self, q, Ef, eta, evec, Um):
+        """J[i, j, mu, nu] of jij_energy at wave vector q; evec[i] = unit d-moment direction, Um per site."""
+        s = self.system
+        nat = s.n_atoms
+        dmask = np.zeros((nat, self.nmax), np.int32)
+        for i, dl in enumerate(s.dorbs):
+            dmask[i, dl] = 1
+        qa = np.ascontiguousarray(q, np.float64)
+        ev = np.ascontiguousarray(evec, np.float64).reshape(nat, 3)
+        um = np.ascontiguousarray(Um, np.float64)
+        J = np.zeros((3, 3, nat, nat), np.complex128)   # Fortran (i, j, mu, nu) read back as [nu, mu, j, i]
+        self._check(self.lib.tg_jij(self.h, _p(qa), Ef, eta, _p(ev), _p(um), _p(dmask, C.c_int), _p(J.view(np.float64))))
+        return np.transpose(J, (3, 2, 1, 0))
 
     def smunu(self, Ef, eta):
         """Smunuiivec as [n_atoms, 3, nOrbMax(mu), nOrbMax(nu)] (calcSmunu, mod_sumrule.F90:162-245)."""
