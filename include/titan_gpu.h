@@ -221,10 +221,13 @@ int tg_ldos(tg_ctx* ctx, int n_e, const double* e, double eta, double* ldosu, do
  * nearly degenerate eigenvectors times the difference of their weights, while the
  * inversion stays near eps.  Sums over the mesh average this out for chi0 (same
  * error against the FP64 oracle as Gauss-Jordan), but the disturbance integral feeds
- * B_eff through an ill-conditioned site-reduced chi^-1, so:
- *   TG_GREEN_AUTO (default)  spectral for chi0, Gauss-Jordan for tg_she
+ * B_eff through an ill-conditioned site-reduced chi^-1, and the occupations feed a Newton
+ * iteration whose step tolerance (mag_tol = 1e-12) the spectral noise exceeds, so:
+ *   TG_GREEN_AUTO (default)  spectral for chi0 and tg_ldos, Gauss-Jordan for tg_she and
+ *                            tg_expectation
  *   TG_GREEN_GAUSS_JORDAN    Gauss-Jordan everywhere
- *   TG_GREEN_SPECTRAL        spectral wherever the mesh allows (tg_she ~4x faster)
+ *   TG_GREEN_SPECTRAL        spectral wherever the mesh allows (tg_she ~4x faster,
+ *                            tg_expectation one eigendecomposition per k for all energies)
  * Other meshes and dimensions always use Gauss-Jordan.  No counterpart in the
  * reference. */
 #define TG_GREEN_AUTO          0

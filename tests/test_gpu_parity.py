@@ -381,3 +381,19 @@ def test_jij_two_sites_tilted_moments(gpu):
     J = gpu.jij(q, s.Ef, s.eta, evec, s.Um())
     ref = O.jij(O.Model(s, h0), deck.ek, q, s.Ef, s.eta, evec, s.Um(), s.dorbs)
     assert np.max(np.abs(J - ref)) < 1e-11 * np.max(np.abs(ref))
+
+
+def test_spectral_expectation_on_request(gpu, fe_deck):
+    """TG_GREEN_SPECTRAL: occupations and moments from one eigendecomposition per k (the energy
+    sum folded per eigenvalue) equal the Gauss-Jordan ones to 1e-11 on the Fe golden state."""
+    s = fe_deck.system
+    st = fe_deck.state
+    gpu.setup(fe_deck, s.h0(st))
+    gj = gpu.expectation(st.Ef, s.eta)
+    try:
+        gpu.set_green_method("spectral")
+        sp = gpu.expectation(st.Ef, s.eta)
+    finally:
+        gpu.set_green_method("auto")
+    for a, b in zip(sp, gj):
+        assert np.max(np.abs(a - b)) < 1e-11

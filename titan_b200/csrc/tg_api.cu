@@ -279,10 +279,11 @@ int build_htab(tg_ctx* c, int slot, const double* d_k, int64_t nk, const double*
 }
 
 // eigendecomposition of every row of H table `slot` (spectral Green functions)
-// chi0 uses spectral Green functions unless Gauss-Jordan is forced; the disturbance
-// integral only when TG_GREEN_SPECTRAL asks for it (see tg_set_green_method)
+// chi0 and the LDOS use spectral Green functions unless Gauss-Jordan is forced; the
+// disturbance integral and the occupations only when TG_GREEN_SPECTRAL asks for them (see
+// tg_set_green_method)
 bool spectral_on(tg_ctx* c) { return c->green_method != TG_GREEN_GAUSS_JORDAN && eig_supported(c->dimH); }
-bool spectral_she_on(tg_ctx* c) { return c->green_method == TG_GREEN_SPECTRAL && eig_supported(c->dimH); }
+bool spectral_forced(tg_ctx* c) { return c->green_method == TG_GREEN_SPECTRAL && eig_supported(c->dimH); }
 
 int build_eig(tg_ctx* c, int slot, int64_t nk) {
   const size_t nn = (size_t)c->dimH * c->dimH;
@@ -1005,7 +1006,19 @@ int tg_expectation(tg_ctx* c, double Ef, double eta, double* rho, double* mx, do
   rc = reset_status(c);
   if (rc) return rc;
   int grid = 0;
-  TG_CHECK(c, launch_green(a, c->num_sms, s, &grid), "green (expectation)");
+  if (a.htab && spectral_forced(c)) {
+    // uniform mesh: one eigendecomposition per k, the energy sum folded into f_a per k
+    if ((rc = reset_eig_status(c))) return rc;
+    if ((rc = build_eig(c, 0, c->nk_u))) return rc;
+    grid = (int)std::min<int64_t>(c->nk_u, maxgrid);
+    c->launches += 1;
+    TG_CHECK(c, launch_spec_expect(c->d_eigU[0].p, c->d_eigL[0].p, c->nk_u, n, c->d_ylist.p, c->n_e_u, c->d_w.p, Ef,
+                                   eta, c->d_exp_rows.p, c->d_acc.p, grid, s),
+             "expectation (spectral)");
+    if ((rc = read_eig_status(c))) return rc;
+  } else {
+    TG_CHECK(c, launch_green(a, c->num_sms, s, &grid), "green (expectation)");
+  }
   TG_CHECK(c, launch_reduce_blocks(c->d_acc.p, grid, len, c->d_acc_red.p, s), "reduce");
   std::vector<double2> h(len);
   TG_CHECK(c, cudaMemcpyAsync(h.data(), c->d_acc_red.p, sizeof(double2) * len, cudaMemcpyDeviceToHost, s), "copy");
@@ -1762,7 +1775,7 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
   const double zero3[3] = {0.0, 0.0, 0.0};
   const bool tab_imag = c->imag_uniform && (int64_t)c->nk_u * nn * 16 <= ((int64_t)8 << 30);
   const bool tab_real = real && (int64_t)c->n_realk * nn * 16 <= ((int64_t)8 << 30);
-  const bool spec = spectral_she_on(c);
+  const bool spec = spectral_forced(c);
   if (spec && (tab_imag || tab_real) && (rc = reset_eig_status(c))) return rc;
   auto tables = [&](int slot, const double* d_k, int64_t nk, bool shift) -> int {
     if ((rc = build_htab(c, slot, d_k, nk, shift ? q : zero3))) return rc;

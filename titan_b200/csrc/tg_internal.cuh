@@ -174,6 +174,10 @@ int eig_supported(int n);
 cudaError_t launch_eig(const double2* H, int64_t nk, int n, double2* U, double* lam, int* status, int num_sms,
                        cudaStream_t s);
 int spectral_supported(int mode, int mode2, bool has_out2);
+// per-CTA slices [grid][2 n] of the energy-summed diagonal spin blocks (uu, dd, ud, du per orbital)
+cudaError_t launch_spec_expect(const double2* U, const double* lam, int64_t nk, int n, const double* ylist, int64_t n_e,
+                               const double* w, double zr, double zi, const int* rows, double2* partial, int grid,
+                               cudaStream_t s);
 // out[ie][r] = -Im G_rr(e_ie + i eta) / pi summed over the tabulated k with weights w
 cudaError_t launch_spec_ldos(const double2* U, const double* lam, const double* w, int64_t nk, int n,
                              const double* e, int n_e, double eta, double* out, int num_sms, cudaStream_t s);

@@ -392,9 +392,63 @@ __global__ void __launch_bounds__(256) spec_ldos_kernel(const double2* __restric
   for (int o = threadIdx.x; o < ne * n; o += blockDim.x) atomicAdd(out + (int64_t)(e0 + o / n) * n + o % n, f * acc[o]);
 }
 
+// --------------------------------------------------------------------------- expectation sums from (U, lambda)
+// For the occupations and moments only the orbital-diagonal spin blocks of G summed over
+// the energies of each k are needed:
+//   S(r, c) = sum_ie w(ie, k) G_rc(k, z_ie) = sum_a U[r][a] f_a conj(U[c][a]),
+//   f_a = sum_ie w(ie, k) / (z_ie - lambda_a),  z_ie = zr + i (zi + y_ie),
+// so each k costs n x n_e divisions and 4 n entries of n terms.  out: per-CTA slices of
+// [n / 2 orbitals][uu, dd, ud, du] (rows[2 o], rows[2 o + 1] = up / down row of orbital o).
+__global__ void __launch_bounds__(256) spec_expect_kernel(const double2* __restrict__ U, const double* __restrict__ lam,
+                                                          int64_t nk, int n, const double* __restrict__ ylist,
+                                                          int64_t n_e, const double* __restrict__ w, double zr,
+                                                          double zi, const int* __restrict__ rows,
+                                                          double2* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double2* f = reinterpret_cast<double2*>(smem);   // [n]
+  double2* acc = f + n;                            // [2 n]
+  for (int e = threadIdx.x; e < 2 * n; e += blockDim.x) acc[e] = make_double2(0.0, 0.0);
+  for (int64_t k = blockIdx.x; k < nk; k += gridDim.x) {
+    __syncthreads();
+    for (int a = threadIdx.x; a < n; a += blockDim.x) {
+      const double l = lam[k * n + a];
+      double fr = 0.0, fi = 0.0;
+      const double x = zr - l;
+      for (int64_t ie = 0; ie < n_e; ++ie) {
+        const double y = zi + ylist[ie];
+        const double inv = w[ie * nk + k] / (x * x + y * y);
+        fr = fma(x, inv, fr);
+        fi = fma(-y, inv, fi);
+      }
+      f[a] = make_double2(fr, fi);
+    }
+    __syncthreads();
+    const double2* Uk = U + k * (int64_t)n * n;
+    for (int e = threadIdx.x; e < 2 * n; e += blockDim.x) {
+      const int o = e >> 2, q = e & 3;
+      const int ru = rows[2 * o], rd = rows[2 * o + 1];
+      const int r = (q == 0 || q == 2) ? ru : rd, c = (q == 0 || q == 3) ? ru : rd;
+      double2 s = make_double2(0.0, 0.0);
+      for (int a = 0; a < n; ++a) s = cfma(cmul(Uk[(int64_t)r * n + a], f[a]), cconj(Uk[(int64_t)c * n + a]), s);
+      acc[e] = cadd(acc[e], s);
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 2 * n; e += blockDim.x) partial[(size_t)blockIdx.x * 2 * n + e] = acc[e];
+}
+
 }  // namespace
 
 // --------------------------------------------------------------------------- host side
+cudaError_t launch_spec_expect(const double2* U, const double* lam, int64_t nk, int n, const double* ylist, int64_t n_e,
+                               const double* w, double zr, double zi, const int* rows, double2* partial, int grid,
+                               cudaStream_t s) {
+  if (nk <= 0) return cudaSuccess;
+  const size_t smem = sizeof(double2) * 3 * (size_t)n;
+  spec_expect_kernel<<<grid, 256, smem, s>>>(U, lam, nk, n, ylist, n_e, w, zr, zi, rows, partial);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_spec_ldos(const double2* U, const double* lam, const double* w, int64_t nk, int n,
                              const double* e, int n_e, double eta, double* out, int num_sms, cudaStream_t s) {
   if (nk <= 0 || n_e <= 0) return cudaSuccess;
