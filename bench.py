@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--compare-fp64", action="store_true", help="also time the FP64 path and report the ratio")
+    ap.add_argument("--no-check", action="store_true",
+                    help="skip the untimed split-vs-FP64 accuracy check of the chi0 workload")
     ap.add_argument("--green", default="auto", choices=["auto", "gauss-jordan", "spectral"],
                     help="Green-function method (tg_set_green_method)")
     ap.add_argument("--workload", default="chi0", choices=["chi0", "she", "ldos"],
@@ -229,6 +231,20 @@ def timed_steps(gpu, deck, h0, omegas, reals, steps, start, per, precision, prof
     return ms, units, launches, t
 
 
+def split_accuracy(gpu, deck, omegas, reals, per):
+    """Normwise ||chi_split - chi_fp64||_F / ||chi_fp64||_F on the full workload, untimed: the
+    frequencies of one step (the largest ones, which carry the real-axis part too), worst one."""
+    s = deck.system
+    idx = list(range(len(omegas) - per, len(omegas)))
+    es = [float(omegas[i]) for i in idx]
+    x2s, p2s = [reals[i][0] for i in idx], [reals[i][1] for i in idx]
+    sp = gpu.chi0_batch(np.zeros(3), es, s.Ef, s.eta, s.etap, x2s, p2s, "split").copy()
+    fp = gpu.chi0_batch(np.zeros(3), es, s.Ef, s.eta, s.etap, x2s, p2s, "fp64")
+    errs = [float(np.linalg.norm(sp[w] - fp[w]) / np.linalg.norm(fp[w])) for w in range(len(idx))]
+    return {"max": max(errs), "per_omega": errs, "omegas": es,
+            "measure": "||chi_split - chi_fp64||_F / ||chi_fp64||_F, same calls, full mesh"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from titan_b200.native import GreenGPU
@@ -268,9 +284,9 @@ def run_ours(args, rank, world, local_rank):
     achieved = flops_con / (con_ms / 1e3) / 1e12 if con_ms > 0 else None
     peak = pk.get("bf16_tflops")
     # DRAM traffic per contraction launch from the ncu capture in
-    # profiles/split_contract_sq2_small.md (3.999 GB over 1984 K-steps of 32 points),
+    # profiles/split_contract_sq2_small.md (2.188 GB over 1984 K-steps of 32 points),
     # scaled by the K-steps one launch of this run processes
-    kstep_bytes = 3.999e9 / 1984
+    kstep_bytes = 2.188e9 / 1984
     traffic = kstep_bytes * (last_units / 32.0) / con_n if (con_n and args.precision == "split") else None
     roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
@@ -305,6 +321,8 @@ def run_ours(args, rank, world, local_rank):
         ms64, u64, _, _ = timed_steps(gpu, deck, h0, omegas, reals, 1, start + args.warmup * per, per, "fp64")
         line["fp64_path"] = {"value": u64 / (sum(ms64) / 1e3), "unit": UNIT, "ms_per_step": sum(ms64)}
         line["split_over_fp64"] = value / world / line["fp64_path"]["value"]
+    if args.precision == "split" and not args.no_check:
+        line["split_rel_err"] = split_accuracy(gpu, deck, omegas, reals, per)
     # end to end: public API from pinned host buffers, full set-up + call + read-back every step
     if not args.no_e2e:
         e2e = run_e2e(gpu, deck, h0, omegas, reals, args, start + args.warmup * per, per, world)

@@ -250,10 +250,10 @@ int read_status(tg_ctx* c) {
   return TG_OK;
 }
 
-int64_t pass_size(tg_ctx* c, int64_t np) {
-  // two operand buffers of P * dimH^2 complex each, bounded to ~6 GiB
+int64_t pass_size(tg_ctx* c, int64_t np, int64_t operand_bytes = (int64_t)3 << 30) {
+  // two operand buffers of P * dimH^2 complex each, operand_bytes apiece
   const int64_t per = (int64_t)c->dimH * c->dimH * sizeof(double2);
-  int64_t P = (int64_t)3 << 30;
+  int64_t P = operand_bytes;
   P /= per;
   P = std::max<int64_t>(P, 1024);
   P = (P / 64) * 64;
@@ -351,6 +351,31 @@ SplitChunks make_chunks(int64_t np, Key key) {
   return ch;
 }
 
+// chunks of a k-major pass over a tabulated mesh of ne energies (work item p0 + i = k * ne
+// + energy): the slots of one energy are ne apart, so every energy of the pass is one chunk
+// (split at kSplitMaxChunk points) with stride ne
+SplitChunks make_chunks_kmajor(int64_t p0, int64_t np, int64_t ne) {
+  SplitChunks ch;
+  ch.stride = (int)ne;
+  ch.kstart.push_back(0);
+  const int64_t e0 = p0 % ne;
+  for (int64_t ie = 0; ie < ne; ++ie) {
+    const int64_t first = (ie - e0 + ne) % ne;   // first slot of energy ie
+    if (first >= np) continue;
+    const int64_t total = (np - 1 - first) / ne + 1;
+    for (int64_t done = 0; done < total; done += kSplitMaxChunk) {
+      const int cnt = (int)std::min<int64_t>(kSplitMaxChunk, total - done);
+      const int nk = (cnt + kSplitK - 1) / kSplitK;
+      const int ci = (int)ch.count.size();
+      ch.slot0.push_back((int)(first + done * ne));
+      ch.count.push_back(cnt);
+      ch.kstart.push_back(ch.kstart.back() + nk);
+      for (int t = 0; t < nk; ++t) ch.kchunk.push_back(ci);
+    }
+  }
+  return ch;
+}
+
 // uploads the chunk tables and sizes the digit / exponent buffers of a pass
 int split_prepare(tg_ctx* c, const SplitChunks& ch, SplitPassDev& pd) {
   const int nc = ch.n_chunks(), nks = ch.n_ksteps();
@@ -363,6 +388,7 @@ int split_prepare(tg_ctx* c, const SplitChunks& ch, SplitPassDev& pd) {
   TG_CHECK(c, c->d_chunks.upload(buf.data(), buf.size(), c->stream), "upload chunks");
   pd.n_chunks = nc;
   pd.n_ksteps = nks;
+  pd.stride = ch.stride;
   pd.slot0 = c->d_chunks.p;
   pd.count = c->d_chunks.p + nc;
   pd.kstart = c->d_chunks.p + 2 * nc;
@@ -703,7 +729,10 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   const bool split = precision == TG_PREC_SPLIT;
   const int64_t cstride = (int64_t)c->dimens * c->dimens;
   // workspace
-  const int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, (int64_t)n_real * c->n_realk));
+  // 6 GiB operands (about 25 GB with the digit planes and tables at dimH = 36): a k-major
+  // pass over a tabulated mesh then holds ~2400 points per energy, so the split
+  // contraction's chunk ends (one per energy and pass) cost little
+  const int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, (int64_t)n_real * c->n_realk), (int64_t)6 << 30);
   const int nsplit = split ? split_nsplit((int)c->split.tiles.size(), c->num_sms, P / kSplitK) : nsplit_for(c);
   if (split) {
     TG_CHECK(c, c->d_split_err.ensure(1), "alloc");
@@ -792,7 +821,9 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     if (split) {
       KindTimer kt(c, 3);
       const double* yv = c->h_y.data() + p0;
-      if ((rc = split_prepare(c, make_chunks(np, [&](int64_t i) { return yv[i]; }), pd))) return rc;
+      const SplitChunks ch = tab_imag ? make_chunks_kmajor(p0, np, c->n_e_u)
+                                      : make_chunks(np, [&](int64_t i) { return yv[i]; });
+      if ((rc = split_prepare(c, ch, pd))) return rc;
       if ((rc = split_quantize_operand(c, 1, c->d_B.p, pd))) return rc;
     }
     if (w_start == 1) {
@@ -894,7 +925,9 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
           const int64_t nrk = c->n_realk, pbase = p0;
           {
             KindTimer kq(c, 3);
-            rc = split_prepare(c, make_chunks(np, [&](int64_t i) { return (pbase + i) / nrk; }), pr);
+            const SplitChunks ch = tab_real ? make_chunks_kmajor(pbase, np, n_real)
+                                            : make_chunks(np, [&](int64_t i) { return (pbase + i) / nrk; });
+            rc = split_prepare(c, ch, pr);
             if (!rc) rc = split_quantize_operand(c, 1, c->d_B.p, pr);
             if (!rc) rc = split_quantize_operand(c, 0, c->d_A.p, pr);
           }

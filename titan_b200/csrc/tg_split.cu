@@ -5,8 +5,9 @@
 // element, the largest |Re|, |Im|), split_quantize_kernel (FP64 operand ->
 // five int8 digit planes, K-step blocks) and split_contract_kernel (warp-
 // specialised: one producer warp stages digit blocks with bulk copies into a
-// six-stage shared-memory ring, one warp issues the 19 MMAs per K-step, four
-// warps drain the six int32 level accumulators from TMEM at every chunk end).
+// six-stage shared-memory ring, one warp issues the 19 MMAs per K-step, eight
+// warps drain the six int32 level accumulators from TMEM at every chunk end
+// into FP64 sums held in registers until the unit ends).
 // Every wait on an mbarrier is bounded (2 s of %globaltimer); on a timeout the
 // kernel records an error code, waits (bounded) for its own copies and MMAs in
 // flight, frees its TMEM and returns.
@@ -26,8 +27,9 @@ namespace {
 
 constexpr int kRowmaxSlots = 64;
 
-__global__ void split_rowmax_kernel(const double2* __restrict__ X, int64_t ld, const int* __restrict__ slot0,
-                                    const int* __restrict__ count, unsigned long long* __restrict__ M64) {
+__global__ void split_rowmax_kernel(const double2* __restrict__ X, int64_t ld, int stride,
+                                    const int* __restrict__ slot0, const int* __restrict__ count,
+                                    unsigned long long* __restrict__ M64) {
   const int c = blockIdx.y;
   const int cnt = count[c];
   const int s_begin = blockIdx.x * kRowmaxSlots;
@@ -37,7 +39,7 @@ __global__ void split_rowmax_kernel(const double2* __restrict__ X, int64_t ld, c
   for (int64_t e = threadIdx.x; e < ld; e += blockDim.x) {
     double m = 0.0;
     for (int s = s_begin; s < s_end; ++s) {
-      const double2 v = X[(base + s) * ld + e];
+      const double2 v = X[(base + (int64_t)s * stride) * ld + e];
       m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
     }
     if (m > 0.0) atomicMax(&M64[(int64_t)c * ld + e], (unsigned long long)__double_as_longlong(m));
@@ -76,7 +78,7 @@ __device__ __forceinline__ void digits16(const long long (&x)[16], uint4 (&out)[
 // one thread per (K-step t, k half kc, group g, row r < rows): 16 points of one
 // element, Re and Im parts
 __global__ void __launch_bounds__(256) split_quantize_kernel(
-    const double2* __restrict__ X, int64_t ld, int n_ksteps, const int* __restrict__ kchunk,
+    const double2* __restrict__ X, int64_t ld, int stride, int n_ksteps, const int* __restrict__ kchunk,
     const int* __restrict__ kstart, const int* __restrict__ slot0, const int* __restrict__ count,
     const SplitGroup* __restrict__ groups, int n_groups, int rows, const unsigned long long* __restrict__ M64,
     int* __restrict__ E, int8_t* __restrict__ dig) {
@@ -104,12 +106,13 @@ __global__ void __launch_bounds__(256) split_quantize_kernel(
     const double scale = __hiloint2double((1023 + kSplitBits - (valid ? Ex : 0)) << 20, 0);
     const int first = (t - kstart[c]) * kSplitK + kc * 16;   // point within the chunk
     const int cnt = count[c];
-    const double2* src = X + ((int64_t)slot0[c] + first) * ld + e;
+    const double2* src = X + ((int64_t)slot0[c] + (int64_t)first * stride) * ld + e;
+    const int64_t step = (int64_t)stride * ld;
     long long xr[16], xi[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
       double2 v = make_double2(0.0, 0.0);
-      if (valid && first + k < cnt) v = src[(int64_t)k * ld];
+      if (valid && first + k < cnt) v = src[k * step];
       xr[k] = __double2ll_rn(v.x * scale);
       xi[k] = __double2ll_rn(v.y * scale);
     }
@@ -135,8 +138,10 @@ constexpr int kMmaN = 2 * kSplitColsB;     // 80
 constexpr int kLevels = 6;                 // L = 2..7
 constexpr int kStages = 6;
 constexpr int kStageBytes = kSplitABlock + kSplitBBlock;   // 33280
-constexpr int kXchBytes = 64 * 8 * 16;                     // 64 rows x 8 complex
-constexpr int kThreads = 192;                              // producer, MMA, 4 epilogue warps
+constexpr int kHalfCols = kSplitColsB / 2;                 // complex columns per epilogue warp
+constexpr int kXchBytes = 2 * 64 * 4 * 16 + 2 * 256;      // 2 halves x 64 rows x 4 complex, 2 x 40 exponents
+constexpr int kEpiThreads = 256;                           // 8 epilogue warps
+constexpr int kThreads = 64 + kEpiThreads;                 // producer, MMA, epilogue
 constexpr uint32_t kTmemCols = 512;
 constexpr int kBarOff = kStages * kStageBytes + kXchBytes;  // 8-byte aligned
 constexpr int kNumBars = 2 * kStages + 3;
@@ -226,15 +231,30 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&v)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
                : "r"(taddr));
 }
 
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// exact double of an integer |v| < 2^51: its bits added to those of 1.5 * 2^52 give
+// 1.5 * 2^52 + v (the same binade), and the subtraction is exact
+__device__ __forceinline__ double i51_to_double(long long v) {
+  return __longlong_as_double(v + 0x4338000000000000LL) - 6755399441055744.0;
+}
 
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+// 2^28 sum_{L=2..7} S_L 2^(4 - 8L) for the six int32 level sums S_L of column k:
+// hi = S_2 2^16 + S_3 2^8 + S_4 and lo = S_5 2^16 + S_6 2^8 + S_7 are exact integers
+// below 2^48, and the value is hi + lo 2^-24 (one rounding)
+__device__ __forceinline__ double levels_value(const uint32_t (&x)[kLevels][4], int k) {
+  const long long hi = (long long)(int)x[0][k] * 65536LL + (long long)(int)x[1][k] * 256LL + (long long)(int)x[2][k];
+  const long long lo = (long long)(int)x[3][k] * 65536LL + (long long)(int)x[4][k] * 256LL + (long long)(int)x[5][k];
+  return fma(i51_to_double(lo), 0x1p-24, i51_to_double(hi));
+}
 
 // Persistent: CTA b takes the units (tile, K-range) b, b + gridDim.x, ...; units
 // are numbered K-range-major so that the CTAs resident at one time share the
@@ -253,7 +273,8 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sbase + kBarOff + kNumBars * 8);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sbase + kBarOff + kNumBars * 8 + 4);
   volatile int* epi_ok = reinterpret_cast<volatile int*>(sbase + kBarOff + kNumBars * 8 + 8);
-  double2* xch = reinterpret_cast<double2*>(sbase + kStages * kStageBytes);
+  double2* xch = reinterpret_cast<double2*>(sbase + kStages * kStageBytes);   // [2][64 * 4]
+  int* ebs = reinterpret_cast<int*>(sbase + kStages * kStageBytes + 2 * 64 * 4 * 16);   // [2][64]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -262,7 +283,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
       mbar_init(bar0 + 8u * (kStages + s), 1);
     }
     mbar_init(accfull, 1);
-    mbar_init(accempty, 128);
+    mbar_init(accempty, kEpiThreads);
     mbar_init(flushbar, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -377,10 +398,17 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
     }
     __syncwarp();
   } else {
-    // ---------------- epilogue: warps 2..5 own TMEM lanes 32 (warp % 4) .. + 31 ----------------
+    // ---------------- epilogue: warps 2..9 ----------------
+    // Warp w reads TMEM lanes 32 (w % 4) .. + 31 (MMA rows: 0..63 Re A, 64..127 Im A of
+    // complex row r % 64) and the half (w - 2) / 4 of the tile's 40 complex columns.  Each
+    // thread keeps its row's FP64 sums for its 20 columns in registers over all chunks of a
+    // unit: per chunk end it folds the six int32 levels into two exact 48-bit integers,
+    // scales them by the chunk's power of two and adds; C is written once per unit.
     const int ep = threadIdx.x - 64;
     const int lane_base = 32 * (warp & 3);
-    const int r = lane_base + lane;   // MMA row: 0..63 Re A, 64..127 Im A of complex row r % 64
+    const int half = (warp - 2) >> 2;
+    const int cbase = half * kHalfCols;
+    const int r = lane_base + lane;
     const int part = r >> 6;
     const int rr = r & 63;
     uint32_t d = 0;
@@ -392,77 +420,75 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
       const int M = a.pair_M[tile.pair];
       const int64_t aoff = a.pair_aoff[tile.pair];
       const int u = tile.u0 + rr;
-      const bool own = part == 0 && u < M;
-      double2* Crow = a.C + (int64_t)split * a.cstride + a.pair_coff[tile.pair] + (int64_t)u * M;
+      double ax[kHalfCols], ay[kHalfCols];   // sums over the B real / imaginary columns
+#pragma unroll
+      for (int j = 0; j < kHalfCols; ++j) ax[j] = ay[j] = 0.0;
       int t = k0;
       while (t < k1) {
         const int c = kchunk[t];
         const int te = min(k1, kstart[c + 1]);
+        // exponents of the chunk, fetched while its MMAs still run (buffer d & 1 was last
+        // read two chunks ago, before the accumulator barrier of the previous chunk)
+        const int64_t erow = (int64_t)c * a.ld + aoff;
+        int* eb = ebs + 64 * (d & 1u);
+        if (ep < kSplitColsB) eb[ep] = tile.v0 + ep < M ? a.EB[erow + tile.v0 + ep] : 0;
+        const int ea = u < M ? a.EA[erow + u] : 0;
         if (ep == 0) *epi_ok = mbar_wait(accfull, d & 1u, abort_flag, a.err, 4) ? 1 : 0;
         epi_sync();
         ok = *epi_ok != 0;
         epi_sync();
         if (!ok) break;
         tc_fence_after();
-        const int64_t erow = (int64_t)c * a.ld + aoff;
-        const int ea = own ? a.EA[erow + u] : 0;
-#pragma unroll 1
-        for (int q = 0; q < kSplitColsB / 8; ++q) {
-          const int vq = tile.v0 + 8 * q;
-          double2 cv[8];
-          int eb[8];
+        const uint32_t trow = tmem + ((uint32_t)lane_base << 16) + (uint32_t)cbase;
 #pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            cv[k] = make_double2(0.0, 0.0);
-            eb[k] = 0;
-            if (own && vq + k < M) {
-              cv[k] = Crow[vq + k];
-              eb[k] = a.EB[erow + vq + k];
-            }
-          }
-          uint32_t x[kLevels][8], y[kLevels][8];
+        for (int g = 0; g < kHalfCols / 4; ++g) {
+          uint32_t x[kLevels][4], y[kLevels][4];
 #pragma unroll
           for (int l = 0; l < kLevels; ++l) {
-            const uint32_t ta = tmem + ((uint32_t)lane_base << 16) + (uint32_t)(l * kMmaN + 8 * q);
-            tmem_ld8(ta, x[l]);
-            tmem_ld8(ta + kSplitColsB, y[l]);
+            tmem_ld4(trow + (uint32_t)(l * kMmaN + 4 * g), x[l]);
+            tmem_ld4(trow + (uint32_t)(l * kMmaN + kSplitColsB + 4 * g), y[l]);
           }
           tmem_wait_ld();
-          double vr[8], vi[8];
-#pragma unroll
-          for (int k = 0; k < 8; ++k) vr[k] = vi[k] = 0.0;
-#pragma unroll
-          for (int l = 0; l < kLevels; ++l) {
-            const double w = __hiloint2double((1023 + 4 - 8 * (l + 2)) << 20, 0);   // 2^(4 - 8L), L = l + 2
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              vr[k] = fma((double)(int)x[l][k], w, vr[k]);
-              vi[k] = fma((double)(int)y[l][k], w, vi[k]);
-            }
+          if (g == kHalfCols / 4 - 1) {
+            // every TMEM read of this thread has landed: the MMA warp may start the next chunk
+            tc_fence_before();
+            mbar_arrive(accempty);
           }
-          // rows of part 0 hold (Ar Br, Ar Bi), rows of part 1 (Ai Br, Ai Bi) of the same complex row
-          if (part == 1) {
 #pragma unroll
-            for (int k = 0; k < 8; ++k) xch[rr * 8 + k] = make_double2(vr[k], vi[k]);
+          for (int k = 0; k < 4; ++k) {
+            const int e = ea + eb[cbase + 4 * g + k] - 28;
+            ax[4 * g + k] += ldexp(levels_value(x, k), e);
+            ay[4 * g + k] += ldexp(levels_value(y, k), e);
           }
-          epi_sync();
-          if (own) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              if (vq + k >= M) continue;
-              const double2 yy = xch[rr * 8 + k];
-              const int e = ea + eb[k];
-              cv[k].x += ldexp(vr[k] - yy.y, e);
-              cv[k].y += ldexp(vi[k] + yy.x, e);
-              Crow[vq + k] = cv[k];
-            }
-          }
-          epi_sync();
         }
-        tc_fence_before();
-        mbar_arrive(accempty);
         ++d;
         t = te;
+      }
+      if (!ok) break;
+      // unit end: rows of part 0 hold (Ar Br, Ar Bi), rows of part 1 (Ai Br, Ai Bi) of the
+      // same complex row; part 1 hands its sums over through shared memory, four columns at a time
+      double2* xh = xch + half * 64 * 4;
+      double2* Crow = a.C + (int64_t)split * a.cstride + a.pair_coff[tile.pair] + (int64_t)u * M;
+#pragma unroll
+      for (int g = 0; g < kHalfCols / 4; ++g) {
+        if (part == 1) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) xh[rr * 4 + k] = make_double2(ax[4 * g + k], ay[4 * g + k]);
+        }
+        epi_sync();
+        if (part == 0 && u < M) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int v = tile.v0 + cbase + 4 * g + k;
+            if (v >= M) continue;
+            const double2 yy = xh[rr * 4 + k];
+            double2 cv = Crow[v];
+            cv.x += ax[4 * g + k] - yy.y;
+            cv.y += ay[4 * g + k] + yy.x;
+            Crow[v] = cv;
+          }
+        }
+        epi_sync();
       }
     }
   }
@@ -514,7 +540,7 @@ cudaError_t split_rowmax(const double2* X, int64_t ld, const SplitPassDev& p, un
                          cudaStream_t s) {
   if (p.n_chunks <= 0) return cudaSuccess;
   const int gx = (kSplitMaxChunk + kRowmaxSlots - 1) / kRowmaxSlots;
-  split_rowmax_kernel<<<dim3(gx, p.n_chunks), 256, 0, s>>>(X, ld, p.slot0, p.count, M64);
+  split_rowmax_kernel<<<dim3(gx, p.n_chunks), 256, 0, s>>>(X, ld, p.stride, p.slot0, p.count, M64);
   return cudaGetLastError();
 }
 
@@ -524,7 +550,7 @@ cudaError_t split_quantize(const double2* X, int64_t ld, const SplitPassDev& p, 
   if (p.n_ksteps <= 0) return cudaSuccess;
   const int64_t total = (int64_t)p.n_ksteps * 2 * n_groups * rows;
   const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
-  split_quantize_kernel<<<blocks, 256, 0, s>>>(X, ld, p.n_ksteps, p.kchunk, p.kstart, p.slot0, p.count, groups,
+  split_quantize_kernel<<<blocks, 256, 0, s>>>(X, ld, p.stride, p.n_ksteps, p.kchunk, p.kstart, p.slot0, p.count, groups,
                                                n_groups, rows, M64, E, dig);
   return cudaGetLastError();
 }

@@ -57,9 +57,12 @@ struct SplitLayout {
 
 void split_build_layout(int n_pairs, const int* pair_M, const int* pair_aoff, SplitLayout& out);
 
-// chunks of one pass: runs of points sharing an energy, at most kSplitMaxChunk long
+// chunks of one pass: points sharing an energy, at most kSplitMaxChunk of them; point s
+// of chunk c sits in slot slot0[c] + s * stride of the pass (stride 1 for a pass in mesh
+// order, the number of energies for a k-major pass over a tabulated mesh)
 struct SplitChunks {
   std::vector<int> slot0, count, kstart, kchunk;   // kstart has n_chunks + 1 entries
+  int stride = 1;
   int n_ksteps() const { return kstart.empty() ? 0 : kstart.back(); }
   int n_chunks() const { return (int)count.size(); }
 };
@@ -67,6 +70,7 @@ struct SplitChunks {
 // device views used by the kernels
 struct SplitPassDev {
   int n_chunks = 0, n_ksteps = 0;
+  int stride = 1;
   const int* slot0 = nullptr;
   const int* count = nullptr;
   const int* kstart = nullptr;
