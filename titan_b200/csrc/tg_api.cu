@@ -36,6 +36,10 @@ template <class T>
 struct DevArray {
   T* p = nullptr;
   size_t n = 0;
+  DevArray() = default;
+  DevArray(const DevArray&) = delete;
+  DevArray& operator=(const DevArray&) = delete;
+  ~DevArray() { free_(); }
   void free_() {
     if (p) cudaFree(p);
     p = nullptr;
@@ -496,7 +500,7 @@ int tg_destroy(tg_ctx* c) {
     cudaEventDestroy(u.second.second);
   }
   if (c->stream) cudaStreamDestroy(c->stream);
-  delete c;
+  delete c;   // every DevArray member frees what the calls above did not
   return TG_OK;
 }
 
