@@ -883,6 +883,9 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     cudaEventElapsedTime(&ms, ev[2], ev[4]);
     t_con += ms;   // includes the G1 inversions of w >= 1 (split below is approximate)
   }
+  // the real-axis time is measured from here (also when the imaginary-axis list is empty:
+  // an event that was never recorded would make cudaEventElapsedTime fail below)
+  TG_CHECK(c, cudaEventRecord(ev[4], s), "event");
   // ---------------- real axis ----------------
   for (int w = 0; w < n_omega; ++w) {
     if (std::fabs(e[w]) < 1e-15) continue;

@@ -21,6 +21,14 @@ LIB_PATH = os.path.join(HERE, "libtitan_gpu.so")
 
 TG_PREC_FP64 = 0
 TG_PREC_SPLIT = 1
+# status codes of titan_gpu.h (> 0: 1-based index of a singular (k, z) point)
+TG_OK = 0
+TG_ERR_ARG = -1
+TG_ERR_CUDA = -2
+TG_ERR_STATE = -3
+TG_ERR_TIMEOUT = -4
+TG_ERR_NOMEM = -5
+TG_ERR_NUMERIC = -6
 _PREC = {"fp64": TG_PREC_FP64, "split": TG_PREC_SPLIT}
 
 _lib = None
