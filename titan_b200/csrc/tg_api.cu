@@ -103,6 +103,7 @@ struct tg_ctx {
   DevArray<SplitTile> d_stiles;
   DevArray<int8_t> d_digA, d_digB;
   DevArray<unsigned long long> d_m64A, d_m64B;
+  DevArray<int16_t> d_e16A, d_e16B;   // exponent sidecars of the FP64 operands (spectral G)
   DevArray<int> d_EA, d_EB, d_chunks, d_split_err;
   std::vector<double> h_y;   // imaginary-axis energies per point (chunk boundaries)
   std::vector<double> h_klist_u, h_rkp;   // host copies of the uniform k list and the real-axis BZ
@@ -408,11 +409,15 @@ int split_prepare(tg_ctx* c, const SplitChunks& ch, SplitPassDev& pd) {
 }
 
 // FP64 operand of a pass -> digits (which = 0: A, 1: B)
-int split_quantize_operand(tg_ctx* c, int which, const double2* X, const SplitPassDev& pd) {
+// (e16: the operand's exponent sidecar when its Green functions wrote one, else null)
+int split_quantize_operand(tg_ctx* c, int which, const double2* X, const SplitPassDev& pd, const int16_t* e16) {
   const int64_t ld = (int64_t)c->dimH * c->dimH;
   unsigned long long* m64 = which ? c->d_m64B.p : c->d_m64A.p;
   TG_CHECK(c, cudaMemsetAsync(m64, 0, sizeof(unsigned long long) * pd.n_chunks * ld, c->stream), "memset");
-  TG_CHECK(c, split_rowmax(X, ld, pd, m64, c->stream), "split rowmax");
+  if (e16)
+    TG_CHECK(c, split_rowmax_e16(e16, ld, pd, m64, c->stream), "split rowmax (sidecar)");
+  else
+    TG_CHECK(c, split_rowmax(X, ld, pd, m64, c->stream), "split rowmax");
   if (which == 0)
     TG_CHECK(c, split_quantize(X, ld, pd, c->d_sgA.p, (int)c->split.groupsA.size(), kSplitRowsA, m64, c->d_EA.p,
                                c->d_digA.p, c->stream),
@@ -740,6 +745,8 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   const int nsplit = split ? split_nsplit((int)c->split.tiles.size(), c->num_sms, P / kSplitK) : nsplit_for(c);
   if (split) {
     TG_CHECK(c, c->d_split_err.ensure(1), "alloc");
+    TG_CHECK(c, c->d_e16A.ensure((size_t)P * nn), "alloc exponents A");
+    TG_CHECK(c, c->d_e16B.ensure((size_t)P * nn), "alloc exponents B");
     TG_CHECK(c, cudaMemsetAsync(c->d_split_err.p, 0, sizeof(int), s), "memset");
   }
   TG_CHECK(c, c->d_A.ensure((size_t)P * nn), "alloc A");
@@ -814,6 +821,12 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       g2.mode2 = MODE_A_IMAG;
       w_start = 1;
     }
+    // the split row maxima read exponent sidecars when the spectral kernel writes G
+    const bool e16_g2 = split && green_is_spectral(g2);
+    if (e16_g2) {
+      g2.eout = c->d_e16B.p;
+      if (g2.out2) g2.eout2 = c->d_e16A.p;
+    }
     cudaEventRecord(ev[1], s);
     {
       KindTimer kt(c, 0);
@@ -828,13 +841,13 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       const SplitChunks ch = tab_imag ? make_chunks_kmajor(p0, np, c->n_e_u)
                                       : make_chunks(np, [&](int64_t i) { return yv[i]; });
       if ((rc = split_prepare(c, ch, pd))) return rc;
-      if ((rc = split_quantize_operand(c, 1, c->d_B.p, pd))) return rc;
+      if ((rc = split_quantize_operand(c, 1, c->d_B.p, pd, e16_g2 ? c->d_e16B.p : nullptr))) return rc;
     }
     if (w_start == 1) {
       if (split) {
         {
           KindTimer kq(c, 3);
-          if ((rc = split_quantize_operand(c, 0, c->d_A.p, pd))) return rc;
+          if ((rc = split_quantize_operand(c, 0, c->d_A.p, pd, e16_g2 ? c->d_e16A.p : nullptr))) return rc;
         }
         KindTimer kt(c, 1);
         rc = split_contract_pass(c, pd, c->d_C.p, nsplit, cstride);
@@ -847,6 +860,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     for (int w = w_start; w < n_omega; ++w) {
       GreenArgs g1 = g2;
       g1.out2 = nullptr;
+      g1.eout = g1.eout2 = nullptr;
       g1.zr = Ef + e[w];
       g1.zi = eta;
       g1.q[0] = q[0]; g1.q[1] = q[1]; g1.q[2] = q[2];
@@ -856,6 +870,8 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
         use_table(g1, q_zero ? 0 : 1, c->n_e_u, c->nk_u, c->d_ylist.p);
         g1.q[0] = g1.q[1] = g1.q[2] = 0.0;   // q is inside the table
       }
+      const bool e16_g1 = split && green_is_spectral(g1);
+      if (e16_g1) g1.eout = c->d_e16A.p;
       {
         KindTimer kt(c, 0);
         TG_CHECK(c, launch_green(g1, c->num_sms, s, nullptr), "green (imag, G1)");
@@ -865,7 +881,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
         if (split) {
           {
             KindTimer kq(c, 3);
-            rc = split_quantize_operand(c, 0, c->d_A.p, pd);
+            rc = split_quantize_operand(c, 0, c->d_A.p, pd, e16_g1 ? c->d_e16A.p : nullptr);
           }
           KindTimer kt(c, 1);
           if (!rc) rc = split_contract_pass(c, pd, Cw, nsplit, cstride);
@@ -907,6 +923,8 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       gr.mode = MODE_B_REAL;
       gr.out = c->d_B.p;
       if (tab_real) use_table(gr, rslot0, n_real, c->n_realk, nullptr);
+      const bool e16_rb = split && green_is_spectral(gr);
+      gr.eout = e16_rb ? c->d_e16B.p : nullptr;
       {
         KindTimer kt(c, 0);
         TG_CHECK(c, launch_green(gr, c->num_sms, s, nullptr), "green (real, G2)");
@@ -921,6 +939,8 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
         use_table(gr, q_zero ? rslot0 : rslot1, n_real, c->n_realk, nullptr);
         gr.q[0] = gr.q[1] = gr.q[2] = 0.0;
       }
+      const bool e16_ra = split && green_is_spectral(gr);
+      gr.eout = e16_ra ? c->d_e16A.p : nullptr;
       {
         KindTimer kt(c, 0);
         TG_CHECK(c, launch_green(gr, c->num_sms, s, nullptr), "green (real, G1)");
@@ -935,8 +955,8 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
             const SplitChunks ch = tab_real ? make_chunks_kmajor(pbase, np, n_real)
                                             : make_chunks(np, [&](int64_t i) { return (pbase + i) / nrk; });
             rc = split_prepare(c, ch, pr);
-            if (!rc) rc = split_quantize_operand(c, 1, c->d_B.p, pr);
-            if (!rc) rc = split_quantize_operand(c, 0, c->d_A.p, pr);
+            if (!rc) rc = split_quantize_operand(c, 1, c->d_B.p, pr, e16_rb ? c->d_e16B.p : nullptr);
+            if (!rc) rc = split_quantize_operand(c, 0, c->d_A.p, pr, e16_ra ? c->d_e16A.p : nullptr);
           }
           KindTimer kt(c, 1);
           if (!rc) rc = split_contract_pass(c, pr, Dw, nsplit, cstride);

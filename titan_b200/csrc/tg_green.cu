@@ -505,11 +505,16 @@ int green_acc_ctas(int n, int64_t np, int num_sms) {
   return (int)std::max<int64_t>(g, 1);
 }
 
+bool green_is_spectral(const GreenArgs& a) {
+  return a.eigU && a.eigL && a.htab && spectral_supported(a.mode, a.mode2, a.out2 != nullptr);
+}
+
 cudaError_t launch_green(const GreenArgs& a, int num_sms, cudaStream_t s, int* grid_used) {
-  if (a.eigU && a.eigL && a.htab && spectral_supported(a.mode, a.mode2, a.out2 != nullptr)) {
+  if (green_is_spectral(a)) {
     if (grid_used) *grid_used = 0;
     return launch_green_spectral(a, a.eigU, a.eigL, a.outinv, num_sms, s);
   }
+  if (a.eout || a.eout2) return cudaErrorInvalidValue;   // only the spectral kernel writes sidecars
   if (green_w1_supported(a.n, a.mode)) return launch_green_w1(a, num_sms, s, grid_used);
   if (green_warp_supported(a.n, a.mode)) return launch_green_warp(a, num_sms, s, grid_used);
   const Cfg* c = find_cfg(a.n);

@@ -139,7 +139,15 @@ struct GreenArgs {
   const double2* eigU = nullptr;
   const double* eigL = nullptr;
   const int* outinv = nullptr;
+  // optional exponent sidecars of out / out2 (spectral G only): per stored value the
+  // frexp exponent of max(|Re|, |Im|), -32768 for zero or subnormal
+  int16_t* eout = nullptr;
+  int16_t* eout2 = nullptr;
 };
+
+// true when launch_green evaluates these arguments with the spectral kernel (the only
+// one that writes exponent sidecars)
+bool green_is_spectral(const GreenArgs& a);
 
 // Launch the fused H(k) + Gauss-Jordan kernel for any supported n.
 // Returns cudaErrorInvalidValue for an unsupported dimension.

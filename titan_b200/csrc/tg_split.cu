@@ -46,6 +46,35 @@ __global__ void split_rowmax_kernel(const double2* __restrict__ X, int64_t ld, i
   }
 }
 
+// the same maxima from the exponent sidecar of the spectral G kernel (int16 per value,
+// ld even): the largest exponent E of a chunk and element is stored as the bits of
+// 2^(E - 1), whose frexp exponent is E, so the quantiser sees the scale it would get
+// from the FP64 values; the pass reads 2 bytes per value instead of 16
+__global__ void split_rowmax_e16_kernel(const int16_t* __restrict__ E16, int64_t ld, int stride,
+                                        const int* __restrict__ slot0, const int* __restrict__ count,
+                                        unsigned long long* __restrict__ M64) {
+  const int c = blockIdx.y;
+  const int cnt = count[c];
+  const int s_begin = blockIdx.x * kRowmaxSlots;
+  if (s_begin >= cnt) return;
+  const int s_end = min(cnt, s_begin + kRowmaxSlots);
+  const int64_t base = (int64_t)slot0[c];
+  const int64_t ld2 = ld / 2;
+  const uint32_t* W = reinterpret_cast<const uint32_t*>(E16);
+  for (int64_t e2 = threadIdx.x; e2 < ld2; e2 += blockDim.x) {
+    int m0 = -32768, m1 = -32768;
+    for (int s = s_begin; s < s_end; ++s) {
+      const uint32_t w = W[((base + (int64_t)s * stride) * ld) / 2 + e2];
+      m0 = max(m0, (int)(int16_t)(w & 0xffffu));
+      m1 = max(m1, (int)(int16_t)(w >> 16));
+    }
+    if (m0 > -32768)
+      atomicMax(&M64[(int64_t)c * ld + 2 * e2], (unsigned long long)(m0 - 1 + 1023) << 52);
+    if (m1 > -32768)
+      atomicMax(&M64[(int64_t)c * ld + 2 * e2 + 1], (unsigned long long)(m1 - 1 + 1023) << 52);
+  }
+}
+
 // Balanced base-256 digits of 16 integers |X| <= 2^38, slice-major: out[0] holds
 // the top digits, out[1..4] the lower ones (most significant first).  With
 // Y = X + 0x80808080 the low four balanced digits are the bytes of the low word
@@ -541,6 +570,15 @@ cudaError_t split_rowmax(const double2* X, int64_t ld, const SplitPassDev& p, un
   if (p.n_chunks <= 0) return cudaSuccess;
   const int gx = (kSplitMaxChunk + kRowmaxSlots - 1) / kRowmaxSlots;
   split_rowmax_kernel<<<dim3(gx, p.n_chunks), 256, 0, s>>>(X, ld, p.stride, p.slot0, p.count, M64);
+  return cudaGetLastError();
+}
+
+cudaError_t split_rowmax_e16(const int16_t* E16, int64_t ld, const SplitPassDev& p, unsigned long long* M64,
+                             cudaStream_t s) {
+  if (p.n_chunks <= 0) return cudaSuccess;
+  if (ld % 2) return cudaErrorInvalidValue;
+  const int gx = (kSplitMaxChunk + kRowmaxSlots - 1) / kRowmaxSlots;
+  split_rowmax_e16_kernel<<<dim3(gx, p.n_chunks), 256, 0, s>>>(E16, ld, p.stride, p.slot0, p.count, M64);
   return cudaGetLastError();
 }
 

@@ -82,6 +82,11 @@ struct SplitPassDev {
 cudaError_t split_rowmax(const double2* X, int64_t ld, const SplitPassDev& p, unsigned long long* M64,
                          cudaStream_t s);
 
+// the same maxima (as the bits of 2^(E - 1), E the largest frexp exponent) from an int16
+// exponent sidecar of the operand; ld must be even
+cudaError_t split_rowmax_e16(const int16_t* E16, int64_t ld, const SplitPassDev& p, unsigned long long* M64,
+                             cudaStream_t s);
+
 // digits of one operand for a pass; writes E[c * ld + e] for every valid element
 cudaError_t split_quantize(const double2* X, int64_t ld, const SplitPassDev& p, const SplitGroup* groups,
                            int n_groups, int rows, const unsigned long long* M64, int* E, int8_t* dig,
