@@ -238,6 +238,9 @@ __device__ __forceinline__ int16_t exponent_code(double2 v) {
 
 // five CTAs per SM (the occupancy its ~30 KB of shared memory allows at n = 36): 48
 // registers with a 4-byte spill, measured faster than 64 registers at four CTAs
+// ANTI (MODE_A_REAL, w (G - G^+)): the diagonal -2i y / |z - lambda|^2 is purely
+// imaginary, so two of the four DMMAs per step would multiply by zero and are skipped
+template <bool ANTI>
 __global__ void __launch_bounds__(kSpecThreads, 5) spec_green_kernel(SpecArgs sa) {
   extern __shared__ __align__(16) unsigned char smem[];
   const GreenArgs& a = sa.g;
@@ -252,7 +255,7 @@ __global__ void __launch_bounds__(kSpecThreads, 5) spec_green_kernel(SpecArgs sa
   const int64_t per_k = (ne + kSpecZ - 1) / kSpecZ;
   const int64_t ik0 = a.p0 / ne, ik1 = (a.p0 + a.np - 1) / ne;
   const int64_t ntask = (ik1 - ik0 + 1) * per_k;
-  const bool anti = a.mode == MODE_A_REAL;
+  const bool anti = ANTI;
   for (int64_t t = blockIdx.x; t < ntask; t += gridDim.x) {
     const int64_t ik = ik0 + t / per_k;
     const int64_t ie0 = (t % per_k) * kSpecZ;
@@ -322,9 +325,9 @@ __global__ void __launch_bounds__(kSpecThreads, 5) spec_green_kernel(SpecArgs sa
 #pragma unroll
         for (int mf = 0; mf < 2; ++mf) {
           const double2 dv = Ds[(mf * 8 + g8) * kp + ka];
-          dmma(cr[mf][0], cr[mf][1], dv.x, pv.x);
+          if (!ANTI) dmma(cr[mf][0], cr[mf][1], dv.x, pv.x);
           dmma(cr[mf][0], cr[mf][1], -dv.y, pv.y);
-          dmma(ci[mf][0], ci[mf][1], dv.x, pv.y);
+          if (!ANTI) dmma(ci[mf][0], ci[mf][1], dv.x, pv.y);
           dmma(ci[mf][0], ci[mf][1], dv.y, pv.x);
         }
       }
@@ -534,16 +537,18 @@ cudaError_t launch_green_spectral(const GreenArgs& g, const double2* U, const do
   sa.outinv = outinv;
   sa.kp = (g.n + 3) / 4 * 4;
   const size_t smem = spec_smem(g.n, sa.kp);
-  cudaError_t e = cudaFuncSetAttribute(spec_green_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const bool anti = g.mode == MODE_A_REAL;
+  auto kernel = anti ? spec_green_kernel<true> : spec_green_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spec_green_kernel, kSpecThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kSpecThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm <= 0) return cudaErrorInvalidValue;
   const int64_t ne = g.n_e;
   const int64_t ntask = ((g.p0 + g.np - 1) / ne - g.p0 / ne + 1) * ((ne + kSpecZ - 1) / kSpecZ);
   const int64_t grid = std::min<int64_t>(ntask, (int64_t)num_sms * per_sm);
-  spec_green_kernel<<<(unsigned)grid, kSpecThreads, smem, s>>>(sa);
+  kernel<<<(unsigned)grid, kSpecThreads, smem, s>>>(sa);
   return cudaGetLastError();
 }
 
