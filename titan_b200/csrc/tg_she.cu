@@ -56,10 +56,11 @@ struct SheSmem {
   size_t bytes;
 };
 
-// Shared-memory layout.  STAGED: both Green functions (row-major) and the df
-// partial live in shared memory; otherwise they are read from / accumulated in
-// global memory (L1 / L2) and only V, V^T, Y and the tables are staged.
-__host__ __device__ inline SheSmem she_layout(int n, int dimens, int n_neigh, bool staged) {
+// Shared-memory layout.  STAGED: both Green functions (row-major) live in shared
+// memory, and the df partial too unless it is held in registers (acc_smem false);
+// otherwise they are read from / accumulated in global memory (L1 / L2) and only
+// V, V^T, Y and the tables are staged.
+__host__ __device__ inline SheSmem she_layout(int n, int dimens, int n_neigh, bool staged, bool acc_smem = true) {
   const int no = n / 2;
   SheSmem L;
   int o = 0;
@@ -68,7 +69,7 @@ __host__ __device__ inline SheSmem she_layout(int n, int dimens, int n_neigh, bo
   L.m = o; o += no * no;
   L.mt = o; o += no * no;
   L.y = o; o += 2 * n * no;
-  L.acc = o; o += staged ? 4 * dimens : 0;
+  L.acc = o; o += staged && acc_smem ? 4 * dimens : 0;
   L.ph = o; o += n_neigh > 0 ? n_neigh : 1;
   L.tab = o * (int)sizeof(double2);
   L.bytes = (size_t)L.tab + sizeof(int) * 4 * (size_t)no;
@@ -100,9 +101,9 @@ struct ColMajor {
 // One sandwich term.  M: no x no row-major (the middle factor as used: V or V^T).
 // Z(r, col) = sum_{o1, o2} L(r, row_b(o2)) M(o2, o1) R(row_c(o1), col) for the
 // output rows (r, col) of each df entry; acc[s' dimens + row] += f Z.
-template <class LM, class RM>
-__device__ void she_term(const SheArgs& a, LM L, const double2* M, RM R, double2* Y, double2* acc, const int* tab,
-                         const unsigned char* spins, double2 f, bool rows_are_nu) {
+// First stage: Y^b = L[:, spin b] M for both spins b (2 n x no).
+template <class LM>
+__device__ void she_y(const SheArgs& a, LM L, const double2* M, double2* Y, const int* tab) {
   const int n = a.n, no = a.no;
   for (int e = threadIdx.x; e < 2 * n * no; e += blockDim.x) {
     const int b = e / (n * no), r = (e / no) % n, o1 = e % no;
@@ -112,30 +113,60 @@ __device__ void she_term(const SheArgs& a, LM L, const double2* M, RM R, double2
     Y[e] = s;
   }
   __syncthreads();
-  const int D = a.dimens;
-  for (int o = threadIdx.x; o < 4 * D; o += blockDim.x) {
-    const int sp = o / D, row = o % D;
-    const int dec = a.decode[row];
-    const int sigma = dec & 3, i = (dec >> 2) & 1023, mu = (dec >> 12) & 63, nu = (dec >> 18) & 63;
-    const int code = spins[sigma * 4 + sp];
-    const int sa = (code >> 3) & 1, b = (code >> 2) & 1, c = (code >> 1) & 1, sd = code & 1;
-    const int x = rows_are_nu ? nu : mu, y = rows_are_nu ? mu : nu;
-    const int ni = a.norb[i];
-    const int r = a.ia[i] + sa * ni + x, col = a.ia[i] + sd * ni + y;
-    const double2* Yr = Y + (b * n + r) * no;
-    const int* rowc = tab + c * no;
-    double2 s = make_double2(0, 0);
-    for (int o1 = 0; o1 < no; ++o1) s = cfma(Yr[o1], R(rowc[o1], col), s);
-    acc[o] = cfma(f, s, acc[o]);
+}
+
+// Second stage for df entry o = s' dimens + row: Z(r, col) of that entry.
+template <class RM>
+__device__ __forceinline__ double2 she_z(const SheArgs& a, int o, const double2* Y, RM R, const int* tab,
+                                         const unsigned char* spins, bool rows_are_nu) {
+  const int n = a.n, no = a.no, D = a.dimens;
+  const int sp = o / D, row = o % D;
+  const int dec = a.decode[row];
+  const int sigma = dec & 3, i = (dec >> 2) & 1023, mu = (dec >> 12) & 63, nu = (dec >> 18) & 63;
+  const int code = spins[sigma * 4 + sp];
+  const int sa = (code >> 3) & 1, b = (code >> 2) & 1, c = (code >> 1) & 1, sd = code & 1;
+  const int x = rows_are_nu ? nu : mu, y = rows_are_nu ? mu : nu;
+  const int ni = a.norb[i];
+  const int r = a.ia[i] + sa * ni + x, col = a.ia[i] + sd * ni + y;
+  const double2* Yr = Y + (b * n + r) * no;
+  const int* rowc = tab + c * no;
+  double2 s = make_double2(0, 0);
+  for (int o1 = 0; o1 < no; ++o1) s = cfma(Yr[o1], R(rowc[o1], col), s);
+  return s;
+}
+
+// the term with the df slice in memory (shared or global)
+template <class LM, class RM>
+__device__ void she_term(const SheArgs& a, LM L, const double2* M, RM R, double2* Y, double2* acc, const int* tab,
+                         const unsigned char* spins, double2 f, bool rows_are_nu) {
+  she_y(a, L, M, Y, tab);
+  for (int o = threadIdx.x; o < 4 * a.dimens; o += blockDim.x)
+    acc[o] = cfma(f, she_z(a, o, Y, R, tab, spins, rows_are_nu), acc[o]);
+  __syncthreads();
+}
+
+// the term with the df slice in registers: entry o = threadIdx.x + i blockDim.x in racc[i]
+template <int RACC, class LM, class RM>
+__device__ void she_term_reg(const SheArgs& a, LM L, const double2* M, RM R, double2* Y, double2 (&racc)[RACC],
+                             const int* tab, const unsigned char* spins, double2 f, bool rows_are_nu) {
+  she_y(a, L, M, Y, tab);
+#pragma unroll
+  for (int i = 0; i < RACC; ++i) {
+    const int o = threadIdx.x + i * blockDim.x;
+    if (o < 4 * a.dimens) racc[i] = cfma(f, she_z(a, o, Y, R, tab, spins, rows_are_nu), racc[i]);
   }
   __syncthreads();
 }
 
-template <bool STAGED>
-__global__ void __launch_bounds__(256) she_kernel(SheArgs a) {
+// STAGED: Green functions in shared memory; RACC > 0 (staged only): the df slice in
+// RACC registers per thread (4 dimens <= RACC x 256), which leaves the shared memory
+// to the Green functions, V and Y and fits three CTAs per SM at dimH 36
+template <bool STAGED, int RACC>
+__device__ __forceinline__ void she_body(const SheArgs& a) {
+  static_assert(STAGED || RACC == 0, "register slices only in the staged kernel");
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = a.n, no = a.no, D = a.dimens;
-  const SheSmem L = she_layout(n, D, a.n_neigh, STAGED);
+  const SheSmem L = she_layout(n, D, a.n_neigh, STAGED, RACC == 0);
   double2* base = reinterpret_cast<double2*>(smem);
   double2* S1 = base + L.s1;
   double2* S2 = base + L.s2;
@@ -145,9 +176,17 @@ __global__ void __launch_bounds__(256) she_kernel(SheArgs a) {
   double2* ph = base + L.ph;
   int* tab = reinterpret_cast<int*>(smem + L.tab);
   double2* mine = a.partial + (size_t)blockIdx.x * 4 * D;
-  double2* acc = STAGED ? base + L.acc : mine;
-  if (STAGED)
+  double2* acc = STAGED && RACC == 0 ? base + L.acc : mine;
+  double2 racc[RACC > 0 ? RACC : 1];
+  if (RACC > 0) {
+#pragma unroll
+    for (int i = 0; i < (RACC > 0 ? RACC : 1); ++i) {
+      const int o = threadIdx.x + i * blockDim.x;
+      racc[i] = o < 4 * D ? mine[o] : make_double2(0.0, 0.0);
+    }
+  } else if (STAGED) {
     for (int e = threadIdx.x; e < 4 * D; e += blockDim.x) acc[e] = mine[e];
+  }
   for (int e = threadIdx.x; e < 4 * no; e += blockDim.x) tab[e] = a.tab[e];
   __syncthreads();
   for (int64_t pl = blockIdx.x; pl < a.np; pl += gridDim.x) {
@@ -214,7 +253,20 @@ __global__ void __launch_bounds__(256) she_kernel(SheArgs a) {
       MT[cc * no + rr] = v;
     }
     __syncthreads();
-    if (STAGED) {
+    if (STAGED && RACC > 0) {
+      if (!a.real_axis) {
+        she_term_reg(a, RowMajor{S1, n}, M, RowMajor{S2, n}, Y, racc, tab, a.spins[0], make_double2(w, 0.0), true);
+        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+          S1[e].y = -S1[e].y;
+          S2[e].y = -S2[e].y;
+        }
+        __syncthreads();
+        she_term_reg(a, RowMajor{S2, n}, MT, RowMajor{S1, n}, Y, racc, tab, a.spins[1], make_double2(w, 0.0),
+                     false);
+      } else {
+        she_term_reg(a, RowMajor{S1, n}, M, RowMajor{S2, n}, Y, racc, tab, a.spins[2], make_double2(0.0, -w), true);
+      }
+    } else if (STAGED) {
       if (!a.real_axis) {
         she_term(a, RowMajor{S1, n}, M, RowMajor{S2, n}, Y, acc, tab, a.spins[0], make_double2(w, 0.0), true);
         for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
@@ -238,8 +290,26 @@ __global__ void __launch_bounds__(256) she_kernel(SheArgs a) {
       }
     }
   }
-  if (STAGED)
+  if (RACC > 0) {
+#pragma unroll
+    for (int i = 0; i < (RACC > 0 ? RACC : 1); ++i) {
+      const int o = threadIdx.x + i * blockDim.x;
+      if (o < 4 * D) mine[o] = racc[i];
+    }
+  } else if (STAGED) {
     for (int e = threadIdx.x; e < 4 * D; e += blockDim.x) mine[e] = acc[e];
+  }
+}
+
+template <bool STAGED>
+__global__ void __launch_bounds__(256) she_kernel(SheArgs a) {
+  she_body<STAGED, 0>(a);
+}
+
+// the register-slice variant: 127 registers, two CTAs per SM (a three-CTA bound spills)
+constexpr int kSheRacc = 12;
+__global__ void __launch_bounds__(256, 2) she_kernel_reg(SheArgs a) {
+  she_body<true, kSheRacc>(a);
 }
 
 // tchi(r, s') = scale sum_c P(r, c) df(c, s'), P column-major (dimens x dimens); P == nullptr: identity
@@ -259,29 +329,47 @@ __global__ void she_prefactor_kernel(const double2* __restrict__ P, const double
 
 }  // namespace
 
-// Variant choice: the staged kernel when its shared memory fits, else the
-// global-operand kernel; 0 bytes when neither fits.
-bool she_staged(int n, int dimens, int n_neigh, size_t optin) {
-  return she_layout(n, dimens, n_neigh, true).bytes <= optin;
+// Variant choice: the staged kernel with register slices when 4 dimens <= kSheRacc x 256
+// and its shared memory fits, else the staged kernel with the slice in shared memory,
+// else the global-operand kernel; 0 bytes when none fits.
+enum SheVariant { SHE_GLOBAL = 0, SHE_STAGED = 1, SHE_STAGED_REG = 2 };
+
+SheVariant she_variant(int n, int dimens, int n_neigh, size_t optin) {
+  if (4 * dimens <= kSheRacc * 256 && she_layout(n, dimens, n_neigh, true, false).bytes <= optin)
+    return SHE_STAGED_REG;
+  if (she_layout(n, dimens, n_neigh, true).bytes <= optin) return SHE_STAGED;
+  return SHE_GLOBAL;
 }
 
-size_t she_smem_bytes(int n, int dimens, int n_neigh) {
+size_t she_variant_bytes(int n, int dimens, int n_neigh, SheVariant v) {
+  return she_layout(n, dimens, n_neigh, v != SHE_GLOBAL, v != SHE_STAGED_REG).bytes;
+}
+
+const void* she_variant_fn(SheVariant v) {
+  if (v == SHE_STAGED_REG) return (const void*)she_kernel_reg;
+  if (v == SHE_STAGED) return (const void*)she_kernel<true>;
+  return (const void*)she_kernel<false>;
+}
+
+int she_optin() {
   int dev = 0, optin = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
-  const bool staged = she_staged(n, dimens, n_neigh, (size_t)optin);
-  const size_t b = she_layout(n, dimens, n_neigh, staged).bytes;
+  return optin;
+}
+
+size_t she_smem_bytes(int n, int dimens, int n_neigh) {
+  const int optin = she_optin();
+  const size_t b = she_variant_bytes(n, dimens, n_neigh, she_variant(n, dimens, n_neigh, (size_t)optin));
   return b <= (size_t)optin ? b : 0;
 }
 
 int she_grid(int n, int dimens, int n_neigh, int num_sms) {
-  int dev = 0, optin = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
-  const bool staged = she_staged(n, dimens, n_neigh, (size_t)optin);
-  const size_t smem = she_layout(n, dimens, n_neigh, staged).bytes;
+  const int optin = she_optin();
+  const SheVariant v = she_variant(n, dimens, n_neigh, (size_t)optin);
+  const size_t smem = she_variant_bytes(n, dimens, n_neigh, v);
   if (smem > (size_t)optin) return 0;
-  const void* fn = staged ? (const void*)she_kernel<true> : (const void*)she_kernel<false>;
+  const void* fn = she_variant_fn(v);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem) != cudaSuccess) return 0;
@@ -318,22 +406,19 @@ cudaError_t launch_she(const SheLaunch& l, cudaStream_t s) {
   a.n_e = l.n_e;
   a.nk_tab = l.nk_tab;
   a.klist = l.klist;
-  int dev = 0, optin = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (e != cudaSuccess) return e;
-  const bool staged = she_staged(a.n, a.dimens, a.n_neigh, (size_t)optin);
-  const size_t smem = she_layout(a.n, a.dimens, a.n_neigh, staged).bytes;
+  const int optin = she_optin();
+  if (optin <= 0) return cudaErrorInvalidValue;
+  const SheVariant v = she_variant(a.n, a.dimens, a.n_neigh, (size_t)optin);
+  const size_t smem = she_variant_bytes(a.n, a.dimens, a.n_neigh, v);
   if (smem > (size_t)optin) return cudaErrorInvalidValue;
-  if (staged) {
-    e = cudaFuncSetAttribute(she_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+  cudaError_t e = cudaFuncSetAttribute(she_variant_fn(v), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (v == SHE_STAGED_REG)
+    she_kernel_reg<<<l.grid, 256, smem, s>>>(a);
+  else if (v == SHE_STAGED)
     she_kernel<true><<<l.grid, 256, smem, s>>>(a);
-  } else {
-    e = cudaFuncSetAttribute(she_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+  else
     she_kernel<false><<<l.grid, 256, smem, s>>>(a);
-  }
   return cudaGetLastError();
 }
 
