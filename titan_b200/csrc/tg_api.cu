@@ -132,7 +132,7 @@ struct tg_ctx {
   DevArray<int> d_jij_tab;
   DevArray<double2> d_jij_part, d_jij_sum;
   // disturbance response (eintshe)
-  DevArray<int> d_she_tab, d_ia;
+  DevArray<int> d_she_tab, d_ia, d_she_ztiles, d_she_rowoff;
   DevArray<double2> d_she_part, d_she_sum, d_she_pref, d_she_out;
 };
 
@@ -1814,6 +1814,23 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
   }
   TG_CHECK(c, c->d_she_tab.upload(tab.data(), tab.size(), s), "upload tables");
   TG_CHECK(c, c->d_ia.upload(c->ia.data(), c->ia.size(), s), "upload ia");
+  // vertex second stage: 3 x 3 tiles of every (sigma, s', site) block of n_i x n_i df
+  // entries, and the first df row of each site (rows in sigmaimunu2i order: sigma fastest,
+  // then nu, mu, site)
+  const int nat = c->n_atoms;
+  std::vector<int> ztiles, rowoff(nat);
+  for (int i = 0, off = 0; i < nat; ++i) {
+    rowoff[i] = off;
+    off += 4 * c->norb[i] * c->norb[i];
+  }
+  for (int sg = 0; sg < 4; ++sg)
+    for (int sp = 0; sp < 4; ++sp)
+      for (int i = 0; i < nat; ++i)
+        for (int x0 = 0; x0 < c->norb[i]; x0 += 3)
+          for (int y0 = 0; y0 < c->norb[i]; y0 += 3) ztiles.push_back(sg | sp << 2 | i << 4 | x0 << 14 | y0 << 20);
+  TG_CHECK(c, c->d_she_ztiles.upload(ztiles.data(), ztiles.size(), s), "upload tiles");
+  TG_CHECK(c, c->d_she_rowoff.upload(rowoff.data(), rowoff.size(), s), "upload");
+  const int n_ztiles = (int)ztiles.size();
   TG_CHECK(c, c->d_she_part.ensure((size_t)grid * 4 * D), "alloc partials");
   TG_CHECK(c, c->d_she_sum.ensure((size_t)4 * D), "alloc");
   TG_CHECK(c, c->d_she_out.ensure((size_t)4 * D), "alloc");
@@ -1875,6 +1892,9 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
   l.ia = c->d_ia.p;
   l.norb = c->d_norb.p;
   l.decode = c->d_decode.p;
+  l.ztiles = c->d_she_ztiles.p;
+  l.n_ztiles = n_ztiles;
+  l.rowoff = c->d_she_rowoff.p;
   for (int i = 0; i < 3; ++i) l.ue[i] = efield[i];
   she_spin_codes(l.spins);
   l.partial = c->d_she_part.p;

@@ -217,6 +217,11 @@ struct SheLaunch {
   const int* ia = nullptr;
   const int* norb = nullptr;
   const int* decode = nullptr;
+  // register-tiled second stage: 3 x 3 tiles of the (sigma, s', site) output blocks, code
+  // sigma | s' << 2 | site << 4 | x0 << 14 | y0 << 20, and the first df row of each site
+  const int* ztiles = nullptr;
+  int n_ztiles = 0;
+  const int* rowoff = nullptr;
   double ue[3] = {0, 0, 0};
   unsigned char spins[3][16] = {};
   double2* partial = nullptr;     // [grid][4 dimens]

@@ -14,7 +14,10 @@
 // Work split: one CTA per point at a time (grid-stride), V built in shared
 // memory from per-neighbour phases, then two small products per term:
 // Y^b = L[:, spin b] V (n x no) and Z = Y^b R[spin c, :] restricted to the
-// output entries.  Each CTA owns a slice (4 dimens complex) of a per-CTA
+// output entries, which form n_i x n_i blocks per (sigma, s', site).  Both
+// products are register-tiled (3 x 3 outputs per thread), so each operand read
+// from shared memory feeds three complex FMAs; shared-memory bandwidth bounds
+// the kernel.  Each CTA owns a slice (4 dimens complex) of a per-CTA
 // global array, so successive launches (passes) accumulate without atomics;
 // the slices are summed once at the end.  When they fit (dimH up to about 48
 // for small dimens), both Green functions are staged row-major in shared memory
@@ -43,6 +46,9 @@ struct SheArgs {
   const int* ia = nullptr;        // first row of each site
   const int* norb = nullptr;
   const int* decode = nullptr;    // [dimens] sigma | i << 2 | mu << 12 | nu << 18
+  const int* ztiles = nullptr;    // second-stage tiles: sigma | s' << 2 | i << 4 | x0 << 14 | y0 << 20
+  int n_ztiles = 0;
+  const int* rowoff = nullptr;    // first df row of each site
   int real_axis = 0;
   double ue[3] = {0, 0, 0};
   unsigned char spins[3][16] = {};   // term t, (s * 4 + s') -> a << 3 | b << 2 | c << 1 | d (0 = up)
@@ -56,11 +62,10 @@ struct SheSmem {
   size_t bytes;
 };
 
-// Shared-memory layout.  STAGED: both Green functions (row-major) live in shared
-// memory, and the df partial too unless it is held in registers (acc_smem false);
-// otherwise they are read from / accumulated in global memory (L1 / L2) and only
-// V, V^T, Y and the tables are staged.
-__host__ __device__ inline SheSmem she_layout(int n, int dimens, int n_neigh, bool staged, bool acc_smem = true) {
+// Shared-memory layout.  STAGED: both Green functions (row-major) and the df
+// partial live in shared memory; otherwise they are read from / accumulated in
+// global memory (L1 / L2) and only V, V^T, Y and the tables are staged.
+__host__ __device__ inline SheSmem she_layout(int n, int dimens, int n_neigh, bool staged) {
   const int no = n / 2;
   SheSmem L;
   int o = 0;
@@ -69,7 +74,7 @@ __host__ __device__ inline SheSmem she_layout(int n, int dimens, int n_neigh, bo
   L.m = o; o += no * no;
   L.mt = o; o += no * no;
   L.y = o; o += 2 * n * no;
-  L.acc = o; o += staged && acc_smem ? 4 * dimens : 0;
+  L.acc = o; o += staged ? 4 * dimens : 0;
   L.ph = o; o += n_neigh > 0 ? n_neigh : 1;
   L.tab = o * (int)sizeof(double2);
   L.bytes = (size_t)L.tab + sizeof(int) * 4 * (size_t)no;
@@ -100,73 +105,104 @@ struct ColMajor {
 
 // One sandwich term.  M: no x no row-major (the middle factor as used: V or V^T).
 // Z(r, col) = sum_{o1, o2} L(r, row_b(o2)) M(o2, o1) R(row_c(o1), col) for the
-// output rows (r, col) of each df entry; acc[s' dimens + row] += f Z.
-// First stage: Y^b = L[:, spin b] M for both spins b (2 n x no).
+// output rows (r, col) of each df entry; acc[s' dimens + row] += f Z, in two stages:
+// Y^b = L[:, spin b] M for both spins b (2 n x no), then Z from Y and R.
+// First stage, register-tiled: each thread computes a 3 x 3 tile (rows r, columns o1) of
+// Y^b, so three L and three M values loaded per o2 feed nine complex FMAs.
 template <class LM>
-__device__ void she_y(const SheArgs& a, LM L, const double2* M, double2* Y, const int* tab) {
+__device__ void she_y_tiled(const SheArgs& a, LM L, const double2* M, double2* Y, const int* tab) {
   const int n = a.n, no = a.no;
-  for (int e = threadIdx.x; e < 2 * n * no; e += blockDim.x) {
-    const int b = e / (n * no), r = (e / no) % n, o1 = e % no;
+  const int tr = (n + 2) / 3, to = (no + 2) / 3;
+  for (int t = threadIdx.x; t < 2 * tr * to; t += blockDim.x) {
+    const int b = t / (tr * to), r0 = 3 * ((t / to) % tr), q0 = 3 * (t % to);
     const int* rowb = tab + b * no;
-    double2 s = make_double2(0, 0);
-    for (int o2 = 0; o2 < no; ++o2) s = cfma(L(r, rowb[o2]), M[o2 * no + o1], s);
-    Y[e] = s;
+    double2 z[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) z[k][l] = make_double2(0.0, 0.0);
+    for (int o2 = 0; o2 < no; ++o2) {
+      const int cb = rowb[o2];
+      double2 lv[3], mv[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) lv[k] = r0 + k < n ? L(r0 + k, cb) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int l = 0; l < 3; ++l) mv[l] = q0 + l < no ? M[o2 * no + q0 + l] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) z[k][l] = cfma(lv[k], mv[l], z[k][l]);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l)
+        if (r0 + k < n && q0 + l < no) Y[(b * n + r0 + k) * no + q0 + l] = z[k][l];
   }
   __syncthreads();
 }
 
-// Second stage for df entry o = s' dimens + row: Z(r, col) of that entry.
+// Second stage, register-tiled: the df entries of one (sigma, s', site i) form an n_i x n_i
+// block Z(x, y) = sum_o1 Y^b(ia + sa n_i + x, o1) R(row_c(o1), ia + sd n_i + y) with
+// (mu, nu) = (y, x) when rows_are_nu else (x, y); each thread takes 3 x 3 tiles of blocks.
 template <class RM>
-__device__ __forceinline__ double2 she_z(const SheArgs& a, int o, const double2* Y, RM R, const int* tab,
-                                         const unsigned char* spins, bool rows_are_nu) {
+__device__ void she_z_tiled(const SheArgs& a, const double2* Y, RM R, double2* acc, const int* tab,
+                            const unsigned char* spins, double2 f, bool rows_are_nu) {
   const int n = a.n, no = a.no, D = a.dimens;
-  const int sp = o / D, row = o % D;
-  const int dec = a.decode[row];
-  const int sigma = dec & 3, i = (dec >> 2) & 1023, mu = (dec >> 12) & 63, nu = (dec >> 18) & 63;
-  const int code = spins[sigma * 4 + sp];
-  const int sa = (code >> 3) & 1, b = (code >> 2) & 1, c = (code >> 1) & 1, sd = code & 1;
-  const int x = rows_are_nu ? nu : mu, y = rows_are_nu ? mu : nu;
-  const int ni = a.norb[i];
-  const int r = a.ia[i] + sa * ni + x, col = a.ia[i] + sd * ni + y;
-  const double2* Yr = Y + (b * n + r) * no;
-  const int* rowc = tab + c * no;
-  double2 s = make_double2(0, 0);
-  for (int o1 = 0; o1 < no; ++o1) s = cfma(Yr[o1], R(rowc[o1], col), s);
-  return s;
+  for (int t = threadIdx.x; t < a.n_ztiles; t += blockDim.x) {
+    const int code = a.ztiles[t];
+    const int sigma = code & 3, sp = (code >> 2) & 3, i = (code >> 4) & 1023;
+    const int x0 = (code >> 14) & 63, y0 = (code >> 20) & 63;
+    const int sc = spins[sigma * 4 + sp];
+    const int sa = (sc >> 3) & 1, b = (sc >> 2) & 1, c = (sc >> 1) & 1, sd = sc & 1;
+    const int ni = a.norb[i], ia = a.ia[i];
+    const double2* Yb = Y + (b * n + ia + sa * ni) * no;
+    const int* rowc = tab + c * no;
+    const int col0 = ia + sd * ni + y0;
+    double2 z[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) z[k][l] = make_double2(0.0, 0.0);
+    for (int o1 = 0; o1 < no; ++o1) {
+      const int rc = rowc[o1];
+      double2 yv[3], rv[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) yv[k] = x0 + k < ni ? Yb[(x0 + k) * no + o1] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int l = 0; l < 3; ++l) rv[l] = y0 + l < ni ? R(rc, col0 + l) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) z[k][l] = cfma(yv[k], rv[l], z[k][l]);
+    }
+    const int base = sp * D + a.rowoff[i] + sigma;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) {
+        if (x0 + k >= ni || y0 + l >= ni) continue;
+        const int mu = rows_are_nu ? y0 + l : x0 + k, nu = rows_are_nu ? x0 + k : y0 + l;
+        const int o = base + 4 * (mu * ni + nu);
+        acc[o] = cfma(f, z[k][l], acc[o]);
+      }
+  }
 }
 
-// the term with the df slice in memory (shared or global)
+// the term with the df slice in memory (shared or global), both stages register-tiled
 template <class LM, class RM>
 __device__ void she_term(const SheArgs& a, LM L, const double2* M, RM R, double2* Y, double2* acc, const int* tab,
                          const unsigned char* spins, double2 f, bool rows_are_nu) {
-  she_y(a, L, M, Y, tab);
-  for (int o = threadIdx.x; o < 4 * a.dimens; o += blockDim.x)
-    acc[o] = cfma(f, she_z(a, o, Y, R, tab, spins, rows_are_nu), acc[o]);
+  she_y_tiled(a, L, M, Y, tab);
+  she_z_tiled(a, Y, R, acc, tab, spins, f, rows_are_nu);
   __syncthreads();
 }
 
-// the term with the df slice in registers: entry o = threadIdx.x + i blockDim.x in racc[i]
-template <int RACC, class LM, class RM>
-__device__ void she_term_reg(const SheArgs& a, LM L, const double2* M, RM R, double2* Y, double2 (&racc)[RACC],
-                             const int* tab, const unsigned char* spins, double2 f, bool rows_are_nu) {
-  she_y(a, L, M, Y, tab);
-#pragma unroll
-  for (int i = 0; i < RACC; ++i) {
-    const int o = threadIdx.x + i * blockDim.x;
-    if (o < 4 * a.dimens) racc[i] = cfma(f, she_z(a, o, Y, R, tab, spins, rows_are_nu), racc[i]);
-  }
-  __syncthreads();
-}
-
-// STAGED: Green functions in shared memory; RACC > 0 (staged only): the df slice in
-// RACC registers per thread (4 dimens <= RACC x 256), which leaves the shared memory
-// to the Green functions, V and Y and fits three CTAs per SM at dimH 36
-template <bool STAGED, int RACC>
-__device__ __forceinline__ void she_body(const SheArgs& a) {
-  static_assert(STAGED || RACC == 0, "register slices only in the staged kernel");
+template <bool STAGED>
+__global__ void __launch_bounds__(256) she_kernel(SheArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = a.n, no = a.no, D = a.dimens;
-  const SheSmem L = she_layout(n, D, a.n_neigh, STAGED, RACC == 0);
+  const SheSmem L = she_layout(n, D, a.n_neigh, STAGED);
   double2* base = reinterpret_cast<double2*>(smem);
   double2* S1 = base + L.s1;
   double2* S2 = base + L.s2;
@@ -176,17 +212,9 @@ __device__ __forceinline__ void she_body(const SheArgs& a) {
   double2* ph = base + L.ph;
   int* tab = reinterpret_cast<int*>(smem + L.tab);
   double2* mine = a.partial + (size_t)blockIdx.x * 4 * D;
-  double2* acc = STAGED && RACC == 0 ? base + L.acc : mine;
-  double2 racc[RACC > 0 ? RACC : 1];
-  if (RACC > 0) {
-#pragma unroll
-    for (int i = 0; i < (RACC > 0 ? RACC : 1); ++i) {
-      const int o = threadIdx.x + i * blockDim.x;
-      racc[i] = o < 4 * D ? mine[o] : make_double2(0.0, 0.0);
-    }
-  } else if (STAGED) {
+  double2* acc = STAGED ? base + L.acc : mine;
+  if (STAGED)
     for (int e = threadIdx.x; e < 4 * D; e += blockDim.x) acc[e] = mine[e];
-  }
   for (int e = threadIdx.x; e < 4 * no; e += blockDim.x) tab[e] = a.tab[e];
   __syncthreads();
   for (int64_t pl = blockIdx.x; pl < a.np; pl += gridDim.x) {
@@ -253,20 +281,7 @@ __device__ __forceinline__ void she_body(const SheArgs& a) {
       MT[cc * no + rr] = v;
     }
     __syncthreads();
-    if (STAGED && RACC > 0) {
-      if (!a.real_axis) {
-        she_term_reg(a, RowMajor{S1, n}, M, RowMajor{S2, n}, Y, racc, tab, a.spins[0], make_double2(w, 0.0), true);
-        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-          S1[e].y = -S1[e].y;
-          S2[e].y = -S2[e].y;
-        }
-        __syncthreads();
-        she_term_reg(a, RowMajor{S2, n}, MT, RowMajor{S1, n}, Y, racc, tab, a.spins[1], make_double2(w, 0.0),
-                     false);
-      } else {
-        she_term_reg(a, RowMajor{S1, n}, M, RowMajor{S2, n}, Y, racc, tab, a.spins[2], make_double2(0.0, -w), true);
-      }
-    } else if (STAGED) {
+    if (STAGED) {
       if (!a.real_axis) {
         she_term(a, RowMajor{S1, n}, M, RowMajor{S2, n}, Y, acc, tab, a.spins[0], make_double2(w, 0.0), true);
         for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
@@ -290,26 +305,8 @@ __device__ __forceinline__ void she_body(const SheArgs& a) {
       }
     }
   }
-  if (RACC > 0) {
-#pragma unroll
-    for (int i = 0; i < (RACC > 0 ? RACC : 1); ++i) {
-      const int o = threadIdx.x + i * blockDim.x;
-      if (o < 4 * D) mine[o] = racc[i];
-    }
-  } else if (STAGED) {
+  if (STAGED)
     for (int e = threadIdx.x; e < 4 * D; e += blockDim.x) mine[e] = acc[e];
-  }
-}
-
-template <bool STAGED>
-__global__ void __launch_bounds__(256) she_kernel(SheArgs a) {
-  she_body<STAGED, 0>(a);
-}
-
-// the register-slice variant: 127 registers, two CTAs per SM (a three-CTA bound spills)
-constexpr int kSheRacc = 12;
-__global__ void __launch_bounds__(256, 2) she_kernel_reg(SheArgs a) {
-  she_body<true, kSheRacc>(a);
 }
 
 // tchi(r, s') = scale sum_c P(r, c) df(c, s'), P column-major (dimens x dimens); P == nullptr: identity
@@ -329,26 +326,10 @@ __global__ void she_prefactor_kernel(const double2* __restrict__ P, const double
 
 }  // namespace
 
-// Variant choice: the staged kernel with register slices when 4 dimens <= kSheRacc x 256
-// and its shared memory fits, else the staged kernel with the slice in shared memory,
-// else the global-operand kernel; 0 bytes when none fits.
-enum SheVariant { SHE_GLOBAL = 0, SHE_STAGED = 1, SHE_STAGED_REG = 2 };
-
-SheVariant she_variant(int n, int dimens, int n_neigh, size_t optin) {
-  if (4 * dimens <= kSheRacc * 256 && she_layout(n, dimens, n_neigh, true, false).bytes <= optin)
-    return SHE_STAGED_REG;
-  if (she_layout(n, dimens, n_neigh, true).bytes <= optin) return SHE_STAGED;
-  return SHE_GLOBAL;
-}
-
-size_t she_variant_bytes(int n, int dimens, int n_neigh, SheVariant v) {
-  return she_layout(n, dimens, n_neigh, v != SHE_GLOBAL, v != SHE_STAGED_REG).bytes;
-}
-
-const void* she_variant_fn(SheVariant v) {
-  if (v == SHE_STAGED_REG) return (const void*)she_kernel_reg;
-  if (v == SHE_STAGED) return (const void*)she_kernel<true>;
-  return (const void*)she_kernel<false>;
+// Variant choice: the staged kernel when its shared memory fits, else the
+// global-operand kernel; 0 bytes when neither fits.
+bool she_staged(int n, int dimens, int n_neigh, size_t optin) {
+  return she_layout(n, dimens, n_neigh, true).bytes <= optin;
 }
 
 int she_optin() {
@@ -360,16 +341,17 @@ int she_optin() {
 
 size_t she_smem_bytes(int n, int dimens, int n_neigh) {
   const int optin = she_optin();
-  const size_t b = she_variant_bytes(n, dimens, n_neigh, she_variant(n, dimens, n_neigh, (size_t)optin));
+  const bool staged = she_staged(n, dimens, n_neigh, (size_t)optin);
+  const size_t b = she_layout(n, dimens, n_neigh, staged).bytes;
   return b <= (size_t)optin ? b : 0;
 }
 
 int she_grid(int n, int dimens, int n_neigh, int num_sms) {
   const int optin = she_optin();
-  const SheVariant v = she_variant(n, dimens, n_neigh, (size_t)optin);
-  const size_t smem = she_variant_bytes(n, dimens, n_neigh, v);
+  const bool staged = she_staged(n, dimens, n_neigh, (size_t)optin);
+  const size_t smem = she_layout(n, dimens, n_neigh, staged).bytes;
   if (smem > (size_t)optin) return 0;
-  const void* fn = she_variant_fn(v);
+  const void* fn = staged ? (const void*)she_kernel<true> : (const void*)she_kernel<false>;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem) != cudaSuccess) return 0;
@@ -398,6 +380,9 @@ cudaError_t launch_she(const SheLaunch& l, cudaStream_t s) {
   a.ia = l.ia;
   a.norb = l.norb;
   a.decode = l.decode;
+  a.ztiles = l.ztiles;
+  a.n_ztiles = l.n_ztiles;
+  a.rowoff = l.rowoff;
   a.real_axis = l.real_axis;
   for (int i = 0; i < 3; ++i) a.ue[i] = l.ue[i];
   for (int t = 0; t < 3; ++t)
@@ -408,14 +393,13 @@ cudaError_t launch_she(const SheLaunch& l, cudaStream_t s) {
   a.klist = l.klist;
   const int optin = she_optin();
   if (optin <= 0) return cudaErrorInvalidValue;
-  const SheVariant v = she_variant(a.n, a.dimens, a.n_neigh, (size_t)optin);
-  const size_t smem = she_variant_bytes(a.n, a.dimens, a.n_neigh, v);
+  const bool staged = she_staged(a.n, a.dimens, a.n_neigh, (size_t)optin);
+  const size_t smem = she_layout(a.n, a.dimens, a.n_neigh, staged).bytes;
   if (smem > (size_t)optin) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(she_variant_fn(v), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const void* fn = staged ? (const void*)she_kernel<true> : (const void*)she_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  if (v == SHE_STAGED_REG)
-    she_kernel_reg<<<l.grid, 256, smem, s>>>(a);
-  else if (v == SHE_STAGED)
+  if (staged)
     she_kernel<true><<<l.grid, 256, smem, s>>>(a);
   else
     she_kernel<false><<<l.grid, 256, smem, s>>>(a);
