@@ -53,9 +53,10 @@ def parse():
                     help="skip the untimed split-vs-FP64 accuracy check of the chi0 workload")
     ap.add_argument("--green", default="auto", choices=["auto", "gauss-jordan", "spectral"],
                     help="Green-function method (tg_set_green_method)")
-    ap.add_argument("--workload", default="chi0", choices=["chi0", "she", "ldos"],
+    ap.add_argument("--workload", default="chi0", choices=["chi0", "she", "ldos", "scf"],
                     help="chi0: the susceptibility integral (headline); she: the disturbance integral "
-                         "(eintshe) of the same mesh, one frequency per step")
+                         "(eintshe) of the same mesh, one frequency per step; ldos: the real-axis LDOS; "
+                         "scf: occupations + Jacobian of one Newton step")
     ap.add_argument("--small", action="store_true",
                     help="30 x 30 k mesh, 64 + 16 energies: a few-second case for profiler captures")
     return ap.parse_args()
@@ -569,6 +570,87 @@ def run_ldos(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+SCF_METRIC = "self-consistency Newton step: occupations + Jacobian (k,E)-points/s on 1 B200 (FP64)"
+
+
+def scf_cpu_baseline(deck, h0, seconds_target=15.0):
+    """The oracle's expectation + jacobian (numpy, all host threads) on a bounded sample: the
+    first imaginary-axis points in mesh order and the first real-axis k (Fermi column)."""
+    from oracle import titan_oracle as O
+    from titan_b200.host.mesh import EKMesh
+    s = deck.system
+    m = O.Model(s, h0)
+    ek = deck.ek
+
+    def run(npts):
+        sub = EKMesh(ek.y, ek.wght, ek.energy_index[:npts], ek.kp[:npts], ek.weight[:npts])
+        nk = max(1, min(deck.real_kp.shape[0], npts // 64))
+        rk = (deck.real_kp[:nk], deck.real_w[:nk])
+        t0 = time.perf_counter()
+        O.expectation(m, sub, s.Ef, s.eta)
+        O.jacobian(m, sub, rk, s.Ef, s.eta, False)
+        return time.perf_counter() - t0
+
+    cal = min(256, ek.n_points)
+    dt = run(cal)
+    npts = int(min(ek.n_points, max(cal, cal * seconds_target / max(dt, 1e-6))))
+    dt = run(npts)
+    cores = os.cpu_count()
+    return {"value": npts / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle expectation + jacobian (numpy/LAPACK, {cores} threads) on the first {npts} "
+                      f"imaginary-axis points of the {s.name} mesh and {max(1, npts // 64)} real-axis k "
+                      f"({dt:.1f} s)"}
+
+
+def run_scf(args, rank, world, local_rank):
+    """One self-consistency step's Green-function work per step: tg_expectation (occupations
+    and moments) and tg_jacobian (GG tensors over the imaginary axis + the Fermi column over the
+    real-axis BZ) at the same state; a unit is one imaginary-axis (E, k) point through both."""
+    import torch
+    from titan_b200.native import GreenGPU
+    torch.cuda.set_device(local_rank)
+    deck, h0, _, _ = workload(args.config, args.small)
+    s = deck.system
+    gpu = GreenGPU(local_rank)
+    gpu.setup(deck, h0)
+    gpu.set_green_method(args.green)
+
+    def step():
+        gpu.expectation(s.Ef, s.eta)
+        gpu.jacobian(s.Ef, s.eta, False)
+
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local_rank)
+    clk.start()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        step()
+    stop.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier(world)
+    ms = allreduce_max(start.elapsed_time(stop), world)
+    units = allreduce_sum(deck.ek.n_points * args.steps, world)
+    line = {"metric": SCF_METRIC, "value": units / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Slater-Koster model, no external data)",
+            "config": {"workload": f"{args.config}: dimH={s.dimH}, {deck.ek.n_points} imag (E,k) points through "
+                                   f"tg_expectation and tg_jacobian, Fermi column over {deck.real_kp.shape[0]} k",
+                       "green": args.green,
+                       "timer": "CUDA events on the current stream around the blocking calls"},
+            "clocks": clocks}
+    if rank == 0 and not args.no_cpu and world == 1:
+        line["cpu_baseline"] = scf_cpu_baseline(deck, h0)
+    gpu.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # --------------------------------------------------------------------------- distributed helpers
 def barrier(world):
     if world > 1:
@@ -616,6 +698,8 @@ def main():
             run_she(args, rank, world, local_rank)
         elif args.workload == "ldos":
             run_ldos(args, rank, world, local_rank)
+        elif args.workload == "scf":
+            run_scf(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:
