@@ -53,10 +53,11 @@ def parse():
                     help="skip the untimed split-vs-FP64 accuracy check of the chi0 workload")
     ap.add_argument("--green", default="auto", choices=["auto", "gauss-jordan", "spectral"],
                     help="Green-function method (tg_set_green_method)")
-    ap.add_argument("--workload", default="chi0", choices=["chi0", "she", "ldos", "scf"],
+    ap.add_argument("--workload", default="chi0", choices=["chi0", "she", "ldos", "scf", "lsoc", "jij"],
                     help="chi0: the susceptibility integral (headline); she: the disturbance integral "
                          "(eintshe) of the same mesh, one frequency per step; ldos: the real-axis LDOS; "
-                         "scf: occupations + Jacobian of one Newton step")
+                         "scf: occupations + Jacobian of one Newton step; lsoc: the linear-SOC chi0; "
+                         "jij: the exchange coupling")
     ap.add_argument("--small", action="store_true",
                     help="30 x 30 k mesh, 64 + 16 energies: a few-second case for profiler captures")
     return ap.parse_args()
@@ -651,6 +652,96 @@ def run_scf(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_row(args, rank, world, local_rank):
+    """The linear-SOC susceptibility (--workload lsoc: one tg_chi0_linear_soc call at the
+    second frequency, q = 0, per step; units as chi0) and the exchange coupling (--workload
+    jij: one tg_jij call at q = 0 with all moments along z, per step; a unit is one
+    imaginary-axis point), each with the oracle on a bounded slice of the same mesh."""
+    import torch
+    from oracle import titan_oracle as O
+    from titan_b200.host.mesh import EKMesh
+    from titan_b200.host.system import initial_state
+    from titan_b200.native import GreenGPU
+    torch.cuda.set_device(local_rank)
+    deck, h0, omegas, reals = workload(args.config, args.small)
+    s = deck.system
+    ek = deck.ek
+    gpu = GreenGPU(local_rank)
+    q = np.zeros(3)
+    e = float(omegas[1])
+    x2, p2 = reals[1]
+    nk = deck.real_kp.shape[0]
+    if args.workload == "lsoc":
+        h00, V = s.linear_soc_split(initial_state(s))
+        gpu.setup(deck, h00)
+        metric = "linear-SOC chi0 (eintshechilinearsoc) (k,E)-points/s on 1 B200 (FP64)"
+        step_units = ek.n_points + len(x2) * nk
+        desc = f"{ek.n_points} imag (E,k) points + {len(x2)} real-axis energies x {nk} k at omega={e:.5f}, q=0"
+
+        def step():
+            gpu.chi0_linear_soc(q, e, s.Ef, s.eta, s.etap, x2, p2, V)
+
+        def cpu(npts):
+            sub = EKMesh(ek.y, ek.wght, ek.energy_index[:npts], ek.kp[:npts], ek.weight[:npts])
+            t0 = time.perf_counter()
+            O.eintshechi_linear_soc(O.Model(s, h00), V, sub, (deck.real_kp[:1], deck.real_w[:1]), q, e, s.Ef, s.eta,
+                                    s.etap, x2, p2)
+            return time.perf_counter() - t0, npts + len(x2)
+        what = "oracle eintshechi_linear_soc"
+    else:
+        gpu.setup(deck, h0)
+        evec = np.tile([0.0, 0.0, 1.0], (s.n_atoms, 1))
+        metric = "exchange coupling J_ij(q) (jij_energy) (k,E)-points/s on 1 B200 (FP64)"
+        step_units = ek.n_points
+        desc = f"{ek.n_points} imag (E,k) points, q=0, moments along z"
+
+        def step():
+            gpu.jij(q, s.Ef, s.eta, evec, s.Um())
+
+        def cpu(npts):
+            sub = EKMesh(ek.y, ek.wght, ek.energy_index[:npts], ek.kp[:npts], ek.weight[:npts])
+            t0 = time.perf_counter()
+            O.jij(O.Model(s, h0), sub, q, s.Ef, s.eta, evec, s.Um(), s.dorbs)
+            return time.perf_counter() - t0, npts
+        what = "oracle jij"
+    gpu.set_green_method(args.green)
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local_rank)
+    clk.start()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        step()
+    stop.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    barrier(world)
+    ms = allreduce_max(start.elapsed_time(stop), world)
+    units = allreduce_sum(step_units * args.steps, world)
+    line = {"metric": metric, "value": units / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Slater-Koster model, no external data)",
+            "config": {"workload": f"{args.config}: dimH={s.dimH}, {desc}", "green": args.green,
+                       "timer": "CUDA events on the current stream around the blocking calls"},
+            "clocks": clocks}
+    if rank == 0 and not args.no_cpu and world == 1:
+        cal = min(256, ek.n_points)
+        dt, _ = cpu(cal)
+        npts = int(min(ek.n_points, max(cal, cal * 15.0 / max(dt, 1e-6))))
+        dt, u = cpu(npts)
+        cores = os.cpu_count()
+        line["cpu_baseline"] = {"value": u / dt, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"{what} (numpy/LAPACK, {cores} threads) on the first {npts} "
+                                          f"imaginary-axis points ({dt:.1f} s)"}
+    gpu.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # --------------------------------------------------------------------------- distributed helpers
 def barrier(world):
     if world > 1:
@@ -700,6 +791,8 @@ def main():
             run_ldos(args, rank, world, local_rank)
         elif args.workload == "scf":
             run_scf(args, rank, world, local_rank)
+        elif args.workload in ("lsoc", "jij"):
+            run_row(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:
