@@ -57,6 +57,10 @@ struct SheArgs {
   const double* klist = nullptr;
 };
 
+// 288 threads: the 288 second-stage tiles of two spd sites (32 blocks of 3 x 3 tiles) and
+// the 216 first-stage tiles at dimH 36 each take one round of the CTA
+constexpr int kSheThreads = 288;
+
 struct SheSmem {
   int s1, s2, m, mt, y, acc, ph, tab;   // offsets in double2 units (tab: in bytes)
   size_t bytes;
@@ -107,34 +111,35 @@ struct ColMajor {
 // Z(r, col) = sum_{o1, o2} L(r, row_b(o2)) M(o2, o1) R(row_c(o1), col) for the
 // output rows (r, col) of each df entry; acc[s' dimens + row] += f Z, in two stages:
 // Y^b = L[:, spin b] M for both spins b (2 n x no), then Z from Y and R.
-// First stage, register-tiled: each thread computes a 3 x 3 tile (rows r, columns o1) of
-// Y^b, so three L and three M values loaded per o2 feed nine complex FMAs.
+// First stage, register-tiled: each thread computes a 2 x 3 tile (rows r, columns o1) of
+// Y^b, so five L and M values loaded per o2 feed six complex FMAs (2 x 18 x 6 = 216 tiles
+// at n = 36: one round of the CTA).
 template <class LM>
 __device__ void she_y_tiled(const SheArgs& a, LM L, const double2* M, double2* Y, const int* tab) {
   const int n = a.n, no = a.no;
-  const int tr = (n + 2) / 3, to = (no + 2) / 3;
+  const int tr = (n + 1) / 2, to = (no + 2) / 3;
   for (int t = threadIdx.x; t < 2 * tr * to; t += blockDim.x) {
-    const int b = t / (tr * to), r0 = 3 * ((t / to) % tr), q0 = 3 * (t % to);
+    const int b = t / (tr * to), r0 = 2 * ((t / to) % tr), q0 = 3 * (t % to);
     const int* rowb = tab + b * no;
-    double2 z[3][3];
+    double2 z[2][3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
+    for (int k = 0; k < 2; ++k)
 #pragma unroll
       for (int l = 0; l < 3; ++l) z[k][l] = make_double2(0.0, 0.0);
     for (int o2 = 0; o2 < no; ++o2) {
       const int cb = rowb[o2];
-      double2 lv[3], mv[3];
+      double2 lv[2], mv[3];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) lv[k] = r0 + k < n ? L(r0 + k, cb) : make_double2(0.0, 0.0);
+      for (int k = 0; k < 2; ++k) lv[k] = r0 + k < n ? L(r0 + k, cb) : make_double2(0.0, 0.0);
 #pragma unroll
       for (int l = 0; l < 3; ++l) mv[l] = q0 + l < no ? M[o2 * no + q0 + l] : make_double2(0.0, 0.0);
 #pragma unroll
-      for (int k = 0; k < 3; ++k)
+      for (int k = 0; k < 2; ++k)
 #pragma unroll
         for (int l = 0; l < 3; ++l) z[k][l] = cfma(lv[k], mv[l], z[k][l]);
     }
 #pragma unroll
-    for (int k = 0; k < 3; ++k)
+    for (int k = 0; k < 2; ++k)
 #pragma unroll
       for (int l = 0; l < 3; ++l)
         if (r0 + k < n && q0 + l < no) Y[(b * n + r0 + k) * no + q0 + l] = z[k][l];
@@ -199,7 +204,7 @@ __device__ void she_term(const SheArgs& a, LM L, const double2* M, RM R, double2
 }
 
 template <bool STAGED>
-__global__ void __launch_bounds__(256) she_kernel(SheArgs a) {
+__global__ void __launch_bounds__(kSheThreads) she_kernel(SheArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = a.n, no = a.no, D = a.dimens;
   const SheSmem L = she_layout(n, D, a.n_neigh, STAGED);
@@ -354,7 +359,7 @@ int she_grid(int n, int dimens, int n_neigh, int num_sms) {
   const void* fn = staged ? (const void*)she_kernel<true> : (const void*)she_kernel<false>;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSheThreads, smem) != cudaSuccess) return 0;
   return num_sms * std::max(per_sm, 1);
 }
 
@@ -400,9 +405,9 @@ cudaError_t launch_she(const SheLaunch& l, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   if (staged)
-    she_kernel<true><<<l.grid, 256, smem, s>>>(a);
+    she_kernel<true><<<l.grid, kSheThreads, smem, s>>>(a);
   else
-    she_kernel<false><<<l.grid, 256, smem, s>>>(a);
+    she_kernel<false><<<l.grid, kSheThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
