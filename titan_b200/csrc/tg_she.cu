@@ -62,22 +62,27 @@ struct SheArgs {
 constexpr int kSheThreads = 288;
 
 struct SheSmem {
-  int s1, s2, m, mt, y, acc, ph, tab;   // offsets in double2 units (tab: in bytes)
+  int s1, s2, m, y, acc, ph, tab;   // offsets in double2 units (tab: in bytes)
   size_t bytes;
 };
 
-// Shared-memory layout.  STAGED: both Green functions (row-major) and the df
-// partial live in shared memory; otherwise they are read from / accumulated in
-// global memory (L1 / L2) and only V, V^T, Y and the tables are staged.
+// Row strides of the staged Green functions and of Y: odd, so the 16-byte reads of a
+// quarter warp on rows a few apart fall into distinct bank groups.
+__host__ __device__ inline int she_sst(int n) { return n | 1; }
+__host__ __device__ inline int she_yst(int no) { return no | 1; }
+
+// Shared-memory layout.  STAGED: both Green functions (row-major, stride she_sst) and
+// the df partial live in shared memory; otherwise they are read from / accumulated in
+// global memory (L1 / L2) and only V, Y and the tables are staged.  V^T is read from
+// V with swapped indices.
 __host__ __device__ inline SheSmem she_layout(int n, int dimens, int n_neigh, bool staged) {
   const int no = n / 2;
   SheSmem L;
   int o = 0;
-  L.s1 = o; o += staged ? n * n : 0;
-  L.s2 = o; o += staged ? n * n : 0;
+  L.s1 = o; o += staged ? n * she_sst(n) : 0;
+  L.s2 = o; o += staged ? n * she_sst(n) : 0;
   L.m = o; o += no * no;
-  L.mt = o; o += no * no;
-  L.y = o; o += 2 * n * no;
+  L.y = o; o += 2 * n * she_yst(no);
   L.acc = o; o += staged ? 4 * dimens : 0;
   L.ph = o; o += n_neigh > 0 ? n_neigh : 1;
   L.tab = o * (int)sizeof(double2);
@@ -115,8 +120,8 @@ struct ColMajor {
 // Y^b, so five L and M values loaded per o2 feed six complex FMAs (2 x 18 x 6 = 216 tiles
 // at n = 36: one round of the CTA).
 template <class LM>
-__device__ void she_y_tiled(const SheArgs& a, LM L, const double2* M, double2* Y, const int* tab) {
-  const int n = a.n, no = a.no;
+__device__ void she_y_tiled(const SheArgs& a, LM L, const double2* M, bool mt, double2* Y, const int* tab) {
+  const int n = a.n, no = a.no, yst = she_yst(no);
   const int tr = (n + 1) / 2, to = (no + 2) / 3;
   for (int t = threadIdx.x; t < 2 * tr * to; t += blockDim.x) {
     const int b = t / (tr * to), r0 = 2 * ((t / to) % tr), q0 = 3 * (t % to);
@@ -132,7 +137,8 @@ __device__ void she_y_tiled(const SheArgs& a, LM L, const double2* M, double2* Y
 #pragma unroll
       for (int k = 0; k < 2; ++k) lv[k] = r0 + k < n ? L(r0 + k, cb) : make_double2(0.0, 0.0);
 #pragma unroll
-      for (int l = 0; l < 3; ++l) mv[l] = q0 + l < no ? M[o2 * no + q0 + l] : make_double2(0.0, 0.0);
+      for (int l = 0; l < 3; ++l)
+        mv[l] = q0 + l < no ? (mt ? M[(q0 + l) * no + o2] : M[o2 * no + q0 + l]) : make_double2(0.0, 0.0);
 #pragma unroll
       for (int k = 0; k < 2; ++k)
 #pragma unroll
@@ -142,7 +148,7 @@ __device__ void she_y_tiled(const SheArgs& a, LM L, const double2* M, double2* Y
     for (int k = 0; k < 2; ++k)
 #pragma unroll
       for (int l = 0; l < 3; ++l)
-        if (r0 + k < n && q0 + l < no) Y[(b * n + r0 + k) * no + q0 + l] = z[k][l];
+        if (r0 + k < n && q0 + l < no) Y[(b * n + r0 + k) * yst + q0 + l] = z[k][l];
   }
   __syncthreads();
 }
@@ -153,7 +159,7 @@ __device__ void she_y_tiled(const SheArgs& a, LM L, const double2* M, double2* Y
 template <class RM>
 __device__ void she_z_tiled(const SheArgs& a, const double2* Y, RM R, double2* acc, const int* tab,
                             const unsigned char* spins, double2 f, bool rows_are_nu) {
-  const int n = a.n, no = a.no, D = a.dimens;
+  const int n = a.n, no = a.no, D = a.dimens, yst = she_yst(no);
   for (int t = threadIdx.x; t < a.n_ztiles; t += blockDim.x) {
     const int code = a.ztiles[t];
     const int sigma = code & 3, sp = (code >> 2) & 3, i = (code >> 4) & 1023;
@@ -161,7 +167,7 @@ __device__ void she_z_tiled(const SheArgs& a, const double2* Y, RM R, double2* a
     const int sc = spins[sigma * 4 + sp];
     const int sa = (sc >> 3) & 1, b = (sc >> 2) & 1, c = (sc >> 1) & 1, sd = sc & 1;
     const int ni = a.norb[i], ia = a.ia[i];
-    const double2* Yb = Y + (b * n + ia + sa * ni) * no;
+    const double2* Yb = Y + (b * n + ia + sa * ni) * yst;
     const int* rowc = tab + c * no;
     const int col0 = ia + sd * ni + y0;
     double2 z[3][3];
@@ -173,7 +179,7 @@ __device__ void she_z_tiled(const SheArgs& a, const double2* Y, RM R, double2* a
       const int rc = rowc[o1];
       double2 yv[3], rv[3];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) yv[k] = x0 + k < ni ? Yb[(x0 + k) * no + o1] : make_double2(0.0, 0.0);
+      for (int k = 0; k < 3; ++k) yv[k] = x0 + k < ni ? Yb[(x0 + k) * yst + o1] : make_double2(0.0, 0.0);
 #pragma unroll
       for (int l = 0; l < 3; ++l) rv[l] = y0 + l < ni ? R(rc, col0 + l) : make_double2(0.0, 0.0);
 #pragma unroll
@@ -196,9 +202,9 @@ __device__ void she_z_tiled(const SheArgs& a, const double2* Y, RM R, double2* a
 
 // the term with the df slice in memory (shared or global), both stages register-tiled
 template <class LM, class RM>
-__device__ void she_term(const SheArgs& a, LM L, const double2* M, RM R, double2* Y, double2* acc, const int* tab,
-                         const unsigned char* spins, double2 f, bool rows_are_nu) {
-  she_y_tiled(a, L, M, Y, tab);
+__device__ void she_term(const SheArgs& a, LM L, const double2* M, bool mt, RM R, double2* Y, double2* acc,
+                         const int* tab, const unsigned char* spins, double2 f, bool rows_are_nu) {
+  she_y_tiled(a, L, M, mt, Y, tab);
   she_z_tiled(a, Y, R, acc, tab, spins, f, rows_are_nu);
   __syncthreads();
 }
@@ -212,8 +218,8 @@ __global__ void __launch_bounds__(kSheThreads) she_kernel(SheArgs a) {
   double2* S1 = base + L.s1;
   double2* S2 = base + L.s2;
   double2* M = base + L.m;
-  double2* MT = base + L.mt;
   double2* Y = base + L.y;
+  const int sst = she_sst(n);
   double2* ph = base + L.ph;
   int* tab = reinterpret_cast<int*>(smem + L.tab);
   double2* mine = a.partial + (size_t)blockIdx.x * 4 * D;
@@ -259,16 +265,16 @@ __global__ void __launch_bounds__(kSheThreads) she_kernel(SheArgs a) {
       if (!a.real_axis) {
         for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
           const int c = e / n, r = e % n;
-          S1[r * n + c] = g1[e];
-          S2[r * n + c] = g2[e];
+          S1[r * sst + c] = g1[e];
+          S2[r * sst + c] = g2[e];
         }
       } else {
         for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
           const int r = e / n, c = e % n;
           const double2 x = g1[(size_t)c * n + r], xt = g1[(size_t)r * n + c];
-          S1[e] = make_double2(x.x - xt.x, x.y + xt.y);
+          S1[r * sst + c] = make_double2(x.x - xt.x, x.y + xt.y);
           const double2 y = g2[(size_t)r * n + c];
-          S2[e] = make_double2(y.x, -y.y);
+          S2[r * sst + c] = make_double2(y.x, -y.y);
         }
       }
     }
@@ -283,29 +289,31 @@ __global__ void __launch_bounds__(kSheThreads) she_kernel(SheArgs a) {
       for (int b = a.pair_start[pb]; b < a.pair_start[pb + 1]; ++b)
         v = cfma(ph[a.pair_neigh[b]], a.pair_t[(size_t)b * a.nmax * a.nmax + occ * a.nmax + orr], v);
       M[rr * no + cc] = v;
-      MT[cc * no + rr] = v;
     }
     __syncthreads();
     if (STAGED) {
       if (!a.real_axis) {
-        she_term(a, RowMajor{S1, n}, M, RowMajor{S2, n}, Y, acc, tab, a.spins[0], make_double2(w, 0.0), true);
-        for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        she_term(a, RowMajor{S1, sst}, M, false, RowMajor{S2, sst}, Y, acc, tab, a.spins[0], make_double2(w, 0.0),
+                 true);
+        for (int e = threadIdx.x; e < n * sst; e += blockDim.x) {
           S1[e].y = -S1[e].y;
           S2[e].y = -S2[e].y;
         }
         __syncthreads();
-        she_term(a, RowMajor{S2, n}, MT, RowMajor{S1, n}, Y, acc, tab, a.spins[1], make_double2(w, 0.0), false);
+        she_term(a, RowMajor{S2, sst}, M, true, RowMajor{S1, sst}, Y, acc, tab, a.spins[1], make_double2(w, 0.0),
+                 false);
       } else {
-        she_term(a, RowMajor{S1, n}, M, RowMajor{S2, n}, Y, acc, tab, a.spins[2], make_double2(0.0, -w), true);
+        she_term(a, RowMajor{S1, sst}, M, false, RowMajor{S2, sst}, Y, acc, tab, a.spins[2], make_double2(0.0, -w),
+                 true);
       }
     } else {
       if (!a.real_axis) {
-        she_term(a, ColMajor{g1, n, GK_G}, M, ColMajor{g2, n, GK_G}, Y, acc, tab, a.spins[0], make_double2(w, 0.0),
+        she_term(a, ColMajor{g1, n, GK_G}, M, false, ColMajor{g2, n, GK_G}, Y, acc, tab, a.spins[0], make_double2(w, 0.0),
                  true);
-        she_term(a, ColMajor{g2, n, GK_CONJ}, MT, ColMajor{g1, n, GK_CONJ}, Y, acc, tab, a.spins[1],
+        she_term(a, ColMajor{g2, n, GK_CONJ}, M, true, ColMajor{g1, n, GK_CONJ}, Y, acc, tab, a.spins[1],
                  make_double2(w, 0.0), false);
       } else {
-        she_term(a, ColMajor{g1, n, GK_ANTI}, M, ColMajor{g2, n, GK_DAGGER}, Y, acc, tab, a.spins[2],
+        she_term(a, ColMajor{g1, n, GK_ANTI}, M, false, ColMajor{g2, n, GK_DAGGER}, Y, acc, tab, a.spins[2],
                  make_double2(0.0, -w), true);
       }
     }
