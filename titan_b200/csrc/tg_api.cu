@@ -1798,7 +1798,9 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
   cudaStream_t s = c->stream;
   const int n = c->dimH, no = n / 2, D = c->dimens;
   const int64_t nn = (int64_t)n * n;
-  const int grid = she_grid(n, D, c->n_neigh, c->num_sms);
+  int n_tiles = 0;
+  for (int i = 0; i < c->n_atoms; ++i) n_tiles += 16 * ((c->norb[i] + 2) / 3) * ((c->norb[i] + 2) / 3);
+  const int grid = she_grid(n, D, c->n_neigh, n_tiles, c->num_sms);
   if (grid <= 0) return set_err(c, TG_ERR_ARG, "tg_she: dimH / dimens too large for the shared-memory vertex kernel");
   // orbital tables of the kernel
   std::vector<int> tab((size_t)4 * no);

@@ -231,9 +231,10 @@ struct SheLaunch {
   int64_t n_e = 0, nk_tab = 0;
   const double* klist = nullptr;
 };
-size_t she_smem_bytes(int n, int dimens, int n_neigh);
+// (n_ztiles: second-stage tiles of the system, 16 sum_i ceil(n_i / 3)^2)
+size_t she_smem_bytes(int n, int dimens, int n_neigh, int n_ztiles);
 // CTAs of one vertex launch (SMs x resident CTAs); 0 when the shared memory does not fit
-int she_grid(int n, int dimens, int n_neigh, int num_sms);
+int she_grid(int n, int dimens, int n_neigh, int n_ztiles, int num_sms);
 cudaError_t launch_she(const SheLaunch& l, cudaStream_t s);
 cudaError_t launch_she_prefactor(const double2* P, const double2* df, int dimens, double scale, double2* out,
                                  cudaStream_t s);

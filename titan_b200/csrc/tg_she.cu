@@ -75,7 +75,7 @@ __host__ __device__ inline int she_yst(int no) { return no | 1; }
 // the df partial live in shared memory; otherwise they are read from / accumulated in
 // global memory (L1 / L2) and only V, Y and the tables are staged.  V^T is read from
 // V with swapped indices.
-__host__ __device__ inline SheSmem she_layout(int n, int dimens, int n_neigh, bool staged) {
+__host__ __device__ inline SheSmem she_layout(int n, int dimens, int n_neigh, bool staged, bool acc_smem = true) {
   const int no = n / 2;
   SheSmem L;
   int o = 0;
@@ -83,7 +83,7 @@ __host__ __device__ inline SheSmem she_layout(int n, int dimens, int n_neigh, bo
   L.s2 = o; o += staged ? n * she_sst(n) : 0;
   L.m = o; o += no * no;
   L.y = o; o += 2 * n * she_yst(no);
-  L.acc = o; o += staged ? 4 * dimens : 0;
+  L.acc = o; o += staged && acc_smem ? 4 * dimens : 0;
   L.ph = o; o += n_neigh > 0 ? n_neigh : 1;
   L.tab = o * (int)sizeof(double2);
   L.bytes = (size_t)L.tab + sizeof(int) * 4 * (size_t)no;
@@ -200,7 +200,77 @@ __device__ void she_z_tiled(const SheArgs& a, const double2* Y, RM R, double2* a
   }
 }
 
+// Second stage with the df entries in registers: the thread owns tile t (one tile per
+// thread) for the whole launch.  Slot (k, l) holds the entry (mu, nu) = (y0 + l, x0 + k).
+// A term with rows on nu (rows_are_nu) computes tile (x0, y0) as stored; a term with
+// rows on mu computes the mirrored tile (y0, x0), whose element (k', l') is that same
+// entry for (k', l') = (l, k), so both terms add into the same slots.
+template <class RM>
+__device__ void she_z_reg(const SheArgs& a, const double2* Y, RM R, double2 (&racc)[9], const int* tab,
+                          const unsigned char* spins, double2 f, bool rows_are_nu) {
+  const int n = a.n, no = a.no, yst = she_yst(no);
+  const int t = threadIdx.x;
+  if (t < a.n_ztiles) {
+    const int code = a.ztiles[t];
+    const int sigma = code & 3, sp = (code >> 2) & 3, i = (code >> 4) & 1023;
+    const int tx = (code >> 14) & 63, ty = (code >> 20) & 63;
+    const int x0 = rows_are_nu ? tx : ty, y0 = rows_are_nu ? ty : tx;
+    const int sc = spins[sigma * 4 + sp];
+    const int sa = (sc >> 3) & 1, b = (sc >> 2) & 1, c = (sc >> 1) & 1, sd = sc & 1;
+    const int ni = a.norb[i], ia = a.ia[i];
+    const double2* Yb = Y + (b * n + ia + sa * ni) * yst;
+    const int* rowc = tab + c * no;
+    const int col0 = ia + sd * ni + y0;
+    double2 z[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) z[k][l] = make_double2(0.0, 0.0);
+    for (int o1 = 0; o1 < no; ++o1) {
+      const int rc = rowc[o1];
+      double2 yv[3], rv[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) yv[k] = x0 + k < ni ? Yb[(x0 + k) * yst + o1] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int l = 0; l < 3; ++l) rv[l] = y0 + l < ni ? R(rc, col0 + l) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int l = 0; l < 3; ++l) z[k][l] = cfma(yv[k], rv[l], z[k][l]);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int l = 0; l < 3; ++l) {
+        const int slot = rows_are_nu ? 3 * k + l : 3 * l + k;
+        racc[slot] = cfma(f, z[k][l], racc[slot]);   // invalid slots only ever add zeros
+      }
+  }
+}
+
+// df entry of register slot (k, l) of this thread's tile, or -1
+__device__ __forceinline__ int she_slot_entry(const SheArgs& a, int slot) {
+  const int t = threadIdx.x;
+  if (t >= a.n_ztiles) return -1;
+  const int code = a.ztiles[t];
+  const int sigma = code & 3, sp = (code >> 2) & 3, i = (code >> 4) & 1023;
+  const int x0 = (code >> 14) & 63, y0 = (code >> 20) & 63;
+  const int k = slot / 3, l = slot % 3, ni = a.norb[i];
+  if (x0 + k >= ni || y0 + l >= ni) return -1;
+  const int mu = y0 + l, nu = x0 + k;
+  return sp * a.dimens + a.rowoff[i] + sigma + 4 * (mu * ni + nu);
+}
+
 // the term with the df slice in memory (shared or global), both stages register-tiled
+template <class LM, class RM>
+__device__ void she_term_reg(const SheArgs& a, LM L, const double2* M, bool mt, RM R, double2* Y,
+                             double2 (&racc)[9], const int* tab, const unsigned char* spins, double2 f,
+                             bool rows_are_nu) {
+  she_y_tiled(a, L, M, mt, Y, tab);
+  she_z_reg(a, Y, R, racc, tab, spins, f, rows_are_nu);
+  __syncthreads();
+}
+
 template <class LM, class RM>
 __device__ void she_term(const SheArgs& a, LM L, const double2* M, bool mt, RM R, double2* Y, double2* acc,
                          const int* tab, const unsigned char* spins, double2 f, bool rows_are_nu) {
@@ -209,11 +279,16 @@ __device__ void she_term(const SheArgs& a, LM L, const double2* M, bool mt, RM R
   __syncthreads();
 }
 
-template <bool STAGED>
-__global__ void __launch_bounds__(kSheThreads) she_kernel(SheArgs a) {
+// STAGED: Green functions in shared memory.  REG (staged only, at most one second-stage
+// tile per thread): each thread keeps its tile's df entries in registers for the whole
+// launch, and the df slice leaves shared memory (no read-modify-write there, whose
+// 16-byte accesses of a quarter warp fell into two bank groups).
+template <bool STAGED, bool REG>
+__device__ __forceinline__ void she_body(const SheArgs& a) {
+  static_assert(STAGED || !REG, "register slices only in the staged kernel");
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = a.n, no = a.no, D = a.dimens;
-  const SheSmem L = she_layout(n, D, a.n_neigh, STAGED);
+  const SheSmem L = she_layout(n, D, a.n_neigh, STAGED, !REG);
   double2* base = reinterpret_cast<double2*>(smem);
   double2* S1 = base + L.s1;
   double2* S2 = base + L.s2;
@@ -223,9 +298,17 @@ __global__ void __launch_bounds__(kSheThreads) she_kernel(SheArgs a) {
   double2* ph = base + L.ph;
   int* tab = reinterpret_cast<int*>(smem + L.tab);
   double2* mine = a.partial + (size_t)blockIdx.x * 4 * D;
-  double2* acc = STAGED ? base + L.acc : mine;
-  if (STAGED)
+  double2* acc = STAGED && !REG ? base + L.acc : mine;
+  double2 racc[9];
+  if (REG) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      const int o = she_slot_entry(a, j);
+      racc[j] = o >= 0 ? mine[o] : make_double2(0.0, 0.0);
+    }
+  } else if (STAGED) {
     for (int e = threadIdx.x; e < 4 * D; e += blockDim.x) acc[e] = mine[e];
+  }
   for (int e = threadIdx.x; e < 4 * no; e += blockDim.x) tab[e] = a.tab[e];
   __syncthreads();
   for (int64_t pl = blockIdx.x; pl < a.np; pl += gridDim.x) {
@@ -291,7 +374,22 @@ __global__ void __launch_bounds__(kSheThreads) she_kernel(SheArgs a) {
       M[rr * no + cc] = v;
     }
     __syncthreads();
-    if (STAGED) {
+    if (REG) {
+      if (!a.real_axis) {
+        she_term_reg(a, RowMajor{S1, sst}, M, false, RowMajor{S2, sst}, Y, racc, tab, a.spins[0],
+                     make_double2(w, 0.0), true);
+        for (int e = threadIdx.x; e < n * sst; e += blockDim.x) {
+          S1[e].y = -S1[e].y;
+          S2[e].y = -S2[e].y;
+        }
+        __syncthreads();
+        she_term_reg(a, RowMajor{S2, sst}, M, true, RowMajor{S1, sst}, Y, racc, tab, a.spins[1],
+                     make_double2(w, 0.0), false);
+      } else {
+        she_term_reg(a, RowMajor{S1, sst}, M, false, RowMajor{S2, sst}, Y, racc, tab, a.spins[2],
+                     make_double2(0.0, -w), true);
+      }
+    } else if (STAGED) {
       if (!a.real_axis) {
         she_term(a, RowMajor{S1, sst}, M, false, RowMajor{S2, sst}, Y, acc, tab, a.spins[0], make_double2(w, 0.0),
                  true);
@@ -318,8 +416,25 @@ __global__ void __launch_bounds__(kSheThreads) she_kernel(SheArgs a) {
       }
     }
   }
-  if (STAGED)
+  if (REG) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      const int o = she_slot_entry(a, j);
+      if (o >= 0) mine[o] = racc[j];
+    }
+  } else if (STAGED) {
     for (int e = threadIdx.x; e < 4 * D; e += blockDim.x) mine[e] = acc[e];
+  }
+}
+
+template <bool STAGED>
+__global__ void __launch_bounds__(kSheThreads) she_kernel(SheArgs a) {
+  she_body<STAGED, false>(a);
+}
+
+// two CTAs per SM: registers capped at 65 536 / (2 x 288)
+__global__ void __launch_bounds__(kSheThreads, 2) she_kernel_reg(SheArgs a) {
+  she_body<true, true>(a);
 }
 
 // tchi(r, s') = scale sum_c P(r, c) df(c, s'), P column-major (dimens x dimens); P == nullptr: identity
@@ -339,11 +454,10 @@ __global__ void she_prefactor_kernel(const double2* __restrict__ P, const double
 
 }  // namespace
 
-// Variant choice: the staged kernel when its shared memory fits, else the
-// global-operand kernel; 0 bytes when neither fits.
-bool she_staged(int n, int dimens, int n_neigh, size_t optin) {
-  return she_layout(n, dimens, n_neigh, true).bytes <= optin;
-}
+// Variant choice: the register-slice kernel when every second-stage tile has its own
+// thread and its shared memory fits, else the staged kernel when its shared memory fits,
+// else the global-operand kernel; 0 bytes when none fits.
+enum SheVariant { SHE_GLOBAL = 0, SHE_STAGED = 1, SHE_REG = 2 };
 
 int she_optin() {
   int dev = 0, optin = 0;
@@ -352,19 +466,34 @@ int she_optin() {
   return optin;
 }
 
-size_t she_smem_bytes(int n, int dimens, int n_neigh) {
+SheVariant she_variant(int n, int dimens, int n_neigh, int n_ztiles, size_t optin) {
+  if (n_ztiles <= kSheThreads && she_layout(n, dimens, n_neigh, true, false).bytes <= optin) return SHE_REG;
+  if (she_layout(n, dimens, n_neigh, true).bytes <= optin) return SHE_STAGED;
+  return SHE_GLOBAL;
+}
+
+size_t she_variant_bytes(int n, int dimens, int n_neigh, SheVariant v) {
+  return she_layout(n, dimens, n_neigh, v != SHE_GLOBAL, v != SHE_REG).bytes;
+}
+
+const void* she_variant_fn(SheVariant v) {
+  if (v == SHE_REG) return (const void*)she_kernel_reg;
+  if (v == SHE_STAGED) return (const void*)she_kernel<true>;
+  return (const void*)she_kernel<false>;
+}
+
+size_t she_smem_bytes(int n, int dimens, int n_neigh, int n_ztiles) {
   const int optin = she_optin();
-  const bool staged = she_staged(n, dimens, n_neigh, (size_t)optin);
-  const size_t b = she_layout(n, dimens, n_neigh, staged).bytes;
+  const size_t b = she_variant_bytes(n, dimens, n_neigh, she_variant(n, dimens, n_neigh, n_ztiles, (size_t)optin));
   return b <= (size_t)optin ? b : 0;
 }
 
-int she_grid(int n, int dimens, int n_neigh, int num_sms) {
+int she_grid(int n, int dimens, int n_neigh, int n_ztiles, int num_sms) {
   const int optin = she_optin();
-  const bool staged = she_staged(n, dimens, n_neigh, (size_t)optin);
-  const size_t smem = she_layout(n, dimens, n_neigh, staged).bytes;
+  const SheVariant v = she_variant(n, dimens, n_neigh, n_ztiles, (size_t)optin);
+  const size_t smem = she_variant_bytes(n, dimens, n_neigh, v);
   if (smem > (size_t)optin) return 0;
-  const void* fn = staged ? (const void*)she_kernel<true> : (const void*)she_kernel<false>;
+  const void* fn = she_variant_fn(v);
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kSheThreads, smem) != cudaSuccess) return 0;
@@ -406,13 +535,14 @@ cudaError_t launch_she(const SheLaunch& l, cudaStream_t s) {
   a.klist = l.klist;
   const int optin = she_optin();
   if (optin <= 0) return cudaErrorInvalidValue;
-  const bool staged = she_staged(a.n, a.dimens, a.n_neigh, (size_t)optin);
-  const size_t smem = she_layout(a.n, a.dimens, a.n_neigh, staged).bytes;
+  const SheVariant v = she_variant(a.n, a.dimens, a.n_neigh, a.n_ztiles, (size_t)optin);
+  const size_t smem = she_variant_bytes(a.n, a.dimens, a.n_neigh, v);
   if (smem > (size_t)optin) return cudaErrorInvalidValue;
-  const void* fn = staged ? (const void*)she_kernel<true> : (const void*)she_kernel<false>;
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(she_variant_fn(v), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  if (staged)
+  if (v == SHE_REG)
+    she_kernel_reg<<<l.grid, kSheThreads, smem, s>>>(a);
+  else if (v == SHE_STAGED)
     she_kernel<true><<<l.grid, kSheThreads, smem, s>>>(a);
   else
     she_kernel<false><<<l.grid, kSheThreads, smem, s>>>(a);
