@@ -15,15 +15,17 @@
 // memory from per-neighbour phases, then two small products per term:
 // Y^b = L[:, spin b] V (n x no) and Z = Y^b R[spin c, :] restricted to the
 // output entries, which form n_i x n_i blocks per (sigma, s', site).  Both
-// products are register-tiled (3 x 3 outputs per thread), so each operand read
-// from shared memory feeds three complex FMAs; shared-memory bandwidth bounds
-// the kernel.  Each CTA owns a slice (4 dimens complex) of a per-CTA
-// global array, so successive launches (passes) accumulate without atomics;
-// the slices are summed once at the end.  When they fit (dimH up to about 48
-// for small dimens), both Green functions are staged row-major in shared memory
-// and the slice is held there during the launch; larger cells read the
-// column-major inversion output through L1 / L2 and add into the slice in
-// place.
+// products are register-tiled (2 x 3 and 3 x 3 outputs per thread), so each
+// operand read from shared memory feeds two to three complex FMAs;
+// shared-memory bandwidth bounds the kernel.  Each CTA owns a slice (4 dimens
+// complex) of a per-CTA global array, so successive launches (passes)
+// accumulate without atomics; the slices are summed once at the end.  Three
+// variants: when every second-stage tile has its own thread (two spd sites at
+// 288 threads), the slice entries stay in the owning threads' registers for the
+// launch (she_kernel_reg); else, when they fit (dimH up to about 48 for small
+// dimens), both Green functions are staged row-major in shared memory and the
+// slice is held there; larger cells read the column-major inversion output
+// through L1 / L2 and add into the slice in place.
 #include "tg_internal.cuh"
 
 #include <algorithm>
