@@ -1,0 +1,104 @@
+"""The split-precision number format of the tcgen05 chi0 contraction, restated in numpy.
+
+Test infrastructure only: the CUDA kernels (split_quantize_kernel,
+split_contract_kernel) are what ships; this file checks the format they
+implement, on the CPU.
+  * per chunk and operand element the scale 2^(38 - E), E the frexp exponent of
+    the chunk's largest |Re|, |Im|; X = rint(x 2^(38 - E)), |X| <= 2^38;
+  * five balanced base-256 digits, most significant first: with Y = X +
+    0x80808080 the low four are the bytes of Y's low word minus 128 and the top
+    one is Y >> 32, so X = d0 2^32 + d1 2^24 + d2 2^16 + d3 2^8 + d4 exactly;
+  * the 19 digit products of levels l = i + j <= 5 summed per level in exact
+    integers, recombined as sum_l S_l 2^(-12 - 8 l) 2^(E_A + E_B).
+The operands are Green functions of the synthetic sq2 system near the real
+axis, in the layout of the contraction (A = w G1, B = G2^T per point), so the
+error is that of the realistic sums the format was chosen on.
+"""
+import numpy as np
+
+from oracle import titan_oracle as O
+from titan_b200.host import synthetic
+from titan_b200.host.system import initial_state
+
+BITS = 38
+
+
+def digits(X):
+    """Balanced base-256 digits of int64 X (|X| <= 2^38), most significant first."""
+    Y = X + 0x80808080
+    low = (Y & 0xFFFFFFFF).astype(np.uint32) ^ np.uint32(0x80808080)
+    d = [(Y >> 32).astype(np.int64)]
+    for sh in (24, 16, 8, 0):
+        d.append(((low >> np.uint32(sh)) & np.uint32(0xFF)).astype(np.int64).astype(np.int8).astype(np.int64))
+    return d
+
+
+def quantise(x):
+    """x [points, elements] real -> (digits, E per element) over the chunk (all points)."""
+    m = np.max(np.abs(x), axis=0)
+    E = np.where(m > 0, np.frexp(m)[1], 0)
+    X = np.rint(np.ldexp(x, BITS - E[None, :])).astype(np.int64)
+    assert np.max(np.abs(X)) <= 2 ** BITS
+    return digits(X), E, X
+
+
+def split_product(a, b, max_level=5):
+    """sum_p a[p, u] b[p, v] for real a, b through the digit format."""
+    da, Ea, _ = quantise(a)
+    db, Eb, _ = quantise(b)
+    out = np.zeros((a.shape[1], b.shape[1]))
+    for lvl in range(max_level + 1):
+        S = np.zeros_like(out)
+        for i in range(5):
+            j = lvl - i
+            if 0 <= j < 5:
+                S += (da[i].T @ db[j]).astype(np.float64)   # exact: |S| < 2^53 here
+        out += np.ldexp(S, -12 - 8 * lvl)
+    return np.ldexp(out, Ea[:, None] + Eb[None, :])
+
+
+def complex_split(A, B, max_level=5):
+    rr = split_product(A.real, B.real, max_level)
+    ii = split_product(A.imag, B.imag, max_level)
+    ri = split_product(A.real, B.imag, max_level)
+    ir = split_product(A.imag, B.real, max_level)
+    return (rr - ii) + 1j * (ri + ir)
+
+
+def operands(npts=96, y=2e-3):
+    s = synthetic.make_system("sq2")
+    m = O.Model(s, s.h0(initial_state(s)))
+    rng = np.random.default_rng(5)
+    k = rng.uniform(-0.5, 0.5, size=(npts, 3))
+    k[:, 2] = 0.0
+    z = s.Ef + 1j * y
+    G2 = m.green(np.full(npts, z), k)
+    G1 = m.green(np.full(npts, z + 0.05), k)
+    w = rng.uniform(0.5, 1.5, size=npts) / npts
+    # one site-pair block (site 0 rows, site 1 columns) of A = w G1 and B = G2^T
+    n0 = s.norbs[0]
+    r = np.r_[0:n0, n0:2 * n0]
+    c = np.r_[2 * n0:2 * n0 + s.norbs[1], 2 * n0 + s.norbs[1]:2 * n0 + 2 * s.norbs[1]]
+    A = (w[:, None, None] * G1[:, r][:, :, c]).reshape(npts, -1)
+    B = np.transpose(G2, (0, 2, 1))[:, c][:, :, r].reshape(npts, -1)
+    return A, B
+
+
+def test_digits_reconstruct_exactly():
+    rng = np.random.default_rng(0)
+    X = rng.integers(-2 ** BITS, 2 ** BITS + 1, size=20000, dtype=np.int64)
+    X[:4] = [2 ** BITS, -2 ** BITS, 0, -1]
+    d = digits(X)
+    assert all(np.all(np.abs(di) <= 128) for di in d[1:])
+    rec = d[0] * 2 ** 32 + d[1] * 2 ** 24 + d[2] * 2 ** 16 + d[3] * 2 ** 8 + d[4]
+    assert np.array_equal(rec, X)
+
+
+def test_split_contraction_error_and_dropped_levels():
+    A, B = operands()
+    ref = A.T @ B
+    err = np.linalg.norm(complex_split(A, B) - ref) / np.linalg.norm(ref)
+    assert err < 1e-9, err
+    # dropping level 5 (the digit products of level L = 7) costs accuracy the format cannot afford
+    err6 = np.linalg.norm(complex_split(A, B, max_level=4) - ref) / np.linalg.norm(ref)
+    assert err6 > 10 * err, (err, err6)
