@@ -102,3 +102,23 @@ def test_split_contraction_error_and_dropped_levels():
     # dropping level 5 (the digit products of level L = 7) costs accuracy the format cannot afford
     err6 = np.linalg.norm(complex_split(A, B, max_level=4) - ref) / np.linalg.norm(ref)
     assert err6 > 10 * err, (err, err6)
+
+
+def test_exponent_sidecar_gives_the_quantiser_the_same_scale():
+    """The spectral G kernel stores per value the exponent field of max(|Re|, |Im|) minus
+    1022 (-32768 for zero or subnormal); the row maxima store 2^(E - 1) of the largest.
+    That equals frexp's exponent of the true maximum, and 2^(E - 1) gives it back."""
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((4000, 2)) * np.exp(rng.uniform(-700, 700, size=(4000, 1)))
+    x[:3] = [[0.0, 0.0], [5e-324, 0.0], [1.0, -1.0]]
+    m = np.max(np.abs(x), axis=1)
+    f = (m.view(np.int64) >> 52) & 0x7FF
+    code = np.where(f == 0, -32768, f - 1022)
+    normal = f != 0
+    assert np.array_equal(code[normal], np.frexp(m[normal])[1])
+    for chunk in np.array_split(np.arange(len(m)), 40):
+        E = code[chunk].max()
+        if E == -32768:
+            continue
+        stored = np.ldexp(1.0, int(E) - 1)
+        assert np.frexp(stored)[1] == np.frexp(m[chunk].max())[1]
