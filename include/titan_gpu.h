@@ -223,8 +223,10 @@ int tg_ldos(tg_ctx* ctx, int n_e, const double* e, double eta, double* ldosu, do
  * error against the FP64 oracle as Gauss-Jordan), but the disturbance integral feeds
  * B_eff through an ill-conditioned site-reduced chi^-1, and the occupations feed a Newton
  * iteration whose step tolerance (mag_tol = 1e-12) the spectral noise exceeds, so:
- *   TG_GREEN_AUTO (default)  spectral for chi0 and tg_ldos, Gauss-Jordan for tg_she and
- *                            tg_expectation
+ *   TG_GREEN_AUTO (default)  spectral for chi0 and tg_ldos; Gauss-Jordan for
+ *                            tg_expectation; for tg_she spectral at Im z >= 10 eta and
+ *                            Gauss-Jordan below and on the real axis (dimH 36; elsewhere
+ *                            Gauss-Jordan)
  *   TG_GREEN_GAUSS_JORDAN    Gauss-Jordan everywhere
  *   TG_GREEN_SPECTRAL        spectral wherever the mesh allows (tg_she ~4x faster,
  *                            tg_expectation one eigendecomposition per k for all energies)

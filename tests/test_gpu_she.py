@@ -113,17 +113,21 @@ def test_she_nanoribbon_golden_through_gpu(gpu):
 
 @pytest.mark.parametrize("shape,e,q", [("bcc1", 0.04, (0.1, 0.0, 0.2)), ("sq2", 0.05, (0.0, 0.0, 0.0))])
 def test_she_spectral_equals_gauss_jordan(gpu, shape, e, q):
-    """The disturbance integral from spectral Green functions (uniform meshes, on request)
-    and from Gauss-Jordan per point (the default for this integral) agree to 1e-12."""
+    """The disturbance integral from spectral Green functions (uniform meshes, on request),
+    from Gauss-Jordan per point and from the default (at dimH 36 the split: spectral for
+    Im z >= 10 eta, Gauss-Jordan below) agree to 1e-12."""
     deck = synthetic.make_deck(shape, nk=(4, 4, 4) if shape == "bcc1" else (6, 6, 1), n1gl=6, parts=1, n3gl=4)
     s = deck.system
     gpu.setup(deck, s.h0(initial_state(s)))
     x2, p2 = deck.real_points(e, s.Ef)
     q = np.array(q, float)
-    gj = gpu.she(q, e, s.Ef, s.eta, s.etap, x2, p2, UE)
+    auto = gpu.she(q, e, s.Ef, s.eta, s.etap, x2, p2, UE)
     try:
         gpu.set_green_method("spectral")
         sp = gpu.she(q, e, s.Ef, s.eta, s.etap, x2, p2, UE)
+        gpu.set_green_method("gauss-jordan")
+        gj = gpu.she(q, e, s.Ef, s.eta, s.etap, x2, p2, UE)
     finally:
         gpu.set_green_method("auto")
     assert np.max(np.abs(sp - gj)) <= 1e-12 * np.max(np.abs(gj))
+    assert np.max(np.abs(auto - gj)) <= 1e-12 * np.max(np.abs(gj))

@@ -1855,10 +1855,16 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
   const bool tab_imag = c->imag_uniform && (int64_t)c->nk_u * nn * 16 <= ((int64_t)8 << 30);
   const bool tab_real = real && (int64_t)c->n_realk * nn * 16 <= ((int64_t)8 << 30);
   const bool spec = spectral_forced(c);
-  if (spec && (tab_imag || tab_real) && (rc = reset_eig_status(c))) return rc;
+  // AUTO at n = 36 on a tabulated imaginary axis: spectral G for the energies with
+  // Im z >= 10 eta (its eps |H| / Im z error is negligible there; the nanoribbon goldens
+  // hold with the split at 10 eta), the one-warp Gauss-Jordan kernel below and on the real axis
+  const bool hybrid = !spec && c->green_method == TG_GREEN_AUTO && tab_imag && eig_supported(n) &&
+                      green_w1_supported(n, MODE_RAW);
+  const double y_split = 10.0 * eta;
+  if ((spec || hybrid) && (tab_imag || tab_real) && (rc = reset_eig_status(c))) return rc;
   auto tables = [&](int slot, const double* d_k, int64_t nk, bool shift) -> int {
     if ((rc = build_htab(c, slot, d_k, nk, shift ? q : zero3))) return rc;
-    if (spec && (rc = build_eig(c, slot, nk))) return rc;
+    if ((spec || (hybrid && slot < 2)) && (rc = build_eig(c, slot, nk))) return rc;
     return TG_OK;
   };
   if (tab_imag) {
@@ -1903,15 +1909,38 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
   l.grid = grid;
   // one pass: G2 = G(k, E), G1 = G(k + q, E + e), both column-major per point, then the
   // vertex; slot2 / slot1 >= 0: H(k) tables of G2 / G1 with n_e energies per k (k-major order)
+  // one G launch, or for the hybrid the spectral part (eigendecomposition of the slot) and
+  // the Gauss-Jordan part of the same points
+  auto green = [&](GreenArgs g, int slot, bool split, const char* what) -> int {
+    if (!split) {
+      KindTimer kt(c, 0);
+      TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), what);
+      return TG_OK;
+    }
+    GreenArgs gs = g;
+    gs.eigU = c->d_eigU[slot].p;
+    gs.eigL = c->d_eigL[slot].p;
+    gs.outinv = c->d_outinv.p;
+    gs.y_split = y_split;
+    gs.y_side = 1;
+    GreenArgs gj = g;
+    gj.eigU = nullptr;
+    gj.eigL = nullptr;
+    gj.y_split = y_split;
+    gj.y_side = -1;
+    KindTimer kt(c, 0);
+    TG_CHECK(c, launch_green(gs, c->num_sms, s, nullptr), what);
+    TG_CHECK(c, launch_green(gj, c->num_sms, s, nullptr), what);
+    c->launches += 1;
+    return TG_OK;
+  };
   auto pass = [&](GreenArgs g, int real_axis, int slot2, int slot1, int64_t n_e, int64_t nk,
                   const double* ylist, const double* klist) -> int {
+    const bool split = hybrid && !real_axis && slot2 >= 0;
     g.mode = MODE_RAW;
     g.out = c->d_B.p;
     if (slot2 >= 0) use_table(g, slot2, n_e, nk, ylist);
-    {
-      KindTimer kt(c, 0);
-      TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), "green (G2)");
-    }
+    if ((rc = green(g, slot2, split, "green (G2)"))) return rc;
     g.zr += e;
     g.zi = eta;
     g.q[0] = q[0];
@@ -1919,10 +1948,7 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
     g.q[2] = q[2];
     g.out = c->d_A.p;
     if (slot1 >= 0) use_table(g, slot1, n_e, nk, ylist);
-    {
-      KindTimer kt(c, 0);
-      TG_CHECK(c, launch_green(g, c->num_sms, s, nullptr), "green (G1)");
-    }
+    if ((rc = green(g, slot1, split, "green (G1)"))) return rc;
     l.n_e = slot2 >= 0 ? n_e : 0;
     l.nk_tab = nk;
     l.klist = klist;
@@ -1991,7 +2017,7 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
   profile_end(c);
   rc = read_status(c);
   if (rc) return rc;
-  if (spec && (tab_imag || tab_real)) return read_eig_status(c);
+  if ((spec || hybrid) && (tab_imag || tab_real)) return read_eig_status(c);
   return TG_OK;
 }
 

@@ -162,6 +162,9 @@ __global__ void __launch_bounds__(32 * kWarps, 1) green_w1_kernel(GreenArgs a) {
     zr = __shfl_sync(0xffffffffu, zr, 0);
     zi = __shfl_sync(0xffffffffu, zi, 0);
     w = __shfl_sync(0xffffffffu, w, 0);
+    // energy split: the spectral kernel writes the points with Im z >= y_split (zi is the
+    // same expression there, warp-uniform here, and this kernel has no block barrier)
+    if (a.y_side < 0 && a.htab && a.pts.kind == 0 && zi >= a.y_split) continue;
     if (ktab < 0) {
       kx = __shfl_sync(0xffffffffu, kx, 0);
       ky = __shfl_sync(0xffffffffu, ky, 0);

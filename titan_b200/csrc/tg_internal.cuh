@@ -143,6 +143,11 @@ struct GreenArgs {
   // frexp exponent of max(|Re|, |Im|), -32768 for zero or subnormal
   int16_t* eout = nullptr;
   int16_t* eout2 = nullptr;
+  // energy split of a tabulated imaginary-axis pass: y_side = +1 keeps the points with
+  // Im z >= y_split (spectral kernel), -1 those below (one-warp Gauss-Jordan kernel); other
+  // kernels ignore it and evaluate every point
+  double y_split = 0.0;
+  int y_side = 0;
 };
 
 // true when launch_green evaluates these arguments with the spectral kernel (the only

@@ -263,7 +263,8 @@ __global__ void __launch_bounds__(kSpecThreads, 5) spec_green_kernel(SpecArgs sa
     if (threadIdx.x < kSpecZ) {
       const int64_t ie = ie0 + threadIdx.x;
       const int64_t wi = ik * ne + ie;
-      item[threadIdx.x] = (ie < ne && wi >= a.p0 && wi < a.p0 + a.np) ? (int)(wi - a.p0) : -1;
+      const bool kept = a.y_side <= 0 || a.pts.kind != 0 || (ie < ne && a.zi + a.ylist[ie] >= a.y_split);
+      item[threadIdx.x] = (ie < ne && wi >= a.p0 && wi < a.p0 + a.np && kept) ? (int)(wi - a.p0) : -1;
     }
     const double2* Uk = sa.U + ik * (int64_t)nn;
     for (int e = threadIdx.x; e < n * kp; e += blockDim.x) {
