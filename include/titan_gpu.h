@@ -2,7 +2,7 @@
  * titan_gpu.h -- C ABI of the B200 Green-function path (k-mesh x complex energy).
  *
  * Drop-in boundary for the reference's swappable Green-function routines.  A
- * Fortran host binds these with ISO_C_BINDING (see INTEGRATION.md); every
+ * Fortran host binds these with ISO_C_BINDING; every
  * array is caller-owned HOST memory in Fortran (column-major) order, complex
  * numbers are interleaved (re, im) doubles, and every call returns a status:
  *
@@ -90,13 +90,17 @@ int tg_expectation(tg_ctx* ctx, double Ef, double eta, double* rho, double* mx, 
                    double* mz, double* mp);
 
 /* tg_expectation without device allocation, for callers that cannot let a
- * library call allocate (a fixed HBM budget, or work recorded into a stream
- * capture).  No counterpart in the reference.  Same outputs as tg_expectation;
- * H(k) is summed inside the kernel and the partial sums live in a fixed 8 MiB
- * device array of the library: (16 x SMs + 1) x 2 dimH complex must fit, else
- * TG_ERR_ARG.  The first call on a device looks the array up (make it before any
- * stream capture); nothing has to start at zero; calls that overlap in time on
- * one device race on the shared array. */
+ * library call allocate: a host that gives the GPU's memory to its own pool or
+ * to another solver up front and budgets every byte of HBM itself.  No
+ * counterpart in the reference.  Same outputs as tg_expectation under its
+ * default method; this call always inverts per (k, z) point (Gauss-Jordan),
+ * whatever tg_set_green_method chose.  H(k) is summed inside the kernel and the
+ * partial sums live in a fixed 8 MiB device array of the library:
+ * (16 x SMs + 1) x 2 dimH complex must fit (dimH <= 90 on a B200), else
+ * TG_ERR_ARG before any work.  The first call on a context looks the array's
+ * address up on the context's device (make it before any stream capture);
+ * nothing has to start at zero; calls that overlap in time on one device race
+ * on the shared array. */
 int tg_expectation_noalloc(tg_ctx* ctx, double Ef, double eta, double* rho, double* mx, double* my,
                            double* mz, double* mp);
 

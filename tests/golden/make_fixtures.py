@@ -99,4 +99,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TITAN_REFERENCE")
+    if not root:
+        sys.exit("usage: make_fixtures.py <TITAN source tree>  (or set TITAN_REFERENCE)")
+    main(root)

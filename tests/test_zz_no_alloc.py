@@ -43,3 +43,23 @@ def test_noalloc_expectation_matches_tg_expectation(shape, nk):
                 assert np.max(np.abs(a - b)) < 1e-12
     finally:
         gpu.close()
+
+
+def test_noalloc_ignores_the_spectral_method():
+    """Under TG_GREEN_SPECTRAL tg_expectation diagonalises H(k); the no-alloc call still
+    inverts per point, so it equals the default (Gauss-Jordan) tg_expectation."""
+    from titan_b200.native import GreenGPU
+    deck = synthetic.make_deck("sq2", nk=(6, 6, 1), n1gl=8, parts=1, n3gl=4)
+    s = deck.system
+    h0 = s.h0(initial_state(s))
+    gpu = GreenGPU(0)
+    try:
+        gpu.setup(deck, h0)
+        ref = list(gpu.expectation(s.Ef, s.eta))
+        gpu.set_green_method("spectral")
+        for _ in range(2):
+            got = _call_noalloc(gpu, s.Ef, s.eta)
+            for a, b in zip(got, ref):
+                assert np.max(np.abs(a - b)) < 1e-12
+    finally:
+        gpu.close()

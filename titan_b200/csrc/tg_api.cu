@@ -10,7 +10,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -134,6 +133,9 @@ struct tg_ctx {
   // disturbance response (eintshe)
   DevArray<int> d_she_tab, d_ia, d_she_ztiles, d_she_rowoff;
   DevArray<double2> d_she_part, d_she_sum, d_she_pref, d_she_out;
+  // tg_expectation_noalloc: device address of the library's fixed scratch array on this
+  // context's device (looked up by the context's first no-alloc call)
+  double2* noalloc_ptr = nullptr;
 };
 
 namespace {
@@ -2025,18 +2027,26 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
 // tg_expectation_noalloc: occupations and moments without device allocation.
 //
 // For callers that cannot let a library call allocate device memory: a host
-// that budgets every byte of HBM up front, or code that records its work into
-// a stream capture, where cudaMalloc is not allowed.  tg_expectation allocates
-// its per-team partial sums (and an H(k) table) on first use; this variant keeps
-// the partial sums in a fixed 8 MiB device array compiled into the library and
-// sums H(k) inside the inversion kernel instead of tabulating it.
+// that hands the GPU's memory to its own pool or to another solver up front and
+// budgets every byte of HBM itself, so that a cudaMalloc inside a library call
+// would fail or break that budget.  tg_expectation allocates its per-team
+// partial sums (and an H(k) table) on first use; this variant keeps the partial
+// sums in a fixed 8 MiB device array compiled into the library and sums H(k)
+// inside the inversion kernel instead of tabulating it.
 //
 // * Size limit: (16 x SMs + 1) x 2 dimH complex doubles must fit in 8 MiB
-//   (dimH <= 90 on a 148-SM B200 needs 6.8 MB); larger requests return
-//   TG_ERR_ARG before any work.
-// * Setup: the first call on each device looks up the array's device address
-//   (cudaGetSymbolAddress, which also loads this module on that device if it is
-//   not loaded yet); make one call before beginning any stream capture.
+//   (dimH <= 90 on a 148-SM B200 needs 6.8 MB); larger requests, and dimensions
+//   that only the general-dimension kernel handles, return TG_ERR_ARG before
+//   any work.
+// * Method: always Gauss-Jordan per (k, z) point, whatever tg_set_green_method
+//   chose (the default choice of tg_expectation; its TG_GREEN_SPECTRAL form would
+//   need eigenvector tables in allocated memory).
+// * Setup: the first call on a context looks up the array's device address on
+//   the context's device (cudaGetSymbolAddress with that device current, which
+//   also loads this module there if it is not loaded yet) and keeps it in the
+//   context; make that first call before any stream capture.  After a
+//   cudaDeviceReset the context's stream and buffers are gone as well: destroy
+//   the context and create a new one, which looks the address up again.
 // * Nothing in the scratch has to start at zero: every partial slot the
 //   reduction reads is written by the kernel of the same call.
 // * One array serves every context and stream of a device: calls that overlap
@@ -2045,27 +2055,22 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
 // ---------------------------------------------------------------------------
 namespace {
 constexpr size_t kNoAllocScratchBytes = (size_t)8 << 20;
-constexpr int kNoAllocMaxDevices = 64;
 constexpr int kNoAllocMaxLen = 512;   // 2 dimH complex sums per partial slot
-std::atomic<double2*> g_noalloc_ptr[kNoAllocMaxDevices];
 }  // namespace
 
 static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double2)];
 
 namespace {
-// device address of the scratch on the current device (looked up once per device)
+// device address of the scratch on the context's device (looked up on the context's
+// first call, with that device current)
 int noalloc_scratch(tg_ctx* c, double2** out) {
-  if (c->device < 0 || c->device >= kNoAllocMaxDevices)
-    return set_err(c, TG_ERR_ARG, "tg_expectation_noalloc: device index beyond the scratch table");
-  double2* p = g_noalloc_ptr[c->device].load(std::memory_order_acquire);
-  if (!p) {
+  if (!c->noalloc_ptr) {
     void* q = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&q, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_err(c, e, "tg_expectation_noalloc: scratch address");
-    p = static_cast<double2*>(q);
-    g_noalloc_ptr[c->device].store(p, std::memory_order_release);
+    c->noalloc_ptr = static_cast<double2*>(q);
   }
-  *out = p;
+  *out = c->noalloc_ptr;
   return TG_OK;
 }
 }  // namespace
@@ -2080,6 +2085,9 @@ extern "C" int tg_expectation_noalloc(tg_ctx* c, double Ef, double eta, double* 
   // partial slots: the team kernel runs at most 15 teams per SM (per-SM CTAs x teams <= 8 + teams - 1)
   const size_t slots = (size_t)c->num_sms * 16;
   const size_t need = (slots + 1) * (size_t)len * sizeof(double2);
+  if (!green_supported(n))
+    return set_err(c, TG_ERR_ARG, "tg_expectation_noalloc: this dimension needs the general-dimension kernel, "
+                                  "which keeps its Green functions in allocated memory");
   if (len > kNoAllocMaxLen || need > kNoAllocScratchBytes) {
     char b[160];
     snprintf(b, sizeof b, "tg_expectation_noalloc: needs %zu bytes of scratch, the fixed scratch holds %zu",
