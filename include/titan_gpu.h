@@ -84,6 +84,19 @@ int tg_chi0_batch(tg_ctx* ctx, const double* q, int n_omega, const double* e, do
                   double eta, double etap, int n_real, const double* x2, const double* p2,
                   int precision, int dimens, double* chiorb_hf);
 
+/* Restricts chi0 (tg_chi0, tg_chi0_batch) to a subset of each site's orbitals:
+ * mask(norb_max, n_atoms) flags the orbitals mu (both spins) that enter chi; null
+ * restores every orbital (the reference's dimens = 4 sum_i nOrb_i^2).  With a mask,
+ * dimens = 4 sum_i nc_i^2 (nc_i flagged orbitals of site i) and chiorb_hf is the
+ * sub-block of the reference's chiorb_hf over those orbitals, in the same
+ * sigmaimunu2i order restricted to them (sigma fastest, then nu, mu, site;
+ * mod_System.F90:176-187).  Flagging the d orbitals gives the d-only chi whose RPA
+ * Dyson solve (tg_dyson with U restricted to the same rows) equals the d-d block of
+ * the full one, because U is non-zero only between d orbitals
+ * (mod_susceptibilities.F90:106-159).  tg_set_system clears the mask.  No
+ * counterpart in the reference. */
+int tg_set_chi_orbitals(tg_ctx* ctx, const int* mask);
+
 /* Occupations and moments: replaces expectation_values_greenfunction
  * (source/mod_expectation.F90:28-149).  All outputs (norb_max, n_atoms). */
 int tg_expectation(tg_ctx* ctx, double Ef, double eta, double* rho, double* mx, double* my,

@@ -105,9 +105,35 @@ def _chunks(P, size):
         yield slice(s, min(P, s + size))
 
 
-def _scatter_fn(s):
-    sidx = s.sigmaimunu2i()
-    norbs = s.norbs
+def _sel_blk(sel):
+    """_blk restricted to the orbitals sel[i] of every site (both spins)."""
+    def blk(G, ia, norbs, i, j, spins):
+        si, sj = _SPIN[spins[0]], _SPIN[spins[1]]
+        r = ia[i][0] + si * norbs[i] + np.asarray(sel[i], dtype=np.int64)
+        c = ia[j][0] + sj * norbs[j] + np.asarray(sel[j], dtype=np.int64)
+        return G[:, r[:, None], c[None, :]]
+    return blk
+
+
+def sel_sigmaimunu2i(sel):
+    """0-based chi row map [4, nAtoms, nc, nc] over the orbital subset sel[i] of each site:
+    the order of sigmaimunu2i (mod_System.F90:176-187) restricted to those orbitals (local
+    indices 0..nc_i-1 in the order of sel[i])."""
+    nmax = max(len(x) for x in sel)
+    idx = np.full((4, len(sel), nmax, nmax), -1, dtype=np.int64)
+    k = 0
+    for i, x in enumerate(sel):
+        for mu in range(len(x)):
+            for nu in range(len(x)):
+                for sg in range(4):
+                    idx[sg, i, mu, nu] = k
+                    k += 1
+    return idx
+
+
+def _scatter_fn(s, sel=None):
+    sidx = s.sigmaimunu2i() if sel is None else sel_sigmaimunu2i(sel)
+    norbs = s.norbs if sel is None else [len(x) for x in sel]
 
     def scatter(target, i, j, s1, s2, block):
         # block[mu, nu, gama, xi] -> target[sigmaimunu2i(s1,i,mu,nu), sigmaimunu2i(s2,j,gama,xi)]
@@ -118,7 +144,7 @@ def _scatter_fn(s):
     return scatter
 
 
-def _imag_terms(s, g1, g2, w, target, scatter):
+def _imag_terms(s, g1, g2, w, target, scatter, _blk=_blk):
     """Imaginary-axis integrand of eintshechi.F90:86-104 for G1 = g1, G2 = g2 (weights w), added to target."""
     ia = s.ia()
     norbs = s.norbs
@@ -135,7 +161,7 @@ def _imag_terms(s, g1, g2, w, target, scatter):
                 scatter(target, i, j, s1, s2, t1 + t2)
 
 
-def _real_terms(s, g1, g2, w, target, scatter):
+def _real_terms(s, g1, g2, w, target, scatter, _blk=_blk):
     """Real-axis integrand of eintshechi.F90:146-164 for G1 = g1, G2 = g2 (weights w), added to target."""
     ia = s.ia()
     norbs = s.norbs
@@ -159,32 +185,49 @@ def _real_list(real_bz, x2, p2):
     return xs, ws, ks
 
 
-def eintshechi(model: Model, mesh, real_bz, q, e, Ef, eta, etap, x2=None, p2=None, chunk=4096):
+def eintshechi(model: Model, mesh, real_bz, q, e, Ef, eta, etap, x2=None, p2=None, chunk=4096, sel=None):
     """chi0_HF(q, e) of eintshechi.F90:2-178 (before the MPI reduction).
 
     ``mesh`` is the imaginary-axis (E, k) list; ``real_bz`` = (kp, w) of the
     real-axis BZ; (x2, p2) the real-axis energy points (generated by the caller
-    with generate_real_epoints).  Returns chiorb_hf[dimens, dimens].
+    with generate_real_epoints).  Returns chiorb_hf[dimens, dimens]; with ``sel``
+    (per site, the local orbital indices kept) only the sub-block over those
+    orbitals, in the sigmaimunu2i order restricted to them (sel_sigmaimunu2i), with
+    the same per-element sums.
     """
     s = model.system
-    D = s.dimens
+    D = s.dimens if sel is None else 4 * sum(len(x) ** 2 for x in sel)
+    blk = _blk if sel is None else _sel_blk(sel)
     chi = np.zeros((D, D), dtype=complex)
     fint = np.zeros((D, D), dtype=complex)
     q = np.asarray(q, float)
-    scatter = _scatter_fn(s)
+    scatter = _scatter_fn(s, sel)
     y = mesh.point_energy()
     for sl in _chunks(mesh.n_points, chunk):
         kp = mesh.kp[sl]
         g1 = model.green(Ef + e + 1j * (y[sl] + eta), kp + q[None, :])   # gfq
         g2 = model.green(Ef + 1j * (y[sl] + etap), kp)                   # gf
-        _imag_terms(s, g1, g2, mesh.weight[sl], chi, scatter)
+        _imag_terms(s, g1, g2, mesh.weight[sl], chi, scatter, blk)
     if x2 is not None and len(x2) > 0:
         xs, ws, ks = _real_list(real_bz, x2, p2)
         for sl in _chunks(xs.shape[0], chunk):
             g1 = model.green(xs[sl] + e + 1j * eta, ks[sl] + q[None, :])
             g2 = model.green(xs[sl] + 1j * etap, ks[sl])
-            _real_terms(s, g1, g2, ws[sl], fint, scatter)
+            _real_terms(s, g1, g2, ws[sl], fint, scatter, blk)
     return (chi + fint) / TPI
+
+
+def sel_rows(system, sel):
+    """Rows of the full chiorb_hf that the orbital subset sel keeps, in the subset's order."""
+    sidx = system.sigmaimunu2i()
+    sub = sel_sigmaimunu2i(sel)
+    rows = np.zeros(4 * sum(len(x) ** 2 for x in sel), dtype=np.int64)
+    for i, x in enumerate(sel):
+        for a, mu in enumerate(x):
+            for b, nu in enumerate(x):
+                for sg in range(4):
+                    rows[sub[sg, i, a, b]] = sidx[sg, i, mu, nu]
+    return rows
 
 
 def eintshechi_linear_soc(model0: Model, vsoc, mesh, real_bz, q, e, Ef, eta, etap, x2=None, p2=None, chunk=2048):

@@ -63,6 +63,39 @@ struct DevArray {
   }
 };
 
+// Layout of the chi0 contraction over a subset of each site's orbitals (tg_set_chi_orbitals):
+// the pair-block operand layout of those orbitals (slot o -> entry outmap[o] = r * dimH + c
+// of the full G), its contraction tiles and split groups, and the epilogue's row decode.
+struct ChiLayout {
+  int dimens = 0;
+  int nsel = 0;                       // rows of G that enter chi (2 sum nc)
+  std::vector<int> nc;                // chi orbitals per site
+  std::vector<int> pair_M, pair_aoff;
+  std::vector<int64_t> pair_coff;
+  std::vector<PairTile> tiles;
+  SplitLayout split;
+  DevArray<int> d_outmap, d_decode, d_norb, d_pair_M, d_pair_aoff;
+  DevArray<int64_t> d_pair_coff;
+  DevArray<PairTile> d_tiles;
+  DevArray<SplitGroup> d_sgA, d_sgB;
+  DevArray<SplitTile> d_stiles;
+};
+
+// what the chi0 helpers read: the full layout of tg_set_system or a ChiLayout; gather: the
+// Green-function kernels write G column-major and launch_gather forms the operands
+struct ChiView {
+  int dimens = 0;
+  int64_t ld = 0;                     // operand slots per point
+  bool gather = false;
+  const int *outmap = nullptr, *decode = nullptr, *norb = nullptr, *pair_M = nullptr, *pair_aoff = nullptr;
+  const int64_t* pair_coff = nullptr;
+  const PairTile* tiles = nullptr;
+  int ntiles = 0;
+  const SplitLayout* split = nullptr;
+  const SplitGroup *sgA = nullptr, *sgB = nullptr;
+  const SplitTile* stiles = nullptr;
+};
+
 }  // namespace
 
 struct tg_ctx {
@@ -133,6 +166,10 @@ struct tg_ctx {
   // disturbance response (eintshe)
   DevArray<int> d_she_tab, d_ia, d_she_ztiles, d_she_rowoff;
   DevArray<double2> d_she_part, d_she_sum, d_she_pref, d_she_out;
+  // chi0 over a subset of orbitals (tg_set_chi_orbitals)
+  bool chi_sel_on = false;
+  ChiLayout chi_sel;
+  DevArray<double2> d_graw;   // column-major G of a pass (gathered chi0 operands)
   // tg_expectation_noalloc: device address of the library's fixed scratch array on this
   // context's device (looked up by the context's first no-alloc call)
   double2* noalloc_ptr = nullptr;
@@ -227,6 +264,18 @@ GreenArgs base_args(tg_ctx* c) {
   a.outmap = c->d_outmap.p;
   a.status = c->d_status.p;
   return a;
+}
+
+// entry points whose Green functions are reduced inside the single-SM kernels' output
+// stages: the dimension must have one of those kernels
+int require_native(tg_ctx* c, const char* who) {
+  if (green_supported(c->dimH)) return TG_OK;
+  char b[256];
+  snprintf(b, sizeof b,
+           "%s: dimH = %d has no single-SM Gauss-Jordan kernel (dimensions 4, 8, 16, 18, 20, 36, 40, 54, 72, 90); "
+           "larger systems are served by tg_chi0, tg_chi0_batch, tg_green_batch, tg_hamiltk_batch and tg_dyson",
+           who, c->dimH);
+  return set_err(c, TG_ERR_ARG, b);
 }
 
 int check_ready(tg_ctx* c, bool need_imag, bool need_real) {
@@ -326,12 +375,108 @@ int read_eig_status(tg_ctx* c) {
 // H(k) tables and eigendecompositions are those of the imaginary axis
 bool real_k_is_imag_k(tg_ctx* c) { return c->imag_uniform && c->real_set && c->h_rkp == c->h_klist_u; }
 
+// the chi0 layout in use: the selected orbitals, or every orbital (gathered when the fused
+// Green-function kernels have no operand output stage for this dimension)
+ChiView full_view(tg_ctx* c);
+
+ChiView chi_view(tg_ctx* c) {
+  if (!c->chi_sel_on) return full_view(c);
+  ChiLayout& L = c->chi_sel;
+  ChiView v;
+  v.dimens = L.dimens;
+  v.ld = (int64_t)L.nsel * L.nsel;
+  v.gather = true;
+  v.outmap = L.d_outmap.p; v.decode = L.d_decode.p; v.norb = L.d_norb.p;
+  v.pair_M = L.d_pair_M.p; v.pair_aoff = L.d_pair_aoff.p; v.pair_coff = L.d_pair_coff.p;
+  v.tiles = L.d_tiles.p; v.ntiles = (int)L.tiles.size(); v.split = &L.split;
+  v.sgA = L.d_sgA.p; v.sgB = L.d_sgB.p; v.stiles = L.d_stiles.p;
+  return v;
+}
+
+// ChiLayout of the orbitals orbs[i] (ascending local indices) of every site i
+int build_chi_layout(tg_ctx* c, const std::vector<std::vector<int>>& orbs, ChiLayout& L) {
+  const int nat = c->n_atoms, n = c->dimH, np2 = nat * nat;
+  L.nc.assign(nat, 0);
+  int dens = 0, nsel = 0;
+  for (int i = 0; i < nat; ++i) {
+    L.nc[i] = (int)orbs[i].size();
+    dens += L.nc[i] * L.nc[i];
+    nsel += 2 * L.nc[i];
+  }
+  L.dimens = 4 * dens;
+  L.nsel = nsel;
+  L.pair_M.assign(np2, 0);
+  L.pair_aoff.assign(np2, 0);
+  L.pair_coff.assign(np2, 0);
+  L.tiles.clear();
+  std::vector<int> outmap((size_t)nsel * nsel);
+  // full-G row of the x-th selected row of site i: spin block x / nc, orbital orbs[i][x % nc]
+  auto row_of = [&](int i, int x) { return c->ia[i] + (x / L.nc[i]) * c->norb[i] + orbs[i][x % L.nc[i]]; };
+  int aoff = 0;
+  int64_t coff = 0;
+  const int T = gemm64_tile();
+  for (int i = 0; i < nat; ++i)
+    for (int j = 0; j < nat; ++j) {
+      const int p = i * nat + j;
+      const int M = 4 * L.nc[i] * L.nc[j];
+      L.pair_M[p] = M;
+      L.pair_aoff[p] = aoff;
+      L.pair_coff[p] = coff;
+      const int ni2 = 2 * L.nc[i], nj2 = 2 * L.nc[j];
+      for (int x = 0; x < ni2; ++x)
+        for (int y = 0; y < nj2; ++y) outmap[aoff + x * nj2 + y] = row_of(i, x) * n + row_of(j, y);
+      for (int u0 = 0; u0 < M; u0 += T)
+        for (int v0 = 0; v0 < M; v0 += T) L.tiles.push_back(PairTile{p, u0, v0});
+      aoff += M;
+      coff += (int64_t)M * M;
+    }
+  // chi row decode over the selected orbitals (sigmaimunu2i order restricted to them)
+  std::vector<int> decode(L.dimens);
+  int kount = 0;
+  for (int i = 0; i < nat; ++i)
+    for (int mu = 0; mu < L.nc[i]; ++mu)
+      for (int nu = 0; nu < L.nc[i]; ++nu)
+        for (int sg = 0; sg < 4; ++sg) decode[kount++] = sg | (i << 2) | (mu << 12) | (nu << 18);
+  split_build_layout(np2, L.pair_M.data(), L.pair_aoff.data(), L.split);
+  cudaStream_t s = c->stream;
+  TG_CHECK(c, L.d_outmap.upload(outmap.data(), outmap.size(), s), "upload");
+  TG_CHECK(c, L.d_decode.upload(decode.data(), decode.size(), s), "upload");
+  TG_CHECK(c, L.d_norb.upload(L.nc.data(), nat, s), "upload");
+  TG_CHECK(c, L.d_pair_M.upload(L.pair_M.data(), np2, s), "upload");
+  TG_CHECK(c, L.d_pair_aoff.upload(L.pair_aoff.data(), np2, s), "upload");
+  TG_CHECK(c, L.d_pair_coff.upload(L.pair_coff.data(), np2, s), "upload");
+  TG_CHECK(c, L.d_tiles.upload(L.tiles.data(), L.tiles.size(), s), "upload");
+  TG_CHECK(c, L.d_sgA.upload(L.split.groupsA.data(), L.split.groupsA.size(), s), "upload");
+  TG_CHECK(c, L.d_sgB.upload(L.split.groupsB.data(), L.split.groupsB.size(), s), "upload");
+  TG_CHECK(c, L.d_stiles.upload(L.split.tiles.data(), L.split.tiles.size(), s), "upload");
+  TG_CHECK(c, cudaStreamSynchronize(s), "sync");
+  return TG_OK;
+}
+
+// every orbital, in the layout of tg_set_system
+ChiView full_view(tg_ctx* c) {
+  ChiView v;
+  v.dimens = c->dimens;
+  v.ld = (int64_t)c->dimH * c->dimH;
+  v.gather = !green_supported(c->dimH);
+  v.outmap = c->d_outmap.p; v.decode = c->d_decode.p; v.norb = c->d_norb.p;
+  v.pair_M = c->d_pair_M.p; v.pair_aoff = c->d_pair_aoff.p; v.pair_coff = c->d_pair_coff.p;
+  v.tiles = c->d_tiles.p; v.ntiles = (int)c->tiles.size(); v.split = &c->split;
+  v.sgA = c->d_sgA.p; v.sgB = c->d_sgB.p; v.stiles = c->d_stiles.p;
+  return v;
+}
+
+int nsplit_view(tg_ctx* c, const ChiView& v) {
+  int s = std::max(1, c->num_sms / std::max(v.ntiles, 1));
+  return std::min(s, 64);
+}
+
 // contraction of one pass into Cpart on the FP64 SIMT path
-int contract(tg_ctx* c, const double2* A, const double2* B, int64_t np, double2* Cpart, int nsplit,
+int contract(tg_ctx* c, const ChiView& v, const double2* A, const double2* B, int64_t np, double2* Cpart, int nsplit,
              int64_t cstride) {
   c->launches += 1;
-  TG_CHECK(c, launch_gemm64(A, B, (int64_t)c->dimH * c->dimH, np, nsplit, c->d_tiles.p, (int)c->tiles.size(),
-                            c->d_pair_M.p, c->d_pair_aoff.p, c->d_pair_coff.p, Cpart, cstride, c->stream),
+  TG_CHECK(c, launch_gemm64(A, B, v.ld, np, nsplit, v.tiles, v.ntiles, v.pair_M, v.pair_aoff, v.pair_coff, Cpart,
+                            cstride, c->stream),
            "contraction (fp64)");
   return TG_OK;
 }
@@ -384,7 +529,7 @@ SplitChunks make_chunks_kmajor(int64_t p0, int64_t np, int64_t ne) {
 }
 
 // uploads the chunk tables and sizes the digit / exponent buffers of a pass
-int split_prepare(tg_ctx* c, const SplitChunks& ch, SplitPassDev& pd) {
+int split_prepare(tg_ctx* c, const ChiView& v, const SplitChunks& ch, SplitPassDev& pd) {
   const int nc = ch.n_chunks(), nks = ch.n_ksteps();
   std::vector<int> buf;
   buf.reserve(3 * nc + 1 + nks);
@@ -400,9 +545,9 @@ int split_prepare(tg_ctx* c, const SplitChunks& ch, SplitPassDev& pd) {
   pd.count = c->d_chunks.p + nc;
   pd.kstart = c->d_chunks.p + 2 * nc;
   pd.kchunk = c->d_chunks.p + 3 * nc + 1;
-  const size_t ld = (size_t)c->dimH * c->dimH;
-  TG_CHECK(c, c->d_digA.ensure((size_t)nks * c->split.groupsA.size() * kSplitABlock), "alloc digits A");
-  TG_CHECK(c, c->d_digB.ensure((size_t)nks * c->split.groupsB.size() * kSplitBBlock), "alloc digits B");
+  const size_t ld = (size_t)v.ld;
+  TG_CHECK(c, c->d_digA.ensure((size_t)nks * v.split->groupsA.size() * kSplitABlock), "alloc digits A");
+  TG_CHECK(c, c->d_digB.ensure((size_t)nks * v.split->groupsB.size() * kSplitBBlock), "alloc digits B");
   TG_CHECK(c, c->d_m64A.ensure((size_t)nc * ld), "alloc");
   TG_CHECK(c, c->d_m64B.ensure((size_t)nc * ld), "alloc");
   TG_CHECK(c, c->d_EA.ensure((size_t)nc * ld), "alloc");
@@ -412,8 +557,9 @@ int split_prepare(tg_ctx* c, const SplitChunks& ch, SplitPassDev& pd) {
 
 // FP64 operand of a pass -> digits (which = 0: A, 1: B)
 // (e16: the operand's exponent sidecar when its Green functions wrote one, else null)
-int split_quantize_operand(tg_ctx* c, int which, const double2* X, const SplitPassDev& pd, const int16_t* e16) {
-  const int64_t ld = (int64_t)c->dimH * c->dimH;
+int split_quantize_operand(tg_ctx* c, const ChiView& v, int which, const double2* X, const SplitPassDev& pd,
+                           const int16_t* e16) {
+  const int64_t ld = v.ld;
   unsigned long long* m64 = which ? c->d_m64B.p : c->d_m64A.p;
   TG_CHECK(c, cudaMemsetAsync(m64, 0, sizeof(unsigned long long) * pd.n_chunks * ld, c->stream), "memset");
   if (e16)
@@ -421,39 +567,59 @@ int split_quantize_operand(tg_ctx* c, int which, const double2* X, const SplitPa
   else
     TG_CHECK(c, split_rowmax(X, ld, pd, m64, c->stream), "split rowmax");
   if (which == 0)
-    TG_CHECK(c, split_quantize(X, ld, pd, c->d_sgA.p, (int)c->split.groupsA.size(), kSplitRowsA, m64, c->d_EA.p,
+    TG_CHECK(c, split_quantize(X, ld, pd, v.sgA, (int)v.split->groupsA.size(), kSplitRowsA, m64, c->d_EA.p,
                                c->d_digA.p, c->stream),
              "split quantize A");
   else
-    TG_CHECK(c, split_quantize(X, ld, pd, c->d_sgB.p, (int)c->split.groupsB.size(), kSplitColsB, m64, c->d_EB.p,
+    TG_CHECK(c, split_quantize(X, ld, pd, v.sgB, (int)v.split->groupsB.size(), kSplitColsB, m64, c->d_EB.p,
                                c->d_digB.p, c->stream),
              "split quantize B");
   c->launches += 2;
   return TG_OK;
 }
 
-int split_contract_pass(tg_ctx* c, const SplitPassDev& pd, double2* Cpart, int nsplit, int64_t cstride) {
+int split_contract_pass(tg_ctx* c, const ChiView& v, const SplitPassDev& pd, double2* Cpart, int nsplit,
+                        int64_t cstride) {
   SplitContractArgs sa;
   sa.A = c->d_digA.p;
   sa.B = c->d_digB.p;
-  sa.GA = (int)c->split.groupsA.size();
-  sa.GB = (int)c->split.groupsB.size();
-  sa.tiles = c->d_stiles.p;
-  sa.ntiles = (int)c->split.tiles.size();
+  sa.GA = (int)v.split->groupsA.size();
+  sa.GB = (int)v.split->groupsB.size();
+  sa.tiles = v.stiles;
+  sa.ntiles = (int)v.split->tiles.size();
   sa.nsplit = nsplit;
   sa.pass = pd;
   sa.EA = c->d_EA.p;
   sa.EB = c->d_EB.p;
-  sa.ld = (int64_t)c->dimH * c->dimH;
-  sa.pair_M = c->d_pair_M.p;
-  sa.pair_aoff = c->d_pair_aoff.p;
-  sa.pair_coff = c->d_pair_coff.p;
+  sa.ld = v.ld;
+  sa.pair_M = v.pair_M;
+  sa.pair_aoff = v.pair_aoff;
+  sa.pair_coff = v.pair_coff;
   sa.C = Cpart;
   sa.cstride = cstride;
   sa.err = c->d_split_err.p;
   sa.num_ctas = c->num_sms;
   c->launches += 1;
   TG_CHECK(c, split_contract(sa, c->stream), "contraction (split)");
+  return TG_OK;
+}
+
+// Green functions of a chi0 pass into the operand buffers: fused (the kernel writes the
+// operand layouts), or gathered (column-major G into d_graw, then the view's slots)
+int chi_green(tg_ctx* c, const ChiView& v, const GreenArgs& g, const char* what) {
+  if (!v.gather) {
+    TG_CHECK(c, launch_green(g, c->num_sms, c->stream, nullptr), what);
+    return TG_OK;
+  }
+  GreenArgs r = g;
+  r.mode = MODE_RAW;
+  r.out = c->d_graw.p;
+  r.out2 = nullptr;
+  r.eout = r.eout2 = nullptr;
+  TG_CHECK(c, launch_green(r, c->num_sms, c->stream, nullptr), what);
+  TG_CHECK(c, launch_gather(g, c->d_graw.p, g.mode, v.outmap, v.ld, g.out, c->num_sms, c->stream), what);
+  if (g.out2) TG_CHECK(c, launch_gather(g, c->d_graw.p, g.mode2, v.outmap, v.ld, g.out2, c->num_sms, c->stream), what);
+  c->launches += g.out2 ? 2 : 1;
   return TG_OK;
 }
 
@@ -546,11 +712,12 @@ int tg_set_system(tg_ctx* c, int n_atoms, const int* norb, int norb_max, int n_n
   }
   c->dimH = pos;
   c->dimens = 4 * dens;
-  if (!green_supported(c->dimH)) {
+  if (!green_supported(c->dimH) && !green_cluster_supported(c->dimH, MODE_RAW)) {
     char b[128];
-    snprintf(b, sizeof b, "dimH = %d has no Gauss-Jordan tile configuration", c->dimH);
+    snprintf(b, sizeof b, "dimH = %d is beyond the largest supported dimension (288)", c->dimH);
     return set_err(c, TG_ERR_ARG, b);
   }
+  c->chi_sel_on = false;
   const int n = c->dimH;
   // row tables
   std::vector<int> ratom(n), rorb(n), rspin(n);
@@ -722,12 +889,37 @@ int tg_set_real_mesh(tg_ctx* c, int64_t n_k, const double* kp, const double* w) 
   return TG_OK;
 }
 
+int tg_set_chi_orbitals(tg_ctx* c, const int* mask) {
+  if (!c) return TG_ERR_ARG;
+  if (!c->sys_set) return set_err(c, TG_ERR_STATE, "tg_set_system has not been called");
+  cudaSetDevice(c->device);
+  if (!mask) {
+    c->chi_sel_on = false;
+    return TG_OK;
+  }
+  std::vector<std::vector<int>> orbs(c->n_atoms);
+  int total = 0;
+  for (int i = 0; i < c->n_atoms; ++i)
+    for (int mu = 0; mu < c->norb[i]; ++mu)
+      if (mask[(size_t)i * c->nmax + mu]) {
+        orbs[i].push_back(mu);
+        ++total;
+      }
+  if (total == 0) return set_err(c, TG_ERR_ARG, "tg_set_chi_orbitals: no orbital selected");
+  c->chi_sel_on = false;
+  int rc = build_chi_layout(c, orbs, c->chi_sel);
+  if (rc) return rc;
+  c->chi_sel_on = true;
+  return TG_OK;
+}
+
 int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, double Ef, double eta, double etap,
                   int n_real, const double* x2, const double* p2, int precision, int dimens, double* chiorb_hf) {
   int rc = check_ready(c, true, false);
   if (rc) return rc;
   if (!q || !e || n_omega <= 0 || !chiorb_hf) return set_err(c, TG_ERR_ARG, "tg_chi0: null argument");
-  if (dimens != c->dimens) return set_err(c, TG_ERR_ARG, "tg_chi0: dimens mismatch");
+  const ChiView v = chi_view(c);
+  if (dimens != v.dimens) return set_err(c, TG_ERR_ARG, "tg_chi0: dimens mismatch (see tg_set_chi_orbitals)");
   if (precision != TG_PREC_FP64 && precision != TG_PREC_SPLIT) return set_err(c, TG_ERR_ARG, "tg_chi0: precision");
   bool any_real = false;
   for (int w = 0; w < n_omega; ++w) any_real |= std::fabs(e[w]) >= 1e-15;
@@ -738,21 +930,22 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   const int n = c->dimH;
   const int64_t nn = (int64_t)n * n;
   const bool split = precision == TG_PREC_SPLIT;
-  const int64_t cstride = (int64_t)c->dimens * c->dimens;
+  const int64_t cstride = (int64_t)v.dimens * v.dimens;
   // workspace
   // 6 GiB operands (about 25 GB with the digit planes and tables at dimH = 36): a k-major
   // pass over a tabulated mesh then holds ~2400 points per energy, so the split
   // contraction's chunk ends (one per energy and pass) cost little
   const int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, (int64_t)n_real * c->n_realk), (int64_t)6 << 30);
-  const int nsplit = split ? split_nsplit((int)c->split.tiles.size(), c->num_sms, P / kSplitK) : nsplit_for(c);
+  const int nsplit = split ? split_nsplit((int)v.split->tiles.size(), c->num_sms, P / kSplitK) : nsplit_view(c, v);
   if (split) {
     TG_CHECK(c, c->d_split_err.ensure(1), "alloc");
     TG_CHECK(c, c->d_e16A.ensure((size_t)P * nn), "alloc exponents A");
     TG_CHECK(c, c->d_e16B.ensure((size_t)P * nn), "alloc exponents B");
     TG_CHECK(c, cudaMemsetAsync(c->d_split_err.p, 0, sizeof(int), s), "memset");
   }
-  TG_CHECK(c, c->d_A.ensure((size_t)P * nn), "alloc A");
-  TG_CHECK(c, c->d_B.ensure((size_t)P * nn), "alloc B");
+  TG_CHECK(c, c->d_A.ensure((size_t)P * v.ld), "alloc A");
+  TG_CHECK(c, c->d_B.ensure((size_t)P * v.ld), "alloc B");
+  if (v.gather) TG_CHECK(c, c->d_graw.ensure((size_t)P * nn), "alloc G");
   TG_CHECK(c, c->d_C.ensure((size_t)n_omega * nsplit * cstride), "alloc C");
   TG_CHECK(c, c->d_D.ensure((size_t)n_omega * nsplit * cstride), "alloc D");
   TG_CHECK(c, c->d_chi.ensure((size_t)cstride), "alloc chi");
@@ -824,7 +1017,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       w_start = 1;
     }
     // the split row maxima read exponent sidecars when the spectral kernel writes G
-    const bool e16_g2 = split && green_is_spectral(g2);
+    const bool e16_g2 = split && !v.gather && green_is_spectral(g2);
     if (e16_g2) {
       g2.eout = c->d_e16B.p;
       if (g2.out2) g2.eout2 = c->d_e16A.p;
@@ -832,7 +1025,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     cudaEventRecord(ev[1], s);
     {
       KindTimer kt(c, 0);
-      TG_CHECK(c, launch_green(g2, c->num_sms, s, nullptr), "green (imag, G2)");
+      if ((rc = chi_green(c, v, g2, "green (imag, G2)"))) return rc;
     }
     cudaEventRecord(ev[2], s);
     float ms = 0;
@@ -842,20 +1035,20 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       const double* yv = c->h_y.data() + p0;
       const SplitChunks ch = tab_imag ? make_chunks_kmajor(p0, np, c->n_e_u)
                                       : make_chunks(np, [&](int64_t i) { return yv[i]; });
-      if ((rc = split_prepare(c, ch, pd))) return rc;
-      if ((rc = split_quantize_operand(c, 1, c->d_B.p, pd, e16_g2 ? c->d_e16B.p : nullptr))) return rc;
+      if ((rc = split_prepare(c, v, ch, pd))) return rc;
+      if ((rc = split_quantize_operand(c, v, 1, c->d_B.p, pd, e16_g2 ? c->d_e16B.p : nullptr))) return rc;
     }
     if (w_start == 1) {
       if (split) {
         {
           KindTimer kq(c, 3);
-          if ((rc = split_quantize_operand(c, 0, c->d_A.p, pd, e16_g2 ? c->d_e16A.p : nullptr))) return rc;
+          if ((rc = split_quantize_operand(c, v, 0, c->d_A.p, pd, e16_g2 ? c->d_e16A.p : nullptr))) return rc;
         }
         KindTimer kt(c, 1);
-        rc = split_contract_pass(c, pd, c->d_C.p, nsplit, cstride);
+        rc = split_contract_pass(c, v, pd, c->d_C.p, nsplit, cstride);
       } else {
         KindTimer kt(c, 1);
-        rc = contract(c, c->d_A.p, c->d_B.p, np, c->d_C.p, nsplit, cstride);
+        rc = contract(c, v, c->d_A.p, c->d_B.p, np, c->d_C.p, nsplit, cstride);
       }
       if (rc) return rc;
     }
@@ -872,24 +1065,24 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
         use_table(g1, q_zero ? 0 : 1, c->n_e_u, c->nk_u, c->d_ylist.p);
         g1.q[0] = g1.q[1] = g1.q[2] = 0.0;   // q is inside the table
       }
-      const bool e16_g1 = split && green_is_spectral(g1);
+      const bool e16_g1 = split && !v.gather && green_is_spectral(g1);
       if (e16_g1) g1.eout = c->d_e16A.p;
       {
         KindTimer kt(c, 0);
-        TG_CHECK(c, launch_green(g1, c->num_sms, s, nullptr), "green (imag, G1)");
+        if ((rc = chi_green(c, v, g1, "green (imag, G1)"))) return rc;
       }
       {
         double2* Cw = c->d_C.p + (size_t)w * nsplit * cstride;
         if (split) {
           {
             KindTimer kq(c, 3);
-            rc = split_quantize_operand(c, 0, c->d_A.p, pd, e16_g1 ? c->d_e16A.p : nullptr);
+            rc = split_quantize_operand(c, v, 0, c->d_A.p, pd, e16_g1 ? c->d_e16A.p : nullptr);
           }
           KindTimer kt(c, 1);
-          if (!rc) rc = split_contract_pass(c, pd, Cw, nsplit, cstride);
+          if (!rc) rc = split_contract_pass(c, v, pd, Cw, nsplit, cstride);
         } else {
           KindTimer kt(c, 1);
-          rc = contract(c, c->d_A.p, c->d_B.p, np, Cw, nsplit, cstride);
+          rc = contract(c, v, c->d_A.p, c->d_B.p, np, Cw, nsplit, cstride);
         }
       }
       if (rc) return rc;
@@ -925,11 +1118,11 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       gr.mode = MODE_B_REAL;
       gr.out = c->d_B.p;
       if (tab_real) use_table(gr, rslot0, n_real, c->n_realk, nullptr);
-      const bool e16_rb = split && green_is_spectral(gr);
+      const bool e16_rb = split && !v.gather && green_is_spectral(gr);
       gr.eout = e16_rb ? c->d_e16B.p : nullptr;
       {
         KindTimer kt(c, 0);
-        TG_CHECK(c, launch_green(gr, c->num_sms, s, nullptr), "green (real, G2)");
+        if ((rc = chi_green(c, v, gr, "green (real, G2)"))) return rc;
       }
       // G1 = G(k + q, x2 + e + i eta) -> w (G1 - G1^dagger)
       gr.zr = e[w];
@@ -941,11 +1134,11 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
         use_table(gr, q_zero ? rslot0 : rslot1, n_real, c->n_realk, nullptr);
         gr.q[0] = gr.q[1] = gr.q[2] = 0.0;
       }
-      const bool e16_ra = split && green_is_spectral(gr);
+      const bool e16_ra = split && !v.gather && green_is_spectral(gr);
       gr.eout = e16_ra ? c->d_e16A.p : nullptr;
       {
         KindTimer kt(c, 0);
-        TG_CHECK(c, launch_green(gr, c->num_sms, s, nullptr), "green (real, G1)");
+        if ((rc = chi_green(c, v, gr, "green (real, G1)"))) return rc;
       }
       {
         double2* Dw = c->d_D.p + (size_t)w * nsplit * cstride;
@@ -956,15 +1149,15 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
             KindTimer kq(c, 3);
             const SplitChunks ch = tab_real ? make_chunks_kmajor(pbase, np, n_real)
                                             : make_chunks(np, [&](int64_t i) { return (pbase + i) / nrk; });
-            rc = split_prepare(c, ch, pr);
-            if (!rc) rc = split_quantize_operand(c, 1, c->d_B.p, pr, e16_rb ? c->d_e16B.p : nullptr);
-            if (!rc) rc = split_quantize_operand(c, 0, c->d_A.p, pr, e16_ra ? c->d_e16A.p : nullptr);
+            rc = split_prepare(c, v, ch, pr);
+            if (!rc) rc = split_quantize_operand(c, v, 1, c->d_B.p, pr, e16_rb ? c->d_e16B.p : nullptr);
+            if (!rc) rc = split_quantize_operand(c, v, 0, c->d_A.p, pr, e16_ra ? c->d_e16A.p : nullptr);
           }
           KindTimer kt(c, 1);
-          if (!rc) rc = split_contract_pass(c, pr, Dw, nsplit, cstride);
+          if (!rc) rc = split_contract_pass(c, v, pr, Dw, nsplit, cstride);
         } else {
           KindTimer kt(c, 1);
-          rc = contract(c, c->d_A.p, c->d_B.p, np, Dw, nsplit, cstride);
+          rc = contract(c, v, c->d_A.p, c->d_B.p, np, Dw, nsplit, cstride);
         }
       }
       if (rc) return rc;
@@ -975,7 +1168,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   for (int w = 0; w < n_omega; ++w) {
     KindTimer kt(c, 2);
     TG_CHECK(c, launch_chi_epilogue(c->d_C.p + (size_t)w * nsplit * cstride, c->d_D.p + (size_t)w * nsplit * cstride,
-                                    nsplit, cstride, c->dimens, c->d_decode.p, c->d_norb.p, c->d_pair_coff.p,
+                                    nsplit, cstride, v.dimens, v.decode, v.norb, v.pair_coff,
                                     c->n_atoms, 1.0 / (2.0 * kPi), c->d_chi.p, s),
              "epilogue");
     TG_CHECK(c, cudaMemcpyAsync(chiorb_hf + 2 * (size_t)w * cstride, c->d_chi.p, sizeof(double2) * cstride,
@@ -1036,6 +1229,7 @@ int tg_profile(tg_ctx* c, int enable) {
 int tg_expectation(tg_ctx* c, double Ef, double eta, double* rho, double* mx, double* my, double* mz, double* mp) {
   int rc = check_ready(c, true, false);
   if (rc) return rc;
+  if ((rc = require_native(c, "tg_expectation"))) return rc;
   if (!rho || !mx || !my || !mz || !mp) return set_err(c, TG_ERR_ARG, "tg_expectation: null output");
   cudaSetDevice(c->device);
   cudaStream_t s = c->stream;
@@ -1115,6 +1309,7 @@ int tg_expectation(tg_ctx* c, double Ef, double eta, double* rho, double* mx, do
 int tg_gg_tensor(tg_ctx* c, double Ef, double eta, int orbital_resolved, const int* dmask, double* T) {
   int rc = check_ready(c, true, false);
   if (rc) return rc;
+  if ((rc = require_native(c, "tg_gg_tensor"))) return rc;
   if (!T || (orbital_resolved && !dmask)) return set_err(c, TG_ERR_ARG, "tg_gg_tensor: null argument");
   cudaSetDevice(c->device);
   cudaStream_t s = c->stream;
@@ -1225,6 +1420,7 @@ int tg_gg_tensor(tg_ctx* c, double Ef, double eta, int orbital_resolved, const i
 int tg_fermi_column(tg_ctx* c, double Ef, double eta, double* D) {
   int rc = check_ready(c, false, true);
   if (rc) return rc;
+  if ((rc = require_native(c, "tg_fermi_column"))) return rc;
   if (!D) return set_err(c, TG_ERR_ARG, "tg_fermi_column: null output");
   cudaSetDevice(c->device);
   cudaStream_t s = c->stream;
@@ -1333,9 +1529,29 @@ int tg_hamiltk_batch(tg_ctx* c, int64_t nk, const double* kp, double* H) {
   a.np = nk;
   a.mode = MODE_HK;
   a.out = c->d_gout.p;
-  TG_CHECK(c, launch_green(a, c->num_sms, s, nullptr), "hamiltk");
-  TG_CHECK(c, cudaMemcpyAsync(H, c->d_gout.p, sizeof(double2) * nk * nn, cudaMemcpyDeviceToHost, s), "copy H");
+  if (green_supported(c->dimH)) {
+    TG_CHECK(c, launch_green(a, c->num_sms, s, nullptr), "hamiltk");
+    TG_CHECK(c, cudaMemcpyAsync(H, c->d_gout.p, sizeof(double2) * nk * nn, cudaMemcpyDeviceToHost, s), "copy H");
+    TG_CHECK(c, cudaStreamSynchronize(s), "sync");
+    return TG_OK;
+  }
+  // other dimensions: the row-major H(k) table, transposed to Fortran order on the host
+  const double zero3[3] = {0.0, 0.0, 0.0};
+  TG_CHECK(c, c->d_hphase.ensure((size_t)nk * std::max(c->n_neigh, 1)), "alloc phases");
+  TG_CHECK(c, c->d_qvec.upload(zero3, 3, s), "upload q");
+  TG_CHECK(c, launch_hk_table(a, c->d_klist.p, nk, c->d_qvec.p, c->d_hphase.p, c->d_gout.p, s), "H table");
+  std::vector<double2> tab((size_t)nk * nn);
+  TG_CHECK(c, cudaMemcpyAsync(tab.data(), c->d_gout.p, sizeof(double2) * nk * nn, cudaMemcpyDeviceToHost, s),
+           "copy H");
   TG_CHECK(c, cudaStreamSynchronize(s), "sync");
+  const int n = c->dimH;
+  for (int64_t k = 0; k < nk; ++k)
+    for (int r = 0; r < n; ++r)
+      for (int cc = 0; cc < n; ++cc) {
+        const double2 v = tab[(size_t)k * nn + (size_t)r * n + cc];
+        H[2 * ((size_t)k * nn + (size_t)cc * n + r)] = v.x;
+        H[2 * ((size_t)k * nn + (size_t)cc * n + r) + 1] = v.y;
+      }
   return TG_OK;
 }
 
@@ -1350,6 +1566,7 @@ int tg_set_green_method(tg_ctx* c, int method) {
 int tg_eig_batch(tg_ctx* c, int64_t nk, const double* kp, double* lam, double* U) {
   int rc = check_ready(c, false, false);
   if (rc) return rc;
+  if ((rc = require_native(c, "tg_eig_batch"))) return rc;
   if (nk < 0 || (nk > 0 && (!kp || !lam || !U))) return set_err(c, TG_ERR_ARG, "tg_eig_batch: bad args");
   if (nk == 0) return TG_OK;
   if (!eig_supported(c->dimH)) return set_err(c, TG_ERR_ARG, "tg_eig_batch: dimH too large for the Jacobi kernel");
@@ -1371,6 +1588,7 @@ int tg_chi0_linear_soc(tg_ctx* c, const double* q, double e, double Ef, double e
                        double* chiorb_lsoc) {
   int rc = check_ready(c, true, false);
   if (rc) return rc;
+  if ((rc = require_native(c, "tg_chi0_linear_soc"))) return rc;
   if (!q || !vsoc || !chiorb_hf || !chiorb_lsoc) return set_err(c, TG_ERR_ARG, "tg_chi0_linear_soc: null argument");
   if (dimens != c->dimens) return set_err(c, TG_ERR_ARG, "tg_chi0_linear_soc: dimens mismatch");
   const bool real = std::fabs(e) >= 1e-15;
@@ -1388,6 +1606,7 @@ int tg_chi0_linear_soc(tg_ctx* c, const double* q, double e, double Ef, double e
   }
   const int64_t cstride = (int64_t)c->dimens * c->dimens;
   const int nsplit = nsplit_for(c);
+  const ChiView fv = full_view(c);
   // eight P x dimH^2 buffers per pass: P a quarter of the chi0 pass
   int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, real ? (int64_t)n_real * c->n_realk : 0)) / 4;
   P = std::max<int64_t>(64, (P / 64) * 64);
@@ -1436,9 +1655,9 @@ int tg_chi0_linear_soc(tg_ctx* c, const double* q, double e, double Ef, double e
     TG_CHECK(c, launch_operand(X1, n, g.np, g.p0, g.pts, ma, c->d_outmap.p, oAx, c->num_sms, s), "operand");
     TG_CHECK(c, launch_operand(X2, n, g.np, g.p0, g.pts, mb, c->d_outmap.p, oBx, c->num_sms, s), "operand");
     KindTimer kt(c, 1);
-    if ((rc = contract(c, oA, oB, g.np, C, nsplit, cstride))) return rc;
-    if ((rc = contract(c, oAx, oB, g.np, Cl, nsplit, cstride))) return rc;
-    return contract(c, oA, oBx, g.np, Cl, nsplit, cstride);
+    if ((rc = contract(c, fv, oA, oB, g.np, C, nsplit, cstride))) return rc;
+    if ((rc = contract(c, fv, oAx, oB, g.np, Cl, nsplit, cstride))) return rc;
+    return contract(c, fv, oA, oBx, g.np, Cl, nsplit, cstride);
   };
   const GreenArgs base = base_args(c);
   for (int64_t p0 = 0; p0 < c->n_imag; p0 += P) {
@@ -1489,6 +1708,7 @@ int tg_jij(tg_ctx* c, const double* q, double Ef, double eta, const double* evec
            double* J) {
   int rc = check_ready(c, true, false);
   if (rc) return rc;
+  if ((rc = require_native(c, "tg_jij"))) return rc;
   if (!q || !evec || !Um || !dmask || !J) return set_err(c, TG_ERR_ARG, "tg_jij: null argument");
   cudaSetDevice(c->device);
   cudaStream_t s = c->stream;
@@ -1600,6 +1820,7 @@ int tg_jij(tg_ctx* c, const double* q, double Ef, double eta, const double* evec
 int tg_smunu(tg_ctx* c, double Ef, double eta, double* S) {
   int rc = check_ready(c, true, false);
   if (rc) return rc;
+  if ((rc = require_native(c, "tg_smunu"))) return rc;
   if (!S) return set_err(c, TG_ERR_ARG, "tg_smunu: null output");
   if (!green_supported(c->dimH)) return set_err(c, TG_ERR_ARG, "tg_smunu: dimH has no accumulating kernel");
   cudaSetDevice(c->device);
@@ -1674,6 +1895,7 @@ int tg_smunu(tg_ctx* c, double Ef, double eta, double* S) {
 int tg_ldos(tg_ctx* c, int n_e, const double* e, double eta, double* ldosu, double* ldosd) {
   int rc = check_ready(c, false, true);
   if (rc) return rc;
+  if ((rc = require_native(c, "tg_ldos"))) return rc;
   if (n_e < 0 || (n_e > 0 && (!e || !ldosu || !ldosd))) return set_err(c, TG_ERR_ARG, "tg_ldos: bad args");
   if (n_e == 0) return TG_OK;
   cudaSetDevice(c->device);
@@ -1791,6 +2013,7 @@ extern "C" int tg_she(tg_ctx* c, const double* q, double e, double Ef, double et
                       double* tchi) {
   int rc = check_ready(c, true, false);
   if (rc) return rc;
+  if ((rc = require_native(c, "tg_she"))) return rc;
   if (!q || !efield || !tchi) return set_err(c, TG_ERR_ARG, "tg_she: null argument");
   if (dimens != c->dimens) return set_err(c, TG_ERR_ARG, "tg_she: dimens mismatch");
   const bool real = std::fabs(e) >= 1e-15;

@@ -518,7 +518,11 @@ cudaError_t launch_green(const GreenArgs& a, int num_sms, cudaStream_t s, int* g
   if (green_w1_supported(a.n, a.mode)) return launch_green_w1(a, num_sms, s, grid_used);
   if (green_warp_supported(a.n, a.mode)) return launch_green_warp(a, num_sms, s, grid_used);
   const Cfg* c = find_cfg(a.n);
-  if (!c) return cudaErrorInvalidValue;
+  if (!c) {
+    if (grid_used) *grid_used = 0;
+    if (green_cluster_supported(a.n, a.mode)) return launch_green_cluster(a, num_sms, s);
+    return cudaErrorInvalidValue;
+  }
   if (a.np <= 0) {
     if (grid_used) *grid_used = 0;
     return cudaSuccess;

@@ -163,6 +163,10 @@ cudaError_t launch_green_warp(const GreenArgs& a, int num_sms, cudaStream_t s, i
 int green_w1_supported(int n, int mode);
 cudaError_t launch_green_w1(const GreenArgs& a, int num_sms, cudaStream_t s, int* grid_used);
 int green_acc_ctas(int n, int64_t np, int num_sms);
+// any dimension up to 288, MODE_RAW only: one thread-block cluster per matrix
+int green_cluster_supported(int n, int mode);
+int green_cluster_size(int n);
+cudaError_t launch_green_cluster(const GreenArgs& a, int num_sms, cudaStream_t s);
 
 // FP64 pair-block contraction: Cpart[split][cpair_off + u*M + v] += sum_p A[p][off+u] B[p][off+v]
 struct PairTile { int pair; int u0; int v0; };
@@ -203,6 +207,10 @@ cudaError_t launch_gvg(const double2* G, const double2* V, int n, int64_t np, do
                        cudaStream_t s);
 cudaError_t launch_operand(const double2* G, int n, int64_t np, int64_t p0, const PointSet& pts, int mode,
                            const int* outmap, double2* out, int num_sms, cudaStream_t s);
+// operand of a Green-function launch g from its column-major G (MODE_RAW output of g):
+// ld slots per point, outmap[o] = r * n + c (an orbital subset in pair-block order)
+cudaError_t launch_gather(const GreenArgs& g, const double2* G, int mode, const int* outmap, int64_t ld, double2* out,
+                          int num_sms, cudaStream_t s);
 
 // Exchange coupling: d-orbital GG tensors T(G(k), G(k - q)) and T(G(k - q), G(k)) per site pair
 cudaError_t launch_jij(const double2* Ga, const double2* Gb, int64_t p0, int64_t np, const double* w, int n,

@@ -90,7 +90,62 @@ __global__ void operand_kernel(const double2* __restrict__ G, int n, int64_t np,
   }
 }
 
+// out[p][o] = transform of the column-major G_p (n x n) at slot o of an operand layout with
+// ld slots per point (outmap[o] = r * n + c, a subset of G's entries in pair-block order);
+// the weights follow the point traversal of the Green-function launch g (tabulated k-major
+// or the flattened list), as the fused output stages do
+__global__ void gather_kernel(GreenArgs g, const double2* __restrict__ G, int mode, const int* __restrict__ outmap,
+                              int64_t ld, double2* __restrict__ out) {
+  const int n = g.n;
+  const int64_t nn = (int64_t)n * n;
+  const int64_t total = g.np * ld;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pl = idx / ld;
+    const int o = (int)(idx - pl * ld);
+    const int rc = outmap[o];
+    const int r = rc / n, c = rc - r * n;
+    const double2* gp = G + pl * nn;
+    const int64_t wi = g.p0 + pl;
+    double w;
+    if (g.htab) {
+      const int64_t ik = wi / g.n_e, ie = wi % g.n_e;
+      w = g.pts.kind == 0 ? g.pts.w[ie * g.nk_tab + ik] : g.pts.p2[ie] * g.pts.w[ik];
+    } else if (g.pts.kind == 0) {
+      w = g.pts.w[wi];
+    } else if (g.pts.kind == 1) {
+      w = g.pts.p2[wi / g.pts.nk] * g.pts.w[wi % g.pts.nk];
+    } else {
+      w = 1.0;
+    }
+    const double2 grc = gp[(int64_t)c * n + r];
+    double2 v;
+    if (mode == MODE_A_IMAG) {
+      v = cscale(grc, w);
+    } else if (mode == MODE_B_IMAG) {
+      v = gp[(int64_t)r * n + c];   // G^T
+    } else if (mode == MODE_A_REAL) {
+      const double2 gcr = gp[(int64_t)r * n + c];
+      v = cscale(make_double2(grc.x - gcr.x, grc.y + gcr.y), w);
+    } else {
+      v = cconj(grc);
+    }
+    out[idx] = v;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_gather(const GreenArgs& g, const double2* G, int mode, const int* outmap, int64_t ld, double2* out,
+                          int num_sms, cudaStream_t s) {
+  if (g.np <= 0) return cudaSuccess;
+  if (mode != MODE_A_IMAG && mode != MODE_B_IMAG && mode != MODE_A_REAL && mode != MODE_B_REAL)
+    return cudaErrorInvalidValue;
+  const int64_t total = g.np * ld;
+  const int64_t grid = std::min<int64_t>((total + 255) / 256, (int64_t)num_sms * 16);
+  gather_kernel<<<(unsigned)grid, 256, 0, s>>>(g, G, mode, outmap, ld, out);
+  return cudaGetLastError();
+}
 
 size_t gvg_smem_bytes(int n) { return sizeof(double2) * 3 * (size_t)n * n; }
 

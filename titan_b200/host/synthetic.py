@@ -19,6 +19,7 @@ sq2        2D square monolayer, 2 atoms/cell       36   200^2 k, 128 imag + 64 r
 slab5      bcc(001) slab, 5 layers                 90   adaptive 400^2 -> 16^2
 bcc4       bcc bulk, 4 atoms/cell                  72   48^3 k, 96 imag
 slab16     bcc(001) slab, 16 layers                288  128^2 k, 128 imag + 96 real, 64 omega
+slabL      bcc(001) slab, L layers (any L >= 1)    18L  as slab5, uniform 32^2 k (test systems)
 =========  =====================================  ===  ======================
 """
 from __future__ import annotations
@@ -45,6 +46,24 @@ SHAPES = {
 }
 
 A0 = 5.30   # lattice constant (bohr), the bcc Fe value of the reference example
+
+
+def _shape(shape: str):
+    """SHAPES entry; "slabL" for any other layer count L is the bcc(001) slab of L layers
+    (seed 2000 + L)."""
+    if shape in SHAPES:
+        return SHAPES[shape]
+    if shape.startswith("slab") and shape[4:].isdigit() and int(shape[4:]) >= 1:
+        nl = int(shape[4:])
+        return (np.array([[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [0.0, 0.0, 0.0]]),
+                np.array([[0.5 * (l % 2), 0.5 * (l % 2), 0.5 * l] for l in range(nl)]), 2, 2000 + nl)
+    raise KeyError(shape)
+
+
+def _mesh_cfg(shape: str):
+    if shape in DEFAULT_MESH:
+        return DEFAULT_MESH[shape]
+    return dict(nk=(32, 32, 1), parts=2, n1gl=32, parts3=1, n3gl=32, omegas=(0.0, 0.3, 4))
 
 
 def draw_parameters(seed: int):
@@ -77,7 +96,7 @@ def make_element(name: str, a_cols: np.ndarray, positions: np.ndarray, sysdim: i
 
 
 def make_system(shape: str, seed: int | None = None, n_stages: int = 2, eta: float = 1.0e-3) -> TBSystem:
-    a, pos, sysdim, default_seed = SHAPES[shape]
+    a, pos, sysdim, default_seed = _shape(shape)
     seed = default_seed if seed is None else seed
     a1, a2, a3 = a[0] * A0, a[1] * A0, a[2] * A0
     basis = L.Basis(shape, A0, a1, a2, a3, [shape], [0] * pos.shape[0], pos * A0, sysdim)
@@ -100,7 +119,7 @@ DEFAULT_MESH = {
 def make_deck(shape: str, seed: int | None = None, nk=None, parts=None, n1gl=None, parts3=None, n3gl=None,
               mesh: bool = True) -> Deck:
     """System + meshes; keyword overrides shrink the mesh for tests."""
-    cfg = dict(DEFAULT_MESH[shape])
+    cfg = dict(_mesh_cfg(shape))
     sysm = make_system(shape, seed)
     nk = tuple(nk) if nk is not None else cfg["nk"]
     sd = sysm.sysdim

@@ -72,6 +72,7 @@ SIGNATURES = {
     "tg_adjoint_vb": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
     "tg_system_shape": (C.c_int, [C.c_void_p, _ip, _ip, _ip]),
     "tg_expectation_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp]),
+    "tg_set_chi_orbitals": (C.c_int, [C.c_void_p, _ip]),
 }
 
 
@@ -195,7 +196,21 @@ class GreenGPU:
         self.system = system
         self.dimH = system.dimH
         self.dimens = system.dimens
+        self.chi_dimens = system.dimens
         self.nmax = nmax
+
+    def set_chi_orbitals(self, sel=None):
+        """chi0 over the orbitals sel[i] (local indices) of each site, e.g. the d orbitals
+        (system.dorbs); None restores every orbital (tg_set_chi_orbitals)."""
+        if sel is None:
+            self._check(self.lib.tg_set_chi_orbitals(self.h, None))
+            self.chi_dimens = self.dimens
+            return
+        mask = np.zeros((self.system.n_atoms, self.nmax), np.int32)
+        for i, x in enumerate(sel):
+            mask[i, list(x)] = 1
+        self._check(self.lib.tg_set_chi_orbitals(self.h, _p(mask, C.c_int)))
+        self.chi_dimens = 4 * sum(len(x) ** 2 for x in sel)
 
     def set_h0(self, h0):
         hF = _fortran_complex(h0)
@@ -241,7 +256,7 @@ class GreenGPU:
                     X2[w, :len(x2s[w])] = x2s[w]
                     P2[w, :len(p2s[w])] = p2s[w]
         qa = np.ascontiguousarray(q, np.float64)
-        D = self.dimens
+        D = self.chi_dimens
         buf = out if out is not None else np.empty((nw, D, D), np.complex128)
         rc = self.lib.tg_chi0_batch(self.h, _p(qa), nw, _p(es), Ef, eta, etap, nreal, _p(X2), _p(P2),
                                     _PREC[precision], D, _p(buf.view(np.float64)))
