@@ -322,10 +322,10 @@ def run_ours(args, rank, world, local_rank):
             "launches_in_last_step": int(con_n), "avg_launch_ms": (con_ms / con_n) if con_n else None,
             "quantize_ms_last_step": q_ms if args.precision == "split" else None}
     if args.precision == "split" and con_n:
-        # what the tensor pipe executes: 19 int8 MMAs of 128 x 80 x 32 per 64 x 40 complex tile
+        # what the tensor pipe executes: 21 int8 MMAs of 128 x 80 x 32 per 64 x 40 complex tile
         # and K-step of 32 points (tiles: ceil(M/64) x ceil(M/40) per site pair, M = 4 n_i n_j)
         tiles = sum(-(-4 * a * b // 64) * -(-4 * a * b // 40) for a in s.norbs for b in s.norbs)
-        ops = tiles * (last_units / 32.0) / con_n * 19 * 2 * 128 * 80 * 32
+        ops = tiles * (last_units / 32.0) / con_n * 21 * 2 * 128 * 80 * 32
         tops = ops / (con_ms / con_n / 1e3) / 1e12
         roof["executed_int8"] = {"tops": tops, "peak_tops": 2.0 * peak, "frac": tops / (2.0 * peak),
                                  "basis": "int8 MMA ops issued per launch (K-step padding not counted) / "

@@ -84,6 +84,13 @@ int tg_chi0_batch(tg_ctx* ctx, const double* q, int n_omega, const double* e, do
                   double eta, double etap, int n_real, const double* x2, const double* p2,
                   int precision, int dimens, double* chiorb_hf);
 
+/* Points per chunk of the split-precision contraction (TG_PREC_SPLIT): each energy's
+ * points are cut into chunks of at most this many, and every operand element gets one
+ * power-of-two scale per chunk, so shorter chunks follow the magnitude of G along the k
+ * list (more accurate near the real axis) at the cost of more accumulator drains.
+ * 1 .. 16384; 0 restores the default.  No counterpart in the reference. */
+int tg_set_split_chunk(tg_ctx* ctx, int points);
+
 /* Restricts chi0 (tg_chi0, tg_chi0_batch) to a subset of each site's orbitals:
  * mask(norb_max, n_atoms) flags the orbitals mu (both spins) that enter chi; null
  * restores every orbital (the reference's dimens = 4 sum_i nOrb_i^2).  With a mask,
@@ -167,6 +174,15 @@ int tg_jacobian_assemble(int n_atoms, const int* norb, int norb_max, const int* 
  * site's orbitals and p = (V, Bx, By, Bz): (1/pi) sum w Re Tr[P_i sigma_a G P_j sigma_b G].
  * No counterpart in the reference (its Jacobian uses the d-shell variables above). */
 int tg_adjoint_vb(tg_ctx* ctx, double Ef, double eta, double* A);
+
+/* tg_adjoint_vb with the potential and the field acting on a subset of each site's
+ * orbitals and the observables summed over the same subset: mask(norb_max, n_atoms)
+ * flags the orbitals (null = every orbital, i.e. tg_adjoint_vb).  With the d orbitals
+ * flagged, p = (V, B) is the d-shell field of update_Umatrix (mod_U_matrix.F90:29-55),
+ * whose exchange part is B_i = -(Um_i / 2) m_i on the d orbitals, so with Un = 0 the
+ * reference's moment Jacobian is J + 1 = -(Um / 2) A on the moment rows and columns.
+ * No counterpart in the reference. */
+int tg_adjoint_vb_orbitals(tg_ctx* ctx, double Ef, double eta, const int* mask, double* A);
 
 /* n_atoms, norb_max and (when norb is not null) norb(n_atoms) of the system set by
  * tg_set_system. */

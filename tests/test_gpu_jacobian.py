@@ -88,6 +88,35 @@ def test_adjoint_vb_matches_central_differences(gpu):
             assert np.max(np.abs(fd - A[:, b + 4 * j])) < 1e-7, (j, b)
 
 
+@pytest.mark.parametrize("shape", ["sq2", "bcc4"])
+def test_adjoint_matches_the_reference_jacobian_through_the_chain_rule(gpu, shape):
+    """The d-shell (V, B) adjoint against the oracle's analytic Jacobian (calcJacobian_greenfunction,
+    mod_self_consistency.F90:795-1205).  With Un = 0 the unknowns are the d-shell moments and
+    update_Umatrix (mod_U_matrix.F90:29-55) sets the d-shell field B_i = -(Um_i / 2) m_i, so
+    J_ref + 1 = -(Um / 2) A on the moment rows and columns (the reference subtracts the identity
+    on the first neq - 1 unknowns only)."""
+    nk = (2, 2, 2) if shape == "bcc4" else (3, 3, 1)
+    deck = synthetic.make_deck(shape, nk=nk, n1gl=6, parts=1, n3gl=4)
+    s = deck.system
+    for el in s.elements:
+        el.Un = 0.0
+    h0 = s.h0(initial_state(s))
+    gpu.setup(deck, h0)
+    A = gpu.adjoint_vb_orbitals(s.Ef, s.eta, s.dorbs)
+    J = O.jacobian(O.Model(s, h0), deck.ek, (deck.real_kp, deck.real_w), s.Ef, s.eta, fixEf=True)
+    neq = J.shape[0]
+    assert neq == 3 * s.n_atoms
+    Jp = J + np.diag([1.0] * (neq - 1) + [0.0])
+    Um = s.Um()
+    pred = np.zeros_like(J)
+    for i in range(s.n_atoms):
+        for j in range(s.n_atoms):
+            for a in range(3):
+                for b in range(3):
+                    pred[3 * i + a, 3 * j + b] = -0.5 * Um[j] * A[1 + a + 4 * i, 1 + b + 4 * j]
+    assert np.max(np.abs(Jp - pred)) <= 1e-10 * max(1.0, np.max(np.abs(Jp)))
+
+
 def test_autograd_function_uses_the_adjoint(gpu):
     import torch
     from titan_b200.autograd import expectation_vb

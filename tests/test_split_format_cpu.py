@@ -3,13 +3,14 @@
 Test infrastructure only: the CUDA kernels (split_quantize_kernel,
 split_contract_kernel) are what ships; this file checks the format they
 implement, on the CPU.
-  * per chunk and operand element the scale 2^(38 - E), E the frexp exponent of
-    the chunk's largest |Re|, |Im|; X = rint(x 2^(38 - E)), |X| <= 2^38;
-  * five balanced base-256 digits, most significant first: with Y = X +
-    0x80808080 the low four are the bytes of Y's low word minus 128 and the top
-    one is Y >> 32, so X = d0 2^32 + d1 2^24 + d2 2^16 + d3 2^8 + d4 exactly;
-  * the 19 digit products of levels l = i + j <= 5 summed per level in exact
-    integers, recombined as sum_l S_l 2^(-12 - 8 l) 2^(E_A + E_B).
+  * per chunk and operand element the scale 2^(46 - E), E the frexp exponent of
+    the chunk's largest |Re|, |Im|; X = rint(x 2^(46 - E)), |X| <= 2^46;
+  * six balanced base-256 digits, most significant first: with Y = X +
+    0x8080808080 the low five are bytes 0..4 of Y minus 128 and the top one
+    is Y >> 40, so X = d0 2^40 + d1 2^32 + d2 2^24 + d3 2^16 + d4 2^8 + d5;
+  * the 21 digit products of levels l = i + j <= 5 summed per level in exact
+    integers, recombined as sum_l S_l 2^(-12 - 8 l) 2^(E_A + E_B) (the same
+    weights as a five-digit 38-bit format: the sixth digit only extends it).
 The operands are Green functions of the synthetic sq2 system near the real
 axis, in the layout of the contraction (A = w G1, B = G2^T per point), so the
 error is that of the realistic sums the format was chosen on.
@@ -20,14 +21,15 @@ from oracle import titan_oracle as O
 from titan_b200.host import synthetic
 from titan_b200.host.system import initial_state
 
-BITS = 38
+BITS = 46
+NDIG = 6
 
 
 def digits(X):
-    """Balanced base-256 digits of int64 X (|X| <= 2^38), most significant first."""
-    Y = X + 0x80808080
+    """Balanced base-256 digits of int64 X (|X| <= 2^46), most significant first."""
+    Y = X + 0x8080808080
     low = (Y & 0xFFFFFFFF).astype(np.uint32) ^ np.uint32(0x80808080)
-    d = [(Y >> 32).astype(np.int64)]
+    d = [(Y >> 40).astype(np.int64), (((Y >> 32) & 0xFF) ^ 0x80).astype(np.int8).astype(np.int64)]
     for sh in (24, 16, 8, 0):
         d.append(((low >> np.uint32(sh)) & np.uint32(0xFF)).astype(np.int64).astype(np.int8).astype(np.int64))
     return d
@@ -42,26 +44,30 @@ def quantise(x):
     return digits(X), E, X
 
 
-def split_product(a, b, max_level=5):
-    """sum_p a[p, u] b[p, v] for real a, b through the digit format."""
+def split_product(a, b, max_level=5, chunk=None):
+    """sum_p a[p, u] b[p, v] for real a, b through the digit format (one scale per element
+    and chunk of `chunk` points; None = one chunk)."""
+    if chunk is not None and chunk < a.shape[0]:
+        return sum(split_product(a[s:s + chunk], b[s:s + chunk], max_level)
+                   for s in range(0, a.shape[0], chunk))
     da, Ea, _ = quantise(a)
     db, Eb, _ = quantise(b)
     out = np.zeros((a.shape[1], b.shape[1]))
     for lvl in range(max_level + 1):
         S = np.zeros_like(out)
-        for i in range(5):
+        for i in range(NDIG):
             j = lvl - i
-            if 0 <= j < 5:
+            if 0 <= j < NDIG:
                 S += (da[i].T @ db[j]).astype(np.float64)   # exact: |S| < 2^53 here
         out += np.ldexp(S, -12 - 8 * lvl)
     return np.ldexp(out, Ea[:, None] + Eb[None, :])
 
 
-def complex_split(A, B, max_level=5):
-    rr = split_product(A.real, B.real, max_level)
-    ii = split_product(A.imag, B.imag, max_level)
-    ri = split_product(A.real, B.imag, max_level)
-    ir = split_product(A.imag, B.real, max_level)
+def complex_split(A, B, max_level=5, chunk=None):
+    rr = split_product(A.real, B.real, max_level, chunk)
+    ii = split_product(A.imag, B.imag, max_level, chunk)
+    ri = split_product(A.real, B.imag, max_level, chunk)
+    ir = split_product(A.imag, B.real, max_level, chunk)
     return (rr - ii) + 1j * (ri + ir)
 
 
@@ -89,19 +95,38 @@ def test_digits_reconstruct_exactly():
     X = rng.integers(-2 ** BITS, 2 ** BITS + 1, size=20000, dtype=np.int64)
     X[:4] = [2 ** BITS, -2 ** BITS, 0, -1]
     d = digits(X)
-    assert all(np.all(np.abs(di) <= 128) for di in d[1:])
-    rec = d[0] * 2 ** 32 + d[1] * 2 ** 24 + d[2] * 2 ** 16 + d[3] * 2 ** 8 + d[4]
+    assert all(np.all(np.abs(di) <= 128) for di in d[1:]) and np.all(np.abs(d[0]) <= 64)
+    rec = d[0] * 2 ** 40 + d[1] * 2 ** 32 + d[2] * 2 ** 24 + d[3] * 2 ** 16 + d[4] * 2 ** 8 + d[5]
     assert np.array_equal(rec, X)
+    # the level sums stay exact int32: at most six products of |d_i d_j| <= 2^14 per level
+    assert 6 * 2 ** 14 * 16384 < 2 ** 31
 
 
 def test_split_contraction_error_and_dropped_levels():
     A, B = operands()
     ref = A.T @ B
     err = np.linalg.norm(complex_split(A, B) - ref) / np.linalg.norm(ref)
-    assert err < 1e-9, err
+    assert err < 1e-11, err
     # dropping level 5 (the digit products of level L = 7) costs accuracy the format cannot afford
     err6 = np.linalg.norm(complex_split(A, B, max_level=4) - ref) / np.linalg.norm(ref)
     assert err6 > 10 * err, (err, err6)
+
+
+def test_short_chunks_bound_the_error_of_every_significant_entry():
+    """Near the real axis (Im z = 2e-3) |G| varies by orders of magnitude along the k list:
+    one scale per element and 128-point chunk keeps every entry holding at least 1e-4 of
+    the largest within 1e-9 relative, where one 4096-point chunk does not."""
+    A, B = operands(npts=4096)
+    ref = A.T @ B
+    big = np.abs(ref) >= 1e-4 * np.abs(ref).max()
+
+    def worst(chunk):
+        got = complex_split(A, B, chunk=chunk)
+        return np.max(np.abs(got - ref)[big] / np.abs(ref)[big])
+
+    short, long_ = worst(128), worst(4096)
+    assert short < 1e-9, short
+    assert long_ > 2 * short, (short, long_)
 
 
 def test_exponent_sidecar_gives_the_quantiser_the_same_scale():

@@ -166,6 +166,8 @@ struct tg_ctx {
   // disturbance response (eintshe)
   DevArray<int> d_she_tab, d_ia, d_she_ztiles, d_she_rowoff;
   DevArray<double2> d_she_part, d_she_sum, d_she_pref, d_she_out;
+  // split precision: points per chunk (one scale per operand element and chunk)
+  int split_chunk = kSplitMaxChunk;
   // chi0 over a subset of orbitals (tg_set_chi_orbitals)
   bool chi_sel_on = false;
   ChiLayout chi_sel;
@@ -481,16 +483,16 @@ int contract(tg_ctx* c, const ChiView& v, const double2* A, const double2* B, in
   return TG_OK;
 }
 
-// chunks of a pass: runs of equal key (energy), at most kSplitMaxChunk points each
+// chunks of a pass: runs of equal key (energy), at most maxc points each
 template <class Key>
-SplitChunks make_chunks(int64_t np, Key key) {
+SplitChunks make_chunks(int64_t np, int maxc, Key key) {
   SplitChunks ch;
   int64_t i = 0;
   ch.kstart.push_back(0);
   while (i < np) {
     const auto k0 = key(i);
     int64_t j = i + 1;
-    while (j < np && j - i < kSplitMaxChunk && key(j) == k0) ++j;
+    while (j < np && j - i < maxc && key(j) == k0) ++j;
     const int cnt = (int)(j - i);
     const int nk = (cnt + kSplitK - 1) / kSplitK;
     const int ci = (int)ch.count.size();
@@ -504,9 +506,9 @@ SplitChunks make_chunks(int64_t np, Key key) {
 }
 
 // chunks of a k-major pass over a tabulated mesh of ne energies (work item p0 + i = k * ne
-// + energy): the slots of one energy are ne apart, so every energy of the pass is one chunk
-// (split at kSplitMaxChunk points) with stride ne
-SplitChunks make_chunks_kmajor(int64_t p0, int64_t np, int64_t ne) {
+// + energy): the slots of one energy are ne apart, so every energy of the pass is cut into
+// chunks of at most maxc points with stride ne
+SplitChunks make_chunks_kmajor(int64_t p0, int64_t np, int64_t ne, int maxc) {
   SplitChunks ch;
   ch.stride = (int)ne;
   ch.kstart.push_back(0);
@@ -515,8 +517,8 @@ SplitChunks make_chunks_kmajor(int64_t p0, int64_t np, int64_t ne) {
     const int64_t first = (ie - e0 + ne) % ne;   // first slot of energy ie
     if (first >= np) continue;
     const int64_t total = (np - 1 - first) / ne + 1;
-    for (int64_t done = 0; done < total; done += kSplitMaxChunk) {
-      const int cnt = (int)std::min<int64_t>(kSplitMaxChunk, total - done);
+    for (int64_t done = 0; done < total; done += maxc) {
+      const int cnt = (int)std::min<int64_t>(maxc, total - done);
       const int nk = (cnt + kSplitK - 1) / kSplitK;
       const int ci = (int)ch.count.size();
       ch.slot0.push_back((int)(first + done * ne));
@@ -889,6 +891,14 @@ int tg_set_real_mesh(tg_ctx* c, int64_t n_k, const double* kp, const double* w) 
   return TG_OK;
 }
 
+int tg_set_split_chunk(tg_ctx* c, int points) {
+  if (!c) return TG_ERR_ARG;
+  if (points < 0 || points > kSplitMaxChunk)
+    return set_err(c, TG_ERR_ARG, "tg_set_split_chunk: points must lie in [0, 16384]");
+  c->split_chunk = points == 0 ? kSplitMaxChunk : points;
+  return TG_OK;
+}
+
 int tg_set_chi_orbitals(tg_ctx* c, const int* mask) {
   if (!c) return TG_ERR_ARG;
   if (!c->sys_set) return set_err(c, TG_ERR_STATE, "tg_set_system has not been called");
@@ -1033,8 +1043,8 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     if (split) {
       KindTimer kt(c, 3);
       const double* yv = c->h_y.data() + p0;
-      const SplitChunks ch = tab_imag ? make_chunks_kmajor(p0, np, c->n_e_u)
-                                      : make_chunks(np, [&](int64_t i) { return yv[i]; });
+      const SplitChunks ch = tab_imag ? make_chunks_kmajor(p0, np, c->n_e_u, c->split_chunk)
+                                      : make_chunks(np, c->split_chunk, [&](int64_t i) { return yv[i]; });
       if ((rc = split_prepare(c, v, ch, pd))) return rc;
       if ((rc = split_quantize_operand(c, v, 1, c->d_B.p, pd, e16_g2 ? c->d_e16B.p : nullptr))) return rc;
     }
@@ -1147,8 +1157,9 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
           const int64_t nrk = c->n_realk, pbase = p0;
           {
             KindTimer kq(c, 3);
-            const SplitChunks ch = tab_real ? make_chunks_kmajor(pbase, np, n_real)
-                                            : make_chunks(np, [&](int64_t i) { return (pbase + i) / nrk; });
+            const SplitChunks ch = tab_real ? make_chunks_kmajor(pbase, np, n_real, c->split_chunk)
+                                            : make_chunks(np, c->split_chunk,
+                                                          [&](int64_t i) { return (pbase + i) / nrk; });
             rc = split_prepare(c, v, ch, pr);
             if (!rc) rc = split_quantize_operand(c, v, 1, c->d_B.p, pr, e16_rb ? c->d_e16B.p : nullptr);
             if (!rc) rc = split_quantize_operand(c, v, 0, c->d_A.p, pr, e16_ra ? c->d_e16A.p : nullptr);

@@ -8,6 +8,7 @@
 // The host part here is O(n_atoms^2 nd^2 256) and runs on the CPU.
 #include <cmath>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "../../include/titan_gpu.h"
@@ -206,6 +207,44 @@ int tg_adjoint_vb(tg_ctx* ctx, double Ef, double eta, double* A) {
       const double* T16 = T.data() + 2 * 16 * ((size_t)i * n_atoms + j);
       for (int a = 0; a < 4; ++a)
         for (int b = 0; b < 4; ++b) A[(size_t)(b + 4 * j) * m + (a + 4 * i)] = vertex(T16, a, b) / kPi;
+    }
+  return TG_OK;
+}
+
+int tg_adjoint_vb_orbitals(tg_ctx* ctx, double Ef, double eta, const int* mask, double* A) {
+  if (!mask) return tg_adjoint_vb(ctx, Ef, eta, A);
+  if (!ctx || !A) return TG_ERR_ARG;
+  int n_atoms = 0, norb_max = 0;
+  int rc = tg_system_shape(ctx, &n_atoms, &norb_max, nullptr);
+  if (rc) return rc;
+  std::vector<int> norb(n_atoms);
+  rc = tg_system_shape(ctx, &n_atoms, &norb_max, norb.data());
+  if (rc) return rc;
+  // the orbital-resolved tensor with the masked orbitals as the resolved ones: row groups
+  // g < n_i (one masked orbital each, then the rest), column groups h < n_i
+  std::vector<int> nsel(n_atoms, 0);
+  int nmax_sel = 0;
+  for (int i = 0; i < n_atoms; ++i) {
+    for (int o = 0; o < norb[i]; ++o) nsel[i] += mask[(size_t)i * norb_max + o] ? 1 : 0;
+    nmax_sel = std::max(nmax_sel, nsel[i]);
+  }
+  if (nmax_sel == 0) return TG_ERR_ARG;
+  const int nrow = nmax_sel + 1, ncol = nmax_sel;
+  std::vector<double> T((size_t)2 * 16 * n_atoms * n_atoms * nrow * ncol, 0.0);
+  rc = tg_gg_tensor(ctx, Ef, eta, 1, mask, T.data());
+  if (rc) return rc;
+  const int m = 4 * n_atoms;
+  std::vector<double> S(2 * 16);
+  for (int i = 0; i < n_atoms; ++i)
+    for (int j = 0; j < n_atoms; ++j) {
+      std::fill(S.begin(), S.end(), 0.0);
+      for (int g = 0; g < nsel[i]; ++g)
+        for (int h = 0; h < nsel[j]; ++h) {
+          const double* T16 = T.data() + 2 * 16 * ((((size_t)i * n_atoms + j) * nrow + g) * ncol + h);
+          for (int e = 0; e < 32; ++e) S[e] += T16[e];
+        }
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) A[(size_t)(b + 4 * j) * m + (a + 4 * i)] = vertex(S.data(), a, b) / kPi;
     }
   return TG_OK;
 }

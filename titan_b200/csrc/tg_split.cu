@@ -3,9 +3,9 @@
 //
 // Three kernels per pass and operand: split_rowmax_kernel (per chunk and
 // element, the largest |Re|, |Im|), split_quantize_kernel (FP64 operand ->
-// five int8 digit planes, K-step blocks) and split_contract_kernel (warp-
+// six int8 digit planes, K-step blocks) and split_contract_kernel (warp-
 // specialised: one producer warp stages digit blocks with bulk copies into a
-// six-stage shared-memory ring, one warp issues the 19 MMAs per K-step, eight
+// five-stage shared-memory ring, one warp issues the 21 MMAs per K-step, eight
 // warps drain the six int32 level accumulators from TMEM at every chunk end
 // into FP64 sums held in registers until the unit ends).
 // Every wait on an mbarrier is bounded (2 s of %globaltimer); on a timeout the
@@ -75,17 +75,18 @@ __global__ void split_rowmax_e16_kernel(const int16_t* __restrict__ E16, int64_t
   }
 }
 
-// Balanced base-256 digits of 16 integers |X| <= 2^38, slice-major: out[0] holds
-// the top digits, out[1..4] the lower ones (most significant first).  With
-// Y = X + 0x80808080 the low four balanced digits are the bytes of the low word
-// of Y minus 128 (a byte-wise XOR with 0x80), and the top digit is Y >> 32.
+// Balanced base-256 digits of 16 integers |X| <= 2^46, slice-major: out[0] holds
+// the top digits, out[1..5] the lower ones (most significant first).  With
+// Y = X + 0x8080808080 the five lower balanced digits are bytes 0..4 of Y minus
+// 128 (a byte-wise XOR with 0x80), and the top digit is Y >> 40 (in [-64, 64]).
 __device__ __forceinline__ void digits16(const long long (&x)[16], uint4 (&out)[kSplitSlices]) {
-  uint32_t lo[16], top[4] = {0u, 0u, 0u, 0u};
+  uint32_t lo[16], top[4] = {0u, 0u, 0u, 0u}, mid[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
-    const long long y = x[k] + 0x80808080LL;
+    const long long y = x[k] + 0x8080808080LL;
     lo[k] = (uint32_t)y ^ 0x80808080u;
-    top[k >> 2] |= ((uint32_t)(int)(y >> 32) & 255u) << (8 * (k & 3));
+    mid[k >> 2] |= (((uint32_t)(y >> 32) & 255u) ^ 0x80u) << (8 * (k & 3));
+    top[k >> 2] |= ((uint32_t)(int)(y >> 40) & 255u) << (8 * (k & 3));
   }
   uint32_t b[4][4];   // b[byte][group of four values]
 #pragma unroll
@@ -100,8 +101,9 @@ __device__ __forceinline__ void digits16(const long long (&x)[16], uint4 (&out)[
     b[3][j] = __byte_perm(t1, t3, 0x7632);
   }
   out[0] = make_uint4(top[0], top[1], top[2], top[3]);
+  out[1] = make_uint4(mid[0], mid[1], mid[2], mid[3]);
 #pragma unroll
-  for (int i = 1; i < kSplitSlices; ++i) out[i] = make_uint4(b[4 - i][0], b[4 - i][1], b[4 - i][2], b[4 - i][3]);
+  for (int i = 2; i < kSplitSlices; ++i) out[i] = make_uint4(b[5 - i][0], b[5 - i][1], b[5 - i][2], b[5 - i][3]);
 }
 
 // one thread per (K-step t, k half kc, group g, row r < rows): 16 points of one
@@ -123,14 +125,15 @@ __global__ void __launch_bounds__(256) split_quantize_kernel(
     const int c = kchunk[t];
     const SplitGroup gr = groups[g];
     const int64_t e = gr.elem0 + r;
-    // scale 2^(38 - E) with max |x| < 2^E; elements below 2^-985 of unit scale count as zero
+    // scale 2^(46 - E) with max |x| < 2^E; elements below 2^-977 of unit scale count as zero
+    // (the scale's exponent field must stay below 2047)
     bool valid = r < gr.nvalid;
     int Ex = 0;
     if (valid) {
       const double m = __longlong_as_double((long long)M64[(int64_t)c * ld + e]);
       if (m > 0.0) frexp(m, &Ex);
       if (t == kstart[c] && kc == 0) E[(int64_t)c * ld + e] = Ex;
-      if (m == 0.0 || Ex < -985) valid = false;
+      if (m == 0.0 || Ex < -977) valid = false;
     }
     const double scale = __hiloint2double((1023 + kSplitBits - (valid ? Ex : 0)) << 20, 0);
     const int first = (t - kstart[c]) * kSplitK + kc * 16;   // point within the chunk
@@ -165,8 +168,8 @@ __global__ void __launch_bounds__(256) split_quantize_kernel(
 constexpr int kMmaM = 128;
 constexpr int kMmaN = 2 * kSplitColsB;     // 80
 constexpr int kLevels = 6;                 // L = 2..7
-constexpr int kStages = 6;
-constexpr int kStageBytes = kSplitABlock + kSplitBBlock;   // 33280
+constexpr int kStages = 5;
+constexpr int kStageBytes = kSplitABlock + kSplitBBlock;   // 39936
 constexpr int kHalfCols = kSplitColsB / 2;                 // complex columns per epilogue warp
 constexpr int kXchBytes = 2 * 64 * 4 * 16 + 2 * 256;      // 2 halves x 64 rows x 4 complex, 2 x 40 exponents
 constexpr int kEpiThreads = 256;                           // 8 epilogue warps
@@ -175,6 +178,7 @@ constexpr uint32_t kTmemCols = 512;
 constexpr int kBarOff = kStages * kStageBytes + kXchBytes;  // 8-byte aligned
 constexpr int kNumBars = 2 * kStages + 3;
 constexpr size_t kSplitSmem = 1024 + kBarOff + kNumBars * 8 + 16;
+static_assert(kSplitSmem <= 232448, "the stage ring must fit the 227 KB of shared memory per CTA");
 constexpr unsigned long long kWaitNs = 2000000000ull;        // 2 s per wait
 
 __host__ __device__ constexpr uint32_t idesc_i8() {
@@ -393,7 +397,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
             tc_fence_after();
             const uint32_t sa = base + (uint32_t)s * kStageBytes;
             const uint32_t sb = sa + kSplitABlock;
-            // digit pairs (i, j) with level l = i + j <= 5, grouped by level
+            // digit pairs (i, j) (0-based) with level l = i + j <= 5, grouped by level: 21 MMAs
 #pragma unroll
             for (int l = 0; l < kLevels; ++l) {
 #pragma unroll

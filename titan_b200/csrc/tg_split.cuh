@@ -1,16 +1,18 @@
 // Split-precision chi0 contraction (int8 slices on the tcgen05 tensor cores).
 //
 // The contraction C_ij[u][v] = sum_p A_p[u] B_p[v] of a pass is evaluated on
-// integers.  Per chunk c of points (one energy, at most kSplitMaxChunk points)
-// and per operand element e, a power-of-two scale 2^E[c][e] bounds
-// max_p |Re|, |Im| of the element over the chunk; the element becomes the
-// 38-bit integer X = rint(x 2^(38 - E)) held as five balanced base-256 digits
-// (int8, most significant first).  The int8 tensor cores give exact int32
-// sums of digit products; products of digit pairs (i, j) are accumulated per
-// level L = i + j (L = 2..7, 19 products; the dropped levels weigh <= 2^-44
-// of the largest product) in six TMEM accumulators, and every chunk end the
-// levels are recombined in FP64 with weights 2^(4 - 8L) 2^(E_A + E_B) and
-// added to the FP64 partial accumulators (same layout as the FP64 path).
+// integers.  Per chunk c of points (a run of one energy, at most the context's
+// chunk length, itself at most kSplitMaxChunk points) and per operand element e,
+// a power-of-two scale 2^E[c][e] bounds max_p |Re|, |Im| of the element over the
+// chunk; the element becomes the 46-bit integer X = rint(x 2^(46 - E)) held as six
+// balanced base-256 digits (int8, most significant first; the top one in
+// [-64, 64]).  The int8 tensor cores give exact int32 sums of digit products;
+// products of digit pairs (i, j) (1-based) are accumulated per level L = i + j
+// (L = 2..7, 21 products) in six TMEM accumulators, and every chunk end the levels
+// are recombined in FP64 with weights 2^(4 - 8L) 2^(E_A + E_B) and added to the
+// FP64 partial accumulators (same layout as the FP64 path).  Short chunks follow
+// the magnitude of G along the k list, so that most points use most of the 46
+// bits: near the real axis the error falls with the chunk length.
 //
 // Operand digits live in HBM as K-step blocks (32 points), K-major in the
 // canonical no-swizzle core-matrix layout, so one bulk copy stages a block:
@@ -29,14 +31,14 @@
 
 namespace tg {
 
-constexpr int kSplitSlices = 5;        // base-256 digits per value
-constexpr int kSplitBits = 38;         // |X| <= 2^38
+constexpr int kSplitSlices = 6;        // base-256 digits per value
+constexpr int kSplitBits = 46;         // |X| <= 2^46
 constexpr int kSplitK = 32;            // points per K-step (one MMA K)
 constexpr int kSplitRowsA = 64;        // complex rows per A group
 constexpr int kSplitColsB = 40;        // complex columns per B group
-constexpr int kSplitMaxChunk = 16384;  // points per chunk: level sums stay below 2^31
-constexpr int kSplitABlock = kSplitSlices * 2 * kSplitRowsA * kSplitK;   // 20480 bytes
-constexpr int kSplitBBlock = kSplitSlices * 2 * kSplitColsB * kSplitK;   // 12800 bytes
+constexpr int kSplitMaxChunk = 16384;  // points per chunk: level sums stay below 6 2^28 < 2^31
+constexpr int kSplitABlock = kSplitSlices * 2 * kSplitRowsA * kSplitK;   // 24576 bytes
+constexpr int kSplitBBlock = kSplitSlices * 2 * kSplitColsB * kSplitK;   // 15360 bytes
 
 // one 64-row (A) or 40-column (B) group of a site pair's operand elements
 struct SplitGroup {

@@ -73,6 +73,8 @@ SIGNATURES = {
     "tg_system_shape": (C.c_int, [C.c_void_p, _ip, _ip, _ip]),
     "tg_expectation_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp]),
     "tg_set_chi_orbitals": (C.c_int, [C.c_void_p, _ip]),
+    "tg_set_split_chunk": (C.c_int, [C.c_void_p, C.c_int]),
+    "tg_adjoint_vb_orbitals": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _ip, _dp]),
 }
 
 
@@ -198,6 +200,10 @@ class GreenGPU:
         self.dimens = system.dimens
         self.chi_dimens = system.dimens
         self.nmax = nmax
+
+    def set_split_chunk(self, points=0):
+        """Points per split-precision chunk (tg_set_split_chunk; 0 = default)."""
+        self._check(self.lib.tg_set_split_chunk(self.h, int(points)))
 
     def set_chi_orbitals(self, sel=None):
         """chi0 over the orbitals sel[i] (local indices) of each site, e.g. the d orbitals
@@ -344,6 +350,17 @@ class GreenGPU:
         m = 4 * self.system.n_atoms
         A = np.zeros((m, m), np.float64, order="F")
         self._check(self.lib.tg_adjoint_vb(self.h, Ef, eta, A.ctypes.data_as(_dp)))
+        return np.ascontiguousarray(A)
+
+    def adjoint_vb_orbitals(self, Ef, eta, sel):
+        """adjoint_vb with the fields on, and the observables summed over, the orbitals sel[i]
+        of each site (tg_adjoint_vb_orbitals)."""
+        m = 4 * self.system.n_atoms
+        mask = np.zeros((self.system.n_atoms, self.nmax), np.int32)
+        for i, x in enumerate(sel):
+            mask[i, list(x)] = 1
+        A = np.zeros((m, m), np.float64, order="F")
+        self._check(self.lib.tg_adjoint_vb_orbitals(self.h, Ef, eta, _p(mask, C.c_int), A.ctypes.data_as(_dp)))
         return np.ascontiguousarray(A)
 
     def dyson(self, chi_hf, U):
