@@ -88,7 +88,7 @@ int tg_chi0_batch(tg_ctx* ctx, const double* q, int n_omega, const double* e, do
  * points are cut into chunks of at most this many, and every operand element gets one
  * power-of-two scale per chunk, so shorter chunks follow the magnitude of G along the k
  * list (more accurate near the real axis) at the cost of more accumulator drains.
- * 1 .. 16384; 0 restores the default.  No counterpart in the reference. */
+ * 1 .. 16384; 0 restores the default (1024).  No counterpart in the reference. */
 int tg_set_split_chunk(tg_ctx* ctx, int points);
 
 /* Restricts chi0 (tg_chi0, tg_chi0_batch) to a subset of each site's orbitals:
@@ -237,6 +237,16 @@ int tg_jij(tg_ctx* ctx, const double* q, double Ef, double eta, const double* ev
  * S(norb_max, norb_max, 3, n_atoms) complex (Smunuiivec).  Gauss-Jordan per point. */
 int tg_smunu(tg_ctx* ctx, double Ef, double eta, double* S);
 
+/* Ground-state orbital density of every site: the Green-function integral of
+ * calc_GS_L_and_E_greenfunction (source/mod_expectation.F90:912-982),
+ *   gupgd(nu, mu, i) = (1/pi) sum_{k,E} w (G(i mu up, i nu up) + G(i mu dn, i nu dn))
+ * at Ef + i(y + eta) over the imaginary-axis mesh; gupgd(norb_max, norb_max, n_atoms)
+ * complex.  The orbital moments follow on the host as in calculate_L (:984-1009):
+ * lxm(i) = Re sum_{mu,nu} lvec(mu, nu, 1) gupgd(mu, nu, i), and likewise lym, lzm and the
+ * local-frame lxpm.. with lpvec.  The band energy is not computed (the reference sets it
+ * to zero on this path).  Gauss-Jordan per point. */
+int tg_gs_orbital(tg_ctx* ctx, double Ef, double eta, double* gupgd);
+
 /* Local density of states on the real axis: replaces ldos_energy(e, ldosu, ldosd)
  * (source/mod_LDOS.F90:95-150) for n_e energies at once:
  *   ldosu(mu, i, ie) = -(1/pi) sum_k w_k Im G(i up mu, i up mu; k, e(ie) + i eta)
@@ -280,6 +290,16 @@ int tg_eig_batch(tg_ctx* ctx, int64_t nk, const double* kp, double* lam, double*
  * and H(dimH, dimH, nk) = h0 + calchk(k). */
 int tg_green_batch(tg_ctx* ctx, int64_t nz, const double* z, const double* kp, double* G);
 int tg_hamiltk_batch(tg_ctx* ctx, int64_t nk, const double* kp, double* H);
+
+/* Measured FP64 throughput of the current device (TFLOP/s): a DFMA loop (8 independent
+ * chains per thread) and a DMMA loop (mma.sync.m8n8k4.f64, 4 chains per warp), 4 CTAs of
+ * 256 threads per SM, timed with CUDA events.  The denominators of the inversion
+ * kernels' roofline.  ctx may be null.  No counterpart in the reference. */
+int tg_fp64_peak(tg_ctx* ctx, double* tflops_dfma, double* tflops_dmma);
+
+/* Test hook: r[i] = the pivot reciprocal of the Gauss-Jordan kernels applied to s[i] > 0
+ * (the hardware approximation refined by three Newton-Raphson steps). */
+int tg_rcp_check(int64_t n, const double* s, double* r);
 
 /* Device timing of the last tg_chi0/tg_chi0_batch call (CUDA events on the
  * context's stream): ms[0] imaginary-axis G2 inversions, ms[1] contraction and

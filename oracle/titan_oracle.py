@@ -18,6 +18,7 @@ It restates the reference's FP64 algorithm with numpy/LAPACK:
                             source/calculate_chi.F90:85-89
 * ``site_reduce``        -- source/calculate_chi.F90:91-107
 * ``expectation``        -- source/mod_expectation.F90:28-149
+* ``gs_orbital``         -- source/mod_expectation.F90:912-982 (orbital density)
 * ``jacobian``           -- source/mod_self_consistency.F90:795-1205
 * ``self_consistency``   -- Newton iteration on sc_eqs
                             (source/mod_self_consistency.F90:1516-1833); the
@@ -781,6 +782,27 @@ def disturbance_outputs(system, chi_hf, tchi_raw, U, lvec, lambda_p, lambda_d, p
 # Local density of states on the real axis, source/mod_LDOS.F90:95-150 (ldos_energy):
 # ldosu(i, mu) = -(1/pi) sum_k w_k Im G(i up mu, i up mu; k, e + i eta), ldosd with the down block.
 # ---------------------------------------------------------------------------
+def gs_orbital(model: Model, mesh, Ef, eta, chunk=4096):
+    """gupgd of calc_GS_L_and_E_greenfunction (mod_expectation.F90:912-982) as [i, a, b] =
+    gupgd(a, b, i) = (1/pi) sum w (G(i b up, i a up) + G(i b dn, i a dn))."""
+    s = model.system
+    ia = s.ia()
+    nmax = max(s.norbs)
+    out = np.zeros((s.n_atoms, nmax, nmax), dtype=complex)
+    y = mesh.point_energy()
+    for sl in _chunks(mesh.n_points, chunk):
+        G = model.green(Ef + 1j * (y[sl] + eta), mesh.kp[sl])
+        w = mesh.weight[sl]
+        for i in range(s.n_atoms):
+            n = s.norbs[i]
+            b = ia[i][0]
+            up = G[:, b:b + n, b:b + n]
+            dn = G[:, b + n:b + 2 * n, b + n:b + 2 * n]
+            # gupgd(nu, mu) += G(mu, nu) + G(mu', nu')
+            out[i, :n, :n] += np.einsum("p,pmn->nm", w, up + dn)
+    return out / PI
+
+
 def ldos(model: Model, real_bz, energies, eta, chunk=4096):
     """(ldosu, ldosd) [n_e, nAtoms, nOrbMax] at each energy e (absolute, as green(e, eta) is called)."""
     s = model.system

@@ -397,3 +397,28 @@ def test_spectral_expectation_on_request(gpu, fe_deck):
         gpu.set_green_method("auto")
     for a, b in zip(sp, gj):
         assert np.max(np.abs(a - b)) < 1e-11
+
+
+def test_gs_orbital_matches_oracle_and_fe_golden(gpu, fe_deck):
+    """tg_gs_orbital (calc_GS_L_and_E_greenfunction's orbital density) against the oracle, and the
+    orbital moment of the golden Fe state against scResult."""
+    from titan_b200.host.orbital import calculate_l
+    from titan_b200.host.response import site_parameters
+    s = fe_deck.system
+    h0 = s.h0(fe_deck.state)
+    gpu.setup(fe_deck, h0)
+    P = gpu.gs_orbital(s.Ef, s.eta)
+    ref = O.gs_orbital(O.Model(s, h0), fe_deck.ek, s.Ef, s.eta)
+    assert np.max(np.abs(P - ref)) <= 1e-12 * np.max(np.abs(ref))
+    lvec, lpvec = site_parameters(s)[:2]
+    lz = calculate_l(s, P, lvec, lpvec)[2][0]
+    line = [l for l in open(os.path.join(GOLDEN, "Fe_bulk_susc", "scResult")) if "Lz=" in l][0]
+    assert abs(lz - float(line.split("Lz=")[1].split()[0])) < 1e-7
+
+
+def test_gs_orbital_multi_site(gpu):
+    deck = synthetic.make_deck("sq2", nk=(5, 5, 1), n1gl=8, parts=1, n3gl=4)
+    s, h0 = _setup(gpu, deck)
+    P = gpu.gs_orbital(s.Ef, s.eta)
+    ref = O.gs_orbital(O.Model(s, h0), deck.ek, s.Ef, s.eta)
+    assert np.max(np.abs(P - ref)) <= 1e-12 * np.max(np.abs(ref))

@@ -178,3 +178,22 @@ def test_fe_sum_rule_holds_and_host_matches_oracle(fe_deck):
     assert diff < 1e-10 * np.abs(lo).max()
     lh, rh, dh = SR.check(s, chi, S, B)
     assert np.abs(lh - lo).max() <= 1e-14 and np.abs(rh - ro).max() <= 1e-13
+
+
+def _golden_lz():
+    line = [l for l in open(os.path.join(GOLDEN, "Fe_bulk_susc", "scResult")) if "Lz=" in l][0]
+    return float(line.split("Lz=")[1].split()[0])
+
+
+def test_fe_orbital_moment_matches_golden(fe_deck):
+    """calc_GS_L_and_E_greenfunction + calculate_L on the golden Fe state give the scResult's
+    orbital moment (global frame, printed to 7 decimals)."""
+    from titan_b200.host.orbital import calculate_l
+    from titan_b200.host.response import site_parameters
+    s = fe_deck.system
+    m = O.Model(s, s.h0(fe_deck.state))
+    P = O.gs_orbital(m, fe_deck.ek, s.Ef, s.eta)
+    lvec, lpvec = site_parameters(s)[:2]
+    lx, ly, lz, _, _, _ = calculate_l(s, P, lvec, lpvec)
+    assert abs(lx[0]) < 1e-7 and abs(ly[0]) < 1e-7
+    assert abs(lz[0] - _golden_lz()) < 1e-7, lz[0]

@@ -171,7 +171,7 @@ constexpr int kLevels = 6;                 // L = 2..7
 constexpr int kStages = 5;
 constexpr int kStageBytes = kSplitABlock + kSplitBBlock;   // 39936
 constexpr int kHalfCols = kSplitColsB / 2;                 // complex columns per epilogue warp
-constexpr int kXchBytes = 2 * 64 * 4 * 16 + 2 * 256;      // 2 halves x 64 rows x 4 complex, 2 x 40 exponents
+constexpr int kXchBytes = 2 * 64 * 4 * 16 + 2 * 64 * 8;   // 2 halves x 64 rows x 4 complex, 2 x 40 column scales
 constexpr int kEpiThreads = 256;                           // 8 epilogue warps
 constexpr int kThreads = 64 + kEpiThreads;                 // producer, MMA, epilogue
 constexpr uint32_t kTmemCols = 512;
@@ -274,6 +274,9 @@ __device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&v)[4]) {
                : "r"(taddr));
 }
 
+// 2^e for -1022 <= e <= 1023, from the bits
+__device__ __forceinline__ double pow2(int e) { return __hiloint2double((1023 + e) << 20, 0); }
+
 // exact double of an integer |v| < 2^51: its bits added to those of 1.5 * 2^52 give
 // 1.5 * 2^52 + v (the same binade), and the subtraction is exact
 __device__ __forceinline__ double i51_to_double(long long v) {
@@ -307,7 +310,7 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sbase + kBarOff + kNumBars * 8 + 4);
   volatile int* epi_ok = reinterpret_cast<volatile int*>(sbase + kBarOff + kNumBars * 8 + 8);
   double2* xch = reinterpret_cast<double2*>(sbase + kStages * kStageBytes);   // [2][64 * 4]
-  int* ebs = reinterpret_cast<int*>(sbase + kStages * kStageBytes + 2 * 64 * 4 * 16);   // [2][64]
+  double* sbs = reinterpret_cast<double*>(sbase + kStages * kStageBytes + 2 * 64 * 4 * 16);   // [2][64]
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -460,12 +463,14 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
       while (t < k1) {
         const int c = kchunk[t];
         const int te = min(k1, kstart[c + 1]);
-        // exponents of the chunk, fetched while its MMAs still run (buffer d & 1 was last
-        // read two chunks ago, before the accumulator barrier of the previous chunk)
+        // scales of the chunk, fetched while its MMAs still run (buffer d & 1 was last
+        // read two chunks ago, before the accumulator barrier of the previous chunk): the
+        // level fold times 2^(E_A - 14) 2^(E_B - 14) is the value (E >= -977, so both are
+        // normal doubles and their product is exact)
         const int64_t erow = (int64_t)c * a.ld + aoff;
-        int* eb = ebs + 64 * (d & 1u);
-        if (ep < kSplitColsB) eb[ep] = tile.v0 + ep < M ? a.EB[erow + tile.v0 + ep] : 0;
-        const int ea = u < M ? a.EA[erow + u] : 0;
+        double* sb = sbs + 64 * (d & 1u);
+        if (ep < kSplitColsB) sb[ep] = pow2(tile.v0 + ep < M ? a.EB[erow + tile.v0 + ep] - 14 : 0);
+        const double sa = pow2(u < M ? a.EA[erow + u] - 14 : 0);
         if (ep == 0) *epi_ok = mbar_wait(accfull, d & 1u, abort_flag, a.err, 4) ? 1 : 0;
         epi_sync();
         ok = *epi_ok != 0;
@@ -489,9 +494,9 @@ __global__ void __launch_bounds__(kThreads, 1) split_contract_kernel(SplitContra
           }
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
-            const int e = ea + eb[cbase + 4 * g + k] - 28;
-            ax[4 * g + k] += ldexp(levels_value(x, k), e);
-            ay[4 * g + k] += ldexp(levels_value(y, k), e);
+            const double sab = sa * sb[cbase + 4 * g + k];
+            ax[4 * g + k] = fma(levels_value(x, k), sab, ax[4 * g + k]);
+            ay[4 * g + k] = fma(levels_value(y, k), sab, ay[4 * g + k]);
           }
         }
         ++d;

@@ -74,8 +74,21 @@ SIGNATURES = {
     "tg_expectation_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp, _dp, _dp, _dp, _dp]),
     "tg_set_chi_orbitals": (C.c_int, [C.c_void_p, _ip]),
     "tg_set_split_chunk": (C.c_int, [C.c_void_p, C.c_int]),
+    "tg_gs_orbital": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
+    "tg_fp64_peak": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "tg_rcp_check": (C.c_int, [C.c_int64, _dp, _dp]),
     "tg_adjoint_vb_orbitals": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _ip, _dp]),
 }
+
+
+def fp64_peak():
+    """(DFMA, DMMA) FP64 TFLOP/s measured on the current device (tg_fp64_peak)."""
+    lib = load_library()
+    a, b = C.c_double(), C.c_double()
+    rc = lib.tg_fp64_peak(None, C.byref(a), C.byref(b))
+    if rc != 0:
+        raise TitanGPUError(rc, "tg_fp64_peak failed")
+    return a.value, b.value
 
 
 class TitanGPUError(RuntimeError):
@@ -408,6 +421,14 @@ class GreenGPU:
         S = np.zeros((nat, 3, self.nmax, self.nmax), np.complex128)   # Fortran (mu, nu, 3, nat) read back
         self._check(self.lib.tg_smunu(self.h, Ef, eta, _p(S.view(np.float64))))
         return np.swapaxes(S, 2, 3)
+
+    def gs_orbital(self, Ef, eta):
+        """gupgd[i, a, b] = the reference's gupgd(a, b, i) of calc_GS_L_and_E_greenfunction
+        (tg_gs_orbital): (1/pi) sum w (G(i b up, i a up) + G(i b dn, i a dn))."""
+        nat = self.system.n_atoms
+        P = np.zeros((nat, self.nmax, self.nmax), np.complex128)   # Fortran (a, b, i) read back as [i, b, a]
+        self._check(self.lib.tg_gs_orbital(self.h, Ef, eta, _p(P.view(np.float64))))
+        return np.swapaxes(P, 1, 2)
 
     def ldos(self, energies, eta):
         """LDOS up / down [n_e, n_atoms, nOrbMax] on the real-axis BZ (ldos_energy, mod_LDOS.F90:95-150)."""
