@@ -174,6 +174,7 @@ struct tg_ctx {
   bool chi_sel_on = false;
   ChiLayout chi_sel;
   DevArray<double2> d_graw;   // column-major G of a pass (gathered chi0 operands)
+  DevArray<unsigned char> d_clws;   // workspace of the thread-block-cluster Gauss-Jordan kernel
   // tg_expectation_noalloc: device address of the library's fixed scratch array on this
   // context's device (looked up by the context's first no-alloc call)
   double2* noalloc_ptr = nullptr;
@@ -267,6 +268,8 @@ GreenArgs base_args(tg_ctx* c) {
   a.h0 = c->d_h0.p;
   a.outmap = c->d_outmap.p;
   a.status = c->d_status.p;
+  a.ws = c->d_clws.p;
+  a.ws_bytes = c->d_clws.n;
   return a;
 }
 
@@ -722,6 +725,8 @@ int tg_set_system(tg_ctx* c, int n_atoms, const int* norb, int norb_max, int n_n
     return set_err(c, TG_ERR_ARG, b);
   }
   c->chi_sel_on = false;
+  if (!green_supported(c->dimH))
+    TG_CHECK(c, c->d_clws.ensure(green_cluster_ws_bytes(c->dimH, c->num_sms)), "alloc cluster workspace");
   const int n = c->dimH;
   // row tables
   std::vector<int> ratom(n), rorb(n), rspin(n);

@@ -1,30 +1,33 @@
 // Batched G(k, z) = (z - h0 - H(k))^-1 for any dimension up to 288: one thread-block
-// cluster per matrix, Gauss-Jordan with partial pivoting across distributed shared memory.
+// cluster per matrix, panel-blocked Gauss-Jordan with partial pivoting.
 //
 // The matrix of one (k, z) point is too large for one SM at the reference's larger
-// systems (a 288 x 288 complex matrix is 1.33 MB), so a cluster of CS <= 8 CTAs shares it:
-//   * column j lives in CTA j % CS (local column j / CS), row t in thread t of every CTA,
-//     so each thread holds one row segment of up to kNLC = 32 complex entries in
-//     registers (288 rows x 9 CTAs x 32 columns at dimH = 288; 9 warps per CTA leave 168
-//     registers per thread, so the segment is 128 of them);
-//   * step p (pivot column p, owned by CTA p % CS): the owner has already published the
-//     column's values and its pivot row r (largest |Re| + |Im| among the rows not yet
-//     used, first index on ties -- the izamax choice of zgetrf) into every CTA's shared
-//     memory; thread r scales its row segment by 1 / a_rp, every other row subtracts its
-//     multiple of the scaled segment, and column p becomes (-a_tp / a_rp, 1 / a_rp on row r);
-//   * lookahead: the owner of column p + 1 updates that column first, searches its pivot
-//     and writes it into the other CTAs (st through the cluster window) before updating its
-//     remaining columns; one cluster barrier per step publishes it (two buffers);
-//   * a CTA's columns become pivot columns in local order, so the next one is always kept
-//     in register slot 0 by rotating the segment after each (no dynamic register index);
-//   * rows are never swapped: the result X holds G[step(t)][piv(j)] at (t, j), where
-//     step(t) is the step whose pivot row was t (the same implicit permutation as the
-//     single-SM kernels); the output stage unpermutes through shared memory and writes
-//     G column-major per point (MODE_RAW), one column per coalesced store run.
-// The kernel is persistent: the grid holds as many clusters as fit, each walking the
-// point range.  This replaces invers = zgetrf + zgetri (mod_tools.F90:796-829) inside
-// green (mod_greenfunction.F90:19-75) for dimensions the single-SM kernels do not cover;
-// H(k) comes from a tabulated row (calchk + hamilt_local) or is summed in the kernel.
+// systems (a 288 x 288 complex matrix is 1.33 MB), so a cluster of CS <= 9 CTAs shares it:
+//   * columns are grouped in panels of kPB = 8; panel P lives in CTA P % CS (local panel
+//     P / CS), so each CTA holds up to kNLC = 32 columns (four panels) of every row, kept in
+//     shared memory as [slot][row] (147 KB at dimH = 288, 9 CTAs); thread t works on row t.
+//     (A row segment of 32 complex entries in registers would leave 9-warp CTAs, 168
+//     registers per thread, spilling; the update runs over register halves of 16 slots);
+//   * panel P, phase 1 (its owner CTA alone): eight Gauss-Jordan steps restricted to the
+//     panel's columns.  Step j picks the pivot row r_j of column 8 P + j (largest
+//     |Re| + |Im| among the rows not yet used, first index on ties -- the izamax choice of
+//     zgetrf), records the column before the step (the multipliers f_j) and 1 / a_rj, and
+//     eliminates inside the panel.  The multipliers and pivots go to a per-cluster buffer in
+//     global memory (L2-resident, read back with ld.global.cg), then one cluster barrier
+//     publishes the panel;
+//   * phase 2 (every CTA, on its other columns): the pivot rows' current segments are
+//     staged in shared memory, 32 threads turn them into the scaled pivot rows of the eight
+//     steps (prow_j = (row r_j - sum_{k<j} f_k[r_j] prow_k) / a_rj), and every row applies
+//     the rank-8 update row_i -= sum_j f_j[i] prow_j (pivot row r_j: prow_j - sum_{k>j} ...);
+//     the result equals eight rank-1 Gauss-Jordan steps, with one cluster barrier per panel
+//     instead of one per step;
+//   * rows are never swapped: the result X holds G[step(t)][piv(j)] at (t, j), where step(t)
+//     is the step whose pivot row was t; the output stage permutes the rows in shared memory
+//     and writes G column-major per point (MODE_RAW), one column per coalesced store run.
+// The kernel is persistent: the grid holds as many clusters as fit, each walking the point
+// range.  This replaces invers = zgetrf + zgetri (mod_tools.F90:796-829) inside green
+// (mod_greenfunction.F90:19-75) for dimensions the single-SM kernels do not cover; H(k)
+// comes from a tabulated row (calchk + hamilt_local) or is summed in the kernel.
 #include "tg_internal.cuh"
 
 #include <cooperative_groups.h>
@@ -37,13 +40,14 @@ namespace {
 
 namespace cg = cooperative_groups;
 
-constexpr int kNLC = 32;       // local columns per CTA (registers per row segment)
-constexpr int kMaxN = 288;     // one row per thread
-constexpr int kMaxCS = 9;      // cluster size (9 > 8: non-portable, enabled at launch)
+constexpr int kPB = 8;           // columns per panel
+constexpr int kNLC = 32;         // local columns per CTA (four panels; registers per row segment)
+constexpr int kMaxN = 288;       // one row per thread
+constexpr int kMaxCS = 9;        // cluster size (9 > 8: non-portable, enabled at launch)
 constexpr int kMaxWarps = kMaxN / 32;
 
 struct ClSmem {
-  size_t fcol, pidx, prow, candv, candr, piv, phase, stage, total;
+  size_t colbuf, prow1, prow, pr, pinv, candv, candr, piv, phase, fs, blk, total;
 };
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -51,27 +55,30 @@ __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15)
 __host__ __device__ inline ClSmem cl_smem(int n, int n_neigh) {
   ClSmem L;
   size_t o = 0;
-  L.fcol = o;  o = al16(o + sizeof(double2) * 2 * (size_t)n);
-  L.pidx = o;  o = al16(o + sizeof(int) * 4);
-  L.prow = o;  o = al16(o + sizeof(double2) * kNLC);
-  L.candv = o; o = al16(o + sizeof(double) * kMaxWarps);
-  L.candr = o; o = al16(o + sizeof(int) * kMaxWarps);
-  L.piv = o;   o = al16(o + sizeof(int) * (size_t)n);
-  L.phase = o; o = al16(o + sizeof(double2) * (size_t)(n_neigh > 0 ? n_neigh : 1));
-  L.stage = o; o = al16(o + sizeof(double2) * (size_t)kNLC * n);
+  L.colbuf = o;  o = al16(o + sizeof(double2) * (size_t)n);
+  L.prow1 = o;   o = al16(o + sizeof(double2) * kPB);
+  L.prow = o;    o = al16(o + sizeof(double2) * kPB * kNLC);
+  L.pr = o;      o = al16(o + sizeof(int) * kPB);
+  L.pinv = o;    o = al16(o + sizeof(double2) * kPB);
+  L.candv = o;   o = al16(o + sizeof(double) * kMaxWarps);
+  L.candr = o;   o = al16(o + sizeof(int) * kMaxWarps);
+  L.piv = o;     o = al16(o + sizeof(int) * (size_t)n);
+  L.phase = o;   o = al16(o + sizeof(double2) * (size_t)(n_neigh > 0 ? n_neigh : 1));
+  L.fs = o;      o = al16(o + sizeof(double2) * (size_t)kPB * n);
+  L.blk = o;     o = al16(o + sizeof(double2) * (size_t)kNLC * n);
   L.total = o;
   return L;
 }
 
+// per-cluster workspace in global memory: F[2][kPB][n] multipliers, INV[2][kPB], R[2][kPB]
+__host__ __device__ inline size_t ws_cluster_bytes(int n) {
+  return sizeof(double2) * (2 * kPB * (size_t)n + 2 * kPB) + sizeof(int) * 2 * kPB;
+}
+
 struct ClState {
-  double2* fcol;       // [2][n] pivot column of the step (this CTA's copy)
-  int* pidx;           // [2] pivot row of the step
-  double2* prow;       // [kNLC] this CTA's part of the scaled pivot row
   double* candv;
   int* candr;
-  int* piv;            // [n] step -> pivot row
-  int n, cs, rank, t;
-  int rot;             // left rotations of the row segment so far (see gj_step)
+  int n, t;
   bool used;           // this thread's row has been a pivot row
   int my_step;         // step at which it became one
 };
@@ -109,95 +116,105 @@ __device__ __forceinline__ int cta_argmax(const ClState& st, double2 v) {
   return i2;
 }
 
-// publish column values (one per thread) and the pivot row into buffer `buf` of every CTA
-__device__ __forceinline__ void publish(const ClState& st, cg::cluster_group& cl, int buf, double2 v, int r) {
-  for (int d = 0; d < st.cs; ++d) {
-    double2* rf = cl.map_shared_rank(st.fcol, d);
-    if (st.t < st.n) rf[buf * st.n + st.t] = v;
-    if (st.t == 0) {
-      int* rp = cl.map_shared_rank(st.pidx, d);
-      rp[buf] = r;
+__device__ __forceinline__ double2 ldcg2(const double2* p) { return __ldcg(p); }
+
+// Phase 1 of the panel in slots s0 .. s0 + 7 of the CTA's block (its owner CTA only): nb
+// Gauss-Jordan steps on the panel's columns; the multipliers f_j (the column before step j)
+// go to F[j][row], 1 / a_rj and r_j to INV[j], R[j]
+__device__ __forceinline__ void factor_panel(ClState& st, double2* blk, int s0, double2* colbuf, double2* prow1,
+                                             double2* F, double2* INV, int* R, int nb, int* status, int64_t point) {
+  const int t = st.t, n = st.n;
+  double2* row = blk + (size_t)s0 * n + t;   // row[s * n] = this thread's entry in slot s0 + s
+  for (int j = 0; j < nb; ++j) {
+    const double2 v = t < n ? row[(size_t)j * n] : make_double2(0, 0);
+    if (t < n) {
+      colbuf[t] = v;
+      F[(size_t)j * n + t] = v;
+    }
+    const int r = cta_argmax(st, v);   // its barrier also publishes colbuf
+    const double2 pv = colbuf[r];
+    if (pv.x == 0.0 && pv.y == 0.0 && t == 0) atomicMin(status, (int)(point + 1));
+    const double2 inv = crecip_fast(pv);
+    if (t == 0) {
+      INV[j] = inv;
+      R[j] = r;
+    }
+    if (t == r) {
+#pragma unroll
+      for (int s = 0; s < kPB; ++s) {
+        const double2 w = cmul(row[(size_t)s * n], inv);
+        prow1[s] = w;
+        row[(size_t)s * n] = w;
+      }
+      row[(size_t)j * n] = inv;
+      st.used = true;
+    }
+    __syncthreads();
+    if (t < n && t != r) {
+#pragma unroll
+      for (int s = 0; s < kPB; ++s) row[(size_t)s * n] = cfms(v, prow1[s], row[(size_t)s * n]);
+      row[(size_t)j * n] = cmul(make_double2(-v.x, -v.y), inv);
     }
   }
 }
 
-// one elimination step p.  The CTA's next own pivot column is always A[0]: after its
-// column has been the pivot column, the owner rotates its row segment left by one
-// (st.rot counts the rotations, physical slot i holds local column (i + rot) % kNLC).
-__device__ __forceinline__ void gj_step(ClState& st, cg::cluster_group& cl, double2 (&A)[kNLC], int p, int* status,
-                                        int64_t point) {
-  const int buf = p & 1;
-  const int r = st.pidx[buf];
-  const double2 fi = st.t < st.n ? st.fcol[buf * st.n + st.t] : make_double2(0, 0);
-  const double2 pv = st.fcol[buf * st.n + r];
-  if (pv.x == 0.0 && pv.y == 0.0 && st.rank == 0 && st.t == 0) atomicMin(status, (int)(point + 1));
-  const double2 inv = crecip_fast(pv);
-  const int q = p % st.cs;
-  const bool own_p = q == st.rank;
-  if (st.t == 0) st.piv[p] = r;
-  if (st.t == r) {
+// this thread's 16-slot half h of its row: every panel step k < nb with multipliers Fs[k][row]
+// and scaled pivot rows prow[k][slot]; the row that was the pivot row of step myj becomes
+// prow[myj] minus the later steps; slots of local panel `skip` are left alone
+__device__ __forceinline__ void update_half(double2* blk, int h, int t, int n, int nb, int myj, int skip,
+                                            const double2* Fs, const double2* prow) {
+  constexpr int kH = kNLC / 2;
+  double2 a[kH];
 #pragma unroll
-    for (int lc = 0; lc < kNLC; ++lc) {
-      const double2 v = cmul(A[lc], inv);
-      st.prow[lc] = v;
-      A[lc] = v;
+  for (int s = 0; s < kH; ++s) a[s] = blk[(size_t)(kH * h + s) * n + t];
+  int k0 = 0;
+  if (myj >= 0) {
+#pragma unroll
+    for (int s = 0; s < kH; ++s)
+      if (((kH * h + s) >> 3) != skip) a[s] = prow[myj * kNLC + kH * h + s];
+    k0 = myj + 1;
+  }
+  for (int k = k0; k < nb; ++k) {
+    const double2 f = Fs[k * n + t];
+    if (myj < 0 || k > myj) {
+#pragma unroll
+      for (int s = 0; s < kH; ++s)
+        if (((kH * h + s) >> 3) != skip) a[s] = cfms(f, prow[k * kNLC + kH * h + s], a[s]);
     }
-    if (own_p) A[0] = inv;
-    st.used = true;
-    st.my_step = p;
   }
-  __syncthreads();
-  const bool upd = st.t < st.n && st.t != r;
-  // lookahead: the owner of column p + 1 updates it first (slot 0, or slot 1 when the
-  // same CTA also owns column p, i.e. a one-CTA cluster), searches its pivot and
-  // publishes it before updating its other columns
-  const bool own_next = p + 1 < st.n && (p + 1) % st.cs == st.rank;
-  const bool one = st.cs == 1;
-  if (own_next) {
-    double2 v = one ? A[1] : A[0];
-    if (upd) v = cfms(fi, one ? st.prow[1] : st.prow[0], v);
-    if (one) A[1] = v; else A[0] = v;
-    const int rn = cta_argmax(st, v);
-    publish(st, cl, buf ^ 1, v, rn);
-  }
-  if (upd) {
-    const bool skip0 = own_next && !one, skip1 = own_next && one;
 #pragma unroll
-    for (int lc = 0; lc < kNLC; ++lc) {
-      if ((lc == 0 && skip0) || (lc == 1 && skip1)) continue;
-      A[lc] = cfms(fi, st.prow[lc], A[lc]);
-    }
-    if (own_p) A[0] = cmul(make_double2(-fi.x, -fi.y), inv);
-  }
-  if (own_p) {
-    const double2 a0 = A[0];
-#pragma unroll
-    for (int lc = 0; lc + 1 < kNLC; ++lc) A[lc] = A[lc + 1];
-    A[kNLC - 1] = a0;
-    ++st.rot;
-  }
-  cl.sync();
+  for (int s = 0; s < kH; ++s) blk[(size_t)(kH * h + s) * n + t] = a[s];
 }
 
-__global__ void __launch_bounds__(kMaxN, 1) green_cluster_kernel(GreenArgs a, int cs) {
+__global__ void __launch_bounds__(kMaxN, 1) green_cluster_kernel(GreenArgs a, int cs, double2* ws) {
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = a.n;
   const ClSmem L = cl_smem(n, a.n_neigh);
+  double2* colbuf = reinterpret_cast<double2*>(smem + L.colbuf);
+  double2* prow1 = reinterpret_cast<double2*>(smem + L.prow1);
+  double2* prow = reinterpret_cast<double2*>(smem + L.prow);         // [kPB][kNLC]
+  int* pr_s = reinterpret_cast<int*>(smem + L.pr);
+  double2* pinv_s = reinterpret_cast<double2*>(smem + L.pinv);
+  int* piv = reinterpret_cast<int*>(smem + L.piv);
+  double2* phase = reinterpret_cast<double2*>(smem + L.phase);
+  double2* Fs = reinterpret_cast<double2*>(smem + L.fs);             // [kPB][n]
+  double2* blk = reinterpret_cast<double2*>(smem + L.blk);           // [kNLC][n]
   ClState st;
-  st.fcol = reinterpret_cast<double2*>(smem + L.fcol);
-  st.pidx = reinterpret_cast<int*>(smem + L.pidx);
-  st.prow = reinterpret_cast<double2*>(smem + L.prow);
   st.candv = reinterpret_cast<double*>(smem + L.candv);
   st.candr = reinterpret_cast<int*>(smem + L.candr);
-  st.piv = reinterpret_cast<int*>(smem + L.piv);
-  double2* phase = reinterpret_cast<double2*>(smem + L.phase);
-  double2* stage = reinterpret_cast<double2*>(smem + L.stage);
   st.n = n;
-  st.cs = cs;
-  st.rank = (int)cl.block_rank();
   st.t = threadIdx.x;
+  const int rank = (int)cl.block_rank();
   const int64_t cid = blockIdx.x / cs, ncl = gridDim.x / cs;
+  // this cluster's workspace
+  unsigned char* wsb = reinterpret_cast<unsigned char*>(ws) + cid * ws_cluster_bytes(n);
+  double2* F = reinterpret_cast<double2*>(wsb);               // [2][kPB][n]
+  double2* INV = F + 2 * kPB * (size_t)n;                     // [2][kPB]
+  int* R = reinterpret_cast<int*>(INV + 2 * kPB);             // [2][kPB]
+  const int npanels = (n + kPB - 1) / kPB;
+  const int t = st.t;
+  int pcount = 0;   // panels processed by this cluster so far (selects the workspace buffer)
 
   for (int64_t pl = cid; pl < a.np; pl += ncl) {
     // ---- point data ----------------------------------------------------------------
@@ -238,13 +255,10 @@ __global__ void __launch_bounds__(kMaxN, 1) green_cluster_kernel(GreenArgs a, in
       }
       __syncthreads();
     }
-    // ---- A = z 1 - H(k): row t, columns j = lc * cs + rank ------------------------------
-    // built through the stage buffer ([lc][row]) so that no address lives beside the row
-    // segment in registers
-    const int t = st.t;
+    // ---- A = z 1 - H(k) into the block: slot ls = 8 lp + c holds column 8 (lp cs + rank) + c
     for (int e = t; e < kNLC * n; e += blockDim.x) {
-      const int lc = e / n, r = e - lc * n;
-      const int j = lc * cs + st.rank;
+      const int ls = e / n, r = e - ls * n;
+      const int j = ((ls / kPB) * cs + rank) * kPB + (ls % kPB);
       double2 v = make_double2(0, 0);
       if (j < n) {
         double2 h;
@@ -261,36 +275,95 @@ __global__ void __launch_bounds__(kMaxN, 1) green_cluster_kernel(GreenArgs a, in
         }
         v = make_double2((r == j ? zr : 0.0) - h.x, (r == j ? zi : 0.0) - h.y);
       }
-      stage[e] = v;
+      blk[e] = v;
     }
-    __syncthreads();
-    double2 A[kNLC];
-#pragma unroll
-    for (int lc = 0; lc < kNLC; ++lc) A[lc] = t < n ? stage[lc * n + t] : make_double2(0, 0);
     st.used = false;
     st.my_step = 0;
-    st.rot = 0;
-    // ---- pivot of column 0 (CTA 0, local column 0), published before the first step ----
-    if (st.rank == 0) {
-      const int r0 = cta_argmax(st, A[0]);
-      publish(st, cl, 0, A[0], r0);
-    }
-    cl.sync();
-    for (int p = 0; p < n; ++p) gj_step(st, cl, A, p, a.status, pg);
-    // ---- output: G[step(t)][piv(j)] = A[t][lc] -> column piv(j), row step(t) ---------------
-#pragma unroll
-    for (int i = 0; i < kNLC; ++i)
-      if (t < n) stage[((i + st.rot) % kNLC) * n + st.my_step] = A[i];
     __syncthreads();
-    double2* out = a.out + pl * ((int64_t)n * n);
-    for (int lc = 0; lc < kNLC; ++lc) {
-      const int j = lc * cs + st.rank;
-      if (j >= n) break;
-      const int col = st.piv[j];
-      for (int r = t; r < n; r += blockDim.x) out[(int64_t)col * n + r] = stage[lc * n + r];
+
+    for (int P = 0; P < npanels; ++P, ++pcount) {
+      const int buf = pcount & 1;
+      const int owner = P % cs;
+      const int nb = min(kPB, n - P * kPB);
+      double2* Fb = F + (size_t)buf * kPB * n;
+      const bool own = rank == owner;
+      // ---- phase 1: the owner factorises the panel (slots 8 lp .. 8 lp + 7) ---------------
+      if (own) {
+        factor_panel(st, blk, kPB * (P / cs), colbuf, prow1, Fb, INV + buf * kPB, R + buf * kPB, nb, a.status, pg);
+        __threadfence();
+      }
+      cl.sync();
+      // ---- phase 2: every CTA applies the panel's steps to its other columns ----------
+      // the panel's multipliers go to shared memory first: one round of independent L2
+      // loads instead of one per use
+      if (t < nb) {
+        pr_s[t] = __ldcg(R + buf * kPB + t);
+        pinv_s[t] = ldcg2(INV + buf * kPB + t);
+      }
+      if (t < n) {
+        double2 fv[kPB];
+#pragma unroll
+        for (int k = 0; k < kPB; ++k)
+          if (k < nb) fv[k] = ldcg2(Fb + (size_t)k * n + t);
+#pragma unroll
+        for (int k = 0; k < kPB; ++k)
+          if (k < nb) Fs[k * n + t] = fv[k];
+      }
+      __syncthreads();
+      int myj = -1;   // the panel step whose pivot row is this thread's row
+      for (int j = 0; j < nb; ++j)
+        if (pr_s[j] == t) myj = j;
+      if (myj >= 0) {
+        st.used = true;
+        st.my_step = P * kPB + myj;
+      }
+      if (t < nb) piv[P * kPB + t] = pr_s[t];
+      // scaled pivot rows: thread t < 32 runs the eight-step recurrence for slot t, reading
+      // the pivot rows' current entries from the block (not written before the barrier below)
+      if (t < kNLC) {
+        for (int j = 0; j < nb; ++j) {
+          const int rj = pr_s[j];
+          double2 x = blk[(size_t)t * n + rj];
+          for (int k = 0; k < j; ++k) x = cfms(Fs[k * n + rj], prow[k * kNLC + t], x);
+          prow[j * kNLC + t] = cmul(x, pinv_s[j]);
+        }
+      }
+      __syncthreads();
+      // the owner's panel slots were done in phase 1
+      const int skip = own ? P / cs : -1;
+      if (t < n) {
+        update_half(blk, 0, t, n, nb, myj, skip, Fs, prow);
+        update_half(blk, 1, t, n, nb, myj, skip, Fs, prow);
+      }
+      // prow, pr_s, pinv_s and Fs are rewritten by the next panel after this barrier; the
+      // next panel's owner reads its panel slots of the block after it as well
+      __syncthreads();
     }
-    // the next point rewrites stage, fcol[0] and pidx[0]: every CTA is done with them
-    cl.sync();
+    // ---- output: G[step(t)][piv(j)] = X[t][slot] -> column piv(j), row step(t) ------------
+    // rows are permuted in place: every thread reads its 32 entries before any is written
+    double2 keep[kNLC / 2];
+#pragma unroll
+    for (int hh = 0; hh < 2; ++hh) {
+      if (t < n) {
+#pragma unroll
+        for (int s = 0; s < kNLC / 2; ++s) keep[s] = blk[(size_t)(kNLC / 2 * hh + s) * n + t];
+      }
+      __syncthreads();
+      if (t < n) {
+#pragma unroll
+        for (int s = 0; s < kNLC / 2; ++s) blk[(size_t)(kNLC / 2 * hh + s) * n + st.my_step] = keep[s];
+      }
+      __syncthreads();
+    }
+    double2* out = a.out + pl * ((int64_t)n * n);
+    for (int ls = 0; ls < kNLC; ++ls) {
+      const int j = ((ls / kPB) * cs + rank) * kPB + (ls % kPB);
+      if (j >= n) continue;
+      const int col = piv[j];
+      for (int r = t; r < n; r += blockDim.x) out[(int64_t)col * n + r] = blk[(size_t)ls * n + r];
+    }
+    // the next point rewrites the block, colbuf and piv: this CTA is done with them
+    __syncthreads();
   }
 }
 
@@ -298,13 +371,18 @@ __global__ void __launch_bounds__(kMaxN, 1) green_cluster_kernel(GreenArgs a, in
 
 int green_cluster_supported(int n, int mode) { return n >= 1 && n <= kMaxN && mode == MODE_RAW; }
 
-int green_cluster_size(int n) { return std::min(kMaxCS, std::max(1, (n + kNLC - 1) / kNLC)); }
+int green_cluster_size(int n) {
+  const int npanels = (n + kPB - 1) / kPB;
+  return std::min(kMaxCS, std::max(1, (npanels + kNLC / kPB - 1) / (kNLC / kPB)));
+}
+
+size_t green_cluster_ws_bytes(int n, int num_sms) { return ws_cluster_bytes(n) * (size_t)std::max(num_sms, 1); }
 
 cudaError_t launch_green_cluster(const GreenArgs& a, int num_sms, cudaStream_t s) {
   if (!green_cluster_supported(a.n, a.mode) || a.out2) return cudaErrorInvalidValue;
   if (a.np <= 0) return cudaSuccess;
   const int cs = green_cluster_size(a.n);
-  if ((a.n + cs - 1) / cs > kNLC) return cudaErrorInvalidValue;
+  if (((a.n + kPB - 1) / kPB + cs - 1) / cs * kPB > kNLC) return cudaErrorInvalidValue;
   const int threads = (a.n + 31) / 32 * 32;
   const size_t smem = cl_smem(a.n, a.n_neigh).total;
   cudaError_t e = cudaFuncSetAttribute(green_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -329,9 +407,11 @@ cudaError_t launch_green_cluster(const GreenArgs& a, int num_sms, cudaStream_t s
   e = cudaOccupancyMaxActiveClusters(&max_clusters, green_cluster_kernel, &cfg);
   if (e != cudaSuccess) return e;
   if (max_clusters < 1) return cudaErrorInvalidConfiguration;
-  const int64_t ncl = std::min<int64_t>(max_clusters, a.np);
+  // the workspace holds num_sms clusters (more than can be resident)
+  const int64_t ncl = std::min<int64_t>(std::min(max_clusters, num_sms), a.np);
+  if (!a.ws || a.ws_bytes < ws_cluster_bytes(a.n) * (size_t)ncl) return cudaErrorInvalidValue;
   cfg.gridDim = dim3((unsigned)(ncl * cs), 1, 1);
-  return cudaLaunchKernelEx(&cfg, green_cluster_kernel, a, cs);
+  return cudaLaunchKernelEx(&cfg, green_cluster_kernel, a, cs, reinterpret_cast<double2*>(a.ws));
 }
 
 }  // namespace tg

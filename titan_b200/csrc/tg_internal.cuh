@@ -148,6 +148,10 @@ struct GreenArgs {
   // kernels ignore it and evaluate every point
   double y_split = 0.0;
   int y_side = 0;
+  // device workspace of the kernels that exchange data through global memory (the
+  // thread-block-cluster Gauss-Jordan kernel: green_cluster_ws_bytes)
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
 };
 
 // true when launch_green evaluates these arguments with the spectral kernel (the only
@@ -166,6 +170,7 @@ int green_acc_ctas(int n, int64_t np, int num_sms);
 // any dimension up to 288, MODE_RAW only: one thread-block cluster per matrix
 int green_cluster_supported(int n, int mode);
 int green_cluster_size(int n);
+size_t green_cluster_ws_bytes(int n, int num_sms);
 cudaError_t launch_green_cluster(const GreenArgs& a, int num_sms, cudaStream_t s);
 
 // FP64 pair-block contraction: Cpart[split][cpair_off + u*M + v] += sum_p A[p][off+u] B[p][off+v]
