@@ -45,7 +45,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="split", choices=["split", "fp64"])
     ap.add_argument("--config", default="sq2")
-    ap.add_argument("--omegas-per-step", type=int, default=4)
+    ap.add_argument("--omegas-per-step", type=int, default=0,
+                    help="frequencies per step (0: 4, or 1 for slab16 whose frequency costs minutes)")
+    ap.add_argument("--chi-orbitals", default="auto", choices=["auto", "all", "d"],
+                    help="orbitals that enter chi (auto: d for slab16, the d-only chi of dimension 1600, else all)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-compare-fp64", action="store_true",
@@ -158,7 +161,7 @@ def peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def cpu_baseline(deck, h0, reals, omegas, seconds_target=15.0):
+def cpu_baseline(deck, h0, reals, omegas, seconds_target=15.0, sel=None):
     """The oracle (numpy/LAPACK, all host threads) on a bounded sample of the workload.
 
     A 200-point calibration run sizes the sample so that it takes about
@@ -178,12 +181,13 @@ def cpu_baseline(deck, h0, reals, omegas, seconds_target=15.0):
         sub = EKMesh(ek.y, ek.wght, ek.energy_index[:n_imag_s], ek.kp[:n_imag_s], ek.weight[:n_imag_s])
         rk = (deck.real_kp[:max(nk_s, 1)], deck.real_w[:max(nk_s, 1)])
         t0 = time.perf_counter()
-        O.eintshechi(m, sub, rk, np.zeros(3), e, s.Ef, s.eta, s.etap, x2 if nk_s else None, p2 if nk_s else None)
+        O.eintshechi(m, sub, rk, np.zeros(3), e, s.Ef, s.eta, s.etap, x2 if nk_s else None, p2 if nk_s else None,
+                     sel=sel)
         return time.perf_counter() - t0
 
-    cal = min(200, ek.n_points)
+    cal = min(200 if s.dimH <= 90 else 20, ek.n_points)
     rate = cal / max(run(cal, 0), 1e-6)
-    n_imag_s = int(min(ek.n_points, max(500, rate * seconds_target * 2 / 3)))
+    n_imag_s = int(min(ek.n_points, max(cal, rate * seconds_target * 2 / 3)))
     nk_s = int(min(deck.real_kp.shape[0], max(1, rate * seconds_target / 3 / max(len(x2), 1)))) if len(x2) else 0
     dt = run(n_imag_s, nk_s)
     units = n_imag_s + len(x2) * nk_s
@@ -195,11 +199,31 @@ def cpu_baseline(deck, h0, reals, omegas, seconds_target=15.0):
 
 
 # --------------------------------------------------------------------------- reference arm
-def chi0_workload_desc(args, deck):
+def chi_selection(args, system):
+    """Per-site orbitals of chi: every orbital, or the d orbitals (the d-only chi of the 16-layer slab)."""
+    mode = args.chi_orbitals
+    if mode == "auto":
+        mode = "d" if args.config == "slab16" else "all"
+    return [list(d) for d in system.dorbs] if mode == "d" else None
+
+
+def chi_dim(system, sel):
+    return system.dimens if sel is None else 4 * sum(len(x) ** 2 for x in sel)
+
+
+def chi0_workload_desc(args, deck, omegas, reals):
     """The headline workload's name, the same on both arms."""
     s = deck.system
-    return (f"{args.config}: dimH={s.dimH}, chi dim={s.dimens}, {deck.ek.n_points} imag (E,k) points, "
-            f"{deck.real_kp.shape[0]} real-axis k x 64 energies, 32 omega in [0,0.5], q=0")
+    sel = chi_selection(args, s)
+    return (f"{args.config}: dimH={s.dimH}, chi dim={chi_dim(s, sel)}{' (d orbitals)' if sel else ''}, "
+            f"{deck.ek.n_points} imag (E,k) points, {deck.real_kp.shape[0]} real-axis k x {len(reals[-1][0])} "
+            f"energies, {len(omegas)} omega in [0,{max(omegas):.2g}], q=0")
+
+
+def omegas_per_step(args):
+    if args.omegas_per_step > 0:
+        return args.omegas_per_step
+    return 1 if args.config == "slab16" else 4
 
 
 def run_reference(args, rank, world):
@@ -210,10 +234,11 @@ def run_reference(args, rank, world):
     vals, secs = [], []
     # every warm-up step runs (on a shorter sample), then the timed steps on ~8 s samples, so
     # that the driver's --steps 20 --warmup 5 ends within a few minutes
+    sel = chi_selection(args, deck.system)
     for _ in range(args.warmup):
-        cpu_baseline(deck, h0, reals, omegas, seconds_target=2.0)
+        cpu_baseline(deck, h0, reals, omegas, seconds_target=2.0, sel=sel)
     for _ in range(args.steps):
-        cb = cpu_baseline(deck, h0, reals, omegas, seconds_target=8.0)
+        cb = cpu_baseline(deck, h0, reals, omegas, seconds_target=8.0, sel=sel)
         vals.append(cb["value"])
         secs.append(cb["seconds"])
     v = statistics.median(vals)
@@ -221,7 +246,7 @@ def run_reference(args, rank, world):
             "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(secs), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Slater-Koster model, no external data)", "impl": "reference",
-            "config": {"workload": chi0_workload_desc(args, deck),
+            "config": {"workload": chi0_workload_desc(args, deck, omegas, reals),
                        "step": "a bounded sample of the workload through the CPU restatement of eintshechi "
                                "(the reference is Fortran; no Fortran compiler in this image)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": "port", "sample": cb["sample"]},
@@ -276,9 +301,12 @@ def run_ours(args, rank, world, local_rank):
     s = deck.system
     gpu = GreenGPU(local_rank)
     gpu.setup(deck, h0)
+    sel = chi_selection(args, s)
+    gpu.set_chi_orbitals(sel)
+    D = chi_dim(s, sel)
     gpu.set_green_method(args.green)
     gpu.profile(True)
-    per = args.omegas_per_step
+    per = omegas_per_step(args)
     start = rank * per * (args.steps + args.warmup)     # ranks take different frequencies
     # warm-up (untimed)
     timed_steps(gpu, deck, h0, omegas, reals, args.warmup, start, per, args.precision)
@@ -303,7 +331,7 @@ def run_ours(args, rank, world, local_rank):
     last_units = units_of(deck, [(start + args.warmup * per + (args.steps - 1) * per + j) % len(omegas)
                                  for j in range(per)], reals)
     pk, pk_kind = peaks()
-    flops_con = 8.0 * s.dimens ** 2 * last_units
+    flops_con = 8.0 * D ** 2 * last_units
     achieved = flops_con / (con_ms / 1e3) / 1e12 if con_ms > 0 else None
     # the contraction runs inside a seconds-long step: the sustained (power-capped) GEMM peak
     peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
@@ -318,13 +346,14 @@ def run_ours(args, rank, world, local_rank):
                                               else "fp64 SIMT gemm64_kernel") + ")",
             "peak_source": ("of measured bf16 dense sustained (MEASURED_PEAKS.json)" if pk_kind == "measured"
                             else "of fallback 1.4 PF sustained"),
-            "flops_per_unit": 8.0 * s.dimens ** 2,
+            "flops_per_unit": 8.0 * D ** 2,
             "launches_in_last_step": int(con_n), "avg_launch_ms": (con_ms / con_n) if con_n else None,
             "quantize_ms_last_step": q_ms if args.precision == "split" else None}
     if args.precision == "split" and con_n:
         # what the tensor pipe executes: 21 int8 MMAs of 128 x 80 x 32 per 64 x 40 complex tile
         # and K-step of 32 points (tiles: ceil(M/64) x ceil(M/40) per site pair, M = 4 n_i n_j)
-        tiles = sum(-(-4 * a * b // 64) * -(-4 * a * b // 40) for a in s.norbs for b in s.norbs)
+        nc = s.norbs if sel is None else [len(x) for x in sel]
+        tiles = sum(-(-4 * a * b // 64) * -(-4 * a * b // 40) for a in nc for b in nc)
         ops = tiles * (last_units / 32.0) / con_n * 21 * 2 * 128 * 80 * 32
         tops = ops / (con_ms / con_n / 1e3) / 1e12
         roof["executed_int8"] = {"tops": tops, "peak_tops": 2.0 * peak, "frac": tops / (2.0 * peak),
@@ -348,7 +377,7 @@ def run_ours(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "s8 tensor-core slices + f64" if args.precision == "split" else "f64",
             "data": "synthetic (seeded Slater-Koster model, no external data)",
-            "config": {"workload": chi0_workload_desc(args, deck),
+            "config": {"workload": chi0_workload_desc(args, deck, omegas, reals),
                        "omegas_per_step": per, "precision": args.precision, "green": args.green,
                        "l2": "inputs larger than L2 (mesh 200+ MB, operands GBs per pass)"},
             "roofline": roof, "roofline_inversion": roof_inv, "gpu_launches": launches, "clocks": clocks}
@@ -368,7 +397,7 @@ def run_ours(args, rank, world, local_rank):
         e2e = run_e2e(gpu, deck, h0, omegas, reals, args, start + args.warmup * per, per, world)
         line["e2e"] = e2e
     if rank == 0 and not args.no_cpu and world == 1:
-        line["cpu_baseline"] = cpu_baseline(deck, h0, reals, omegas)
+        line["cpu_baseline"] = cpu_baseline(deck, h0, reals, omegas, sel=sel)
     gpu.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -390,7 +419,9 @@ def run_e2e(gpu, deck, h0, omegas, reals, args, start, per, world):
     rk = pinned(np.ascontiguousarray(deck.real_kp, np.float64))
     rw = pinned(np.ascontiguousarray(deck.real_w, np.float64))
     h0p = pinned(np.ascontiguousarray(h0, np.complex128).view(np.float64))
-    out = torch.empty((per, s.dimens, s.dimens * 2), dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
+    sel = chi_selection(args, s)
+    D = chi_dim(s, sel)
+    out = torch.empty((per, D, D * 2), dtype=torch.float64, pin_memory=True).numpy().view(np.complex128)
     gpu.profile(False)
     h2d = y.nbytes + kp.nbytes + w.nbytes + rk.nbytes + rw.nbytes + h0p.nbytes
     units = 0
@@ -399,6 +430,7 @@ def run_e2e(gpu, deck, h0, omegas, reals, args, start, per, world):
     for st in range(args.steps):
         idx = [(start + st * per + j) % len(omegas) for j in range(per)]
         gpu.set_system(s)
+        gpu.set_chi_orbitals(sel)
         gpu.set_h0(h0p.view(np.complex128).reshape(s.dimH, s.dimH))
         gpu.set_imag_mesh_arrays(y, kp.reshape(-1, 3), w)
         gpu.set_real_mesh(rk.reshape(-1, 3), rw)

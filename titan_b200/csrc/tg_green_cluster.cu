@@ -47,7 +47,7 @@ constexpr int kMaxCS = 9;        // cluster size (9 > 8: non-portable, enabled a
 constexpr int kMaxWarps = kMaxN / 32;
 
 struct ClSmem {
-  size_t colbuf, prow1, prow, pr, pinv, candv, candr, piv, phase, fs, blk, total;
+  size_t candrow, prow, pr, pinv, piv, phase, fs, blk, total;
 };
 
 __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -55,13 +55,10 @@ __host__ __device__ inline size_t al16(size_t x) { return (x + 15) & ~size_t(15)
 __host__ __device__ inline ClSmem cl_smem(int n, int n_neigh) {
   ClSmem L;
   size_t o = 0;
-  L.colbuf = o;  o = al16(o + sizeof(double2) * (size_t)n);
-  L.prow1 = o;   o = al16(o + sizeof(double2) * kPB);
+  L.candrow = o; o = al16(o + sizeof(double2) * 2 * kMaxWarps * (kPB + 1));
   L.prow = o;    o = al16(o + sizeof(double2) * kPB * kNLC);
   L.pr = o;      o = al16(o + sizeof(int) * kPB);
   L.pinv = o;    o = al16(o + sizeof(double2) * kPB);
-  L.candv = o;   o = al16(o + sizeof(double) * kMaxWarps);
-  L.candr = o;   o = al16(o + sizeof(int) * kMaxWarps);
   L.piv = o;     o = al16(o + sizeof(int) * (size_t)n);
   L.phase = o;   o = al16(o + sizeof(double2) * (size_t)(n_neigh > 0 ? n_neigh : 1));
   L.fs = o;      o = al16(o + sizeof(double2) * (size_t)kPB * n);
@@ -76,85 +73,88 @@ __host__ __device__ inline size_t ws_cluster_bytes(int n) {
 }
 
 struct ClState {
-  double* candv;
-  int* candr;
   int n, t;
   bool used;           // this thread's row has been a pivot row
   int my_step;         // step at which it became one
 };
 
-// |Re| + |Im| argmax over the CTA's unused rows (first index on ties); all threads call it
-__device__ __forceinline__ int cta_argmax(const ClState& st, double2 v) {
-  double best = (st.t < st.n && !st.used) ? fabs(v.x) + fabs(v.y) : -1.0;
-  int bi = st.t;
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    const double ob = __shfl_xor_sync(0xffffffffu, best, off);
-    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-    if (ob > best || (ob == best && oi < bi)) {
-      best = ob;
-      bi = oi;
-    }
-  }
-  const int warp = st.t >> 5, lane = st.t & 31;
-  if (lane == 0) {
-    st.candv[warp] = best;
-    st.candr[warp] = bi;
-  }
-  __syncthreads();
-  const int nw = (blockDim.x + 31) >> 5;
-  double b2 = -2.0;
-  int i2 = 0x7fffffff;
-  for (int w = 0; w < nw; ++w) {
-    const double cv = st.candv[w];
-    const int cr = st.candr[w];
-    if (cv > b2 || (cv == b2 && cr < i2)) {
-      b2 = cv;
-      i2 = cr;
-    }
-  }
-  return i2;
-}
-
 __device__ __forceinline__ double2 ldcg2(const double2* p) { return __ldcg(p); }
 
 // Phase 1 of the panel in slots s0 .. s0 + 7 of the CTA's block (its owner CTA only): nb
 // Gauss-Jordan steps on the panel's columns; the multipliers f_j (the column before step j)
-// go to F[j][row], 1 / a_rj and r_j to INV[j], R[j]
-__device__ __forceinline__ void factor_panel(ClState& st, double2* blk, int s0, double2* colbuf, double2* prow1,
-                                             double2* F, double2* INV, int* R, int nb, int* status, int64_t point) {
+// go to F[j][row], 1 / a_rj and r_j to INV[j], R[j].  One CTA barrier per step: every warp
+// reduces its best candidate row by shuffles and its winning lane posts that row's panel
+// entries (cand rows, two buffers by step parity); after the barrier every thread picks the
+// CTA-wide winner (largest |Re| + |Im|, smallest row on ties), scales the winner's posted
+// entries itself and updates its own row.
+__device__ __forceinline__ void factor_panel(ClState& st, double2* blk, int s0, double2* candrow, double2* F,
+                                             double2* INV, int* R, int nb, int* status, int64_t point) {
   const int t = st.t, n = st.n;
+  const int warp = t >> 5, lane = t & 31, nw = (blockDim.x + 31) >> 5;
   double2* row = blk + (size_t)s0 * n + t;   // row[s * n] = this thread's entry in slot s0 + s
-  for (int j = 0; j < nb; ++j) {
-    const double2 v = t < n ? row[(size_t)j * n] : make_double2(0, 0);
-    if (t < n) {
-      colbuf[t] = v;
-      F[(size_t)j * n + t] = v;
-    }
-    const int r = cta_argmax(st, v);   // its barrier also publishes colbuf
-    const double2 pv = colbuf[r];
-    if (pv.x == 0.0 && pv.y == 0.0 && t == 0) atomicMin(status, (int)(point + 1));
-    const double2 inv = crecip_fast(pv);
-    if (t == 0) {
-      INV[j] = inv;
-      R[j] = r;
-    }
-    if (t == r) {
+  double2 x[kPB];
 #pragma unroll
-      for (int s = 0; s < kPB; ++s) {
-        const double2 w = cmul(row[(size_t)s * n], inv);
-        prow1[s] = w;
-        row[(size_t)s * n] = w;
+  for (int s = 0; s < kPB; ++s) x[s] = t < n ? row[(size_t)s * n] : make_double2(0, 0);
+#pragma unroll
+  for (int j = 0; j < kPB; ++j) {
+    if (j < nb) {
+      const double2 v = x[j];
+      if (t < n) F[(size_t)j * n + t] = v;
+      double best = (t < n && !st.used) ? fabs(v.x) + fabs(v.y) : -1.0;
+      int bi = t;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
       }
-      row[(size_t)j * n] = inv;
-      st.used = true;
-    }
-    __syncthreads();
-    if (t < n && t != r) {
+      const int pb = j & 1;
+      double2* cw = candrow + (size_t)(pb * kMaxWarps + warp) * (kPB + 1);   // [value, row] + kPB entries
+      if (t == bi) {
+        cw[0] = make_double2(best, (double)bi);
 #pragma unroll
-      for (int s = 0; s < kPB; ++s) row[(size_t)s * n] = cfms(v, prow1[s], row[(size_t)s * n]);
-      row[(size_t)j * n] = cmul(make_double2(-v.x, -v.y), inv);
+        for (int s = 0; s < kPB; ++s) cw[1 + s] = x[s];
+      }
+      __syncthreads();
+      int wbest = 0;
+      double vb = -2.0;
+      int rb = 0x7fffffff;
+      for (int w = 0; w < nw; ++w) {
+        const double2 h = candrow[(size_t)(pb * kMaxWarps + w) * (kPB + 1)];
+        const int hr = (int)h.y;
+        if (h.x > vb || (h.x == vb && hr < rb)) {
+          vb = h.x;
+          rb = hr;
+          wbest = w;
+        }
+      }
+      const double2* pr = candrow + (size_t)(pb * kMaxWarps + wbest) * (kPB + 1) + 1;
+      const double2 pv = pr[j];
+      if (pv.x == 0.0 && pv.y == 0.0 && t == 0) atomicMin(status, (int)(point + 1));
+      const double2 inv = crecip_fast(pv);
+      if (t == 0) {
+        INV[j] = inv;
+        R[j] = rb;
+      }
+      if (t == rb) {
+#pragma unroll
+        for (int s = 0; s < kPB; ++s) x[s] = cmul(x[s], inv);
+        x[j] = inv;
+        st.used = true;
+      } else if (t < n) {
+#pragma unroll
+        for (int s = 0; s < kPB; ++s) x[s] = cfms(v, cmul(pr[s], inv), x[s]);
+        x[j] = cmul(make_double2(-v.x, -v.y), inv);
+      }
+      // buffer pb is posted again two steps later, after the next step's barrier
     }
+  }
+  if (t < n) {
+#pragma unroll
+    for (int s = 0; s < kPB; ++s) row[(size_t)s * n] = x[s];
   }
 }
 
@@ -191,8 +191,7 @@ __global__ void __launch_bounds__(kMaxN, 1) green_cluster_kernel(GreenArgs a, in
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = a.n;
   const ClSmem L = cl_smem(n, a.n_neigh);
-  double2* colbuf = reinterpret_cast<double2*>(smem + L.colbuf);
-  double2* prow1 = reinterpret_cast<double2*>(smem + L.prow1);
+  double2* candrow = reinterpret_cast<double2*>(smem + L.candrow);
   double2* prow = reinterpret_cast<double2*>(smem + L.prow);         // [kPB][kNLC]
   int* pr_s = reinterpret_cast<int*>(smem + L.pr);
   double2* pinv_s = reinterpret_cast<double2*>(smem + L.pinv);
@@ -201,8 +200,6 @@ __global__ void __launch_bounds__(kMaxN, 1) green_cluster_kernel(GreenArgs a, in
   double2* Fs = reinterpret_cast<double2*>(smem + L.fs);             // [kPB][n]
   double2* blk = reinterpret_cast<double2*>(smem + L.blk);           // [kNLC][n]
   ClState st;
-  st.candv = reinterpret_cast<double*>(smem + L.candv);
-  st.candr = reinterpret_cast<int*>(smem + L.candr);
   st.n = n;
   st.t = threadIdx.x;
   const int rank = (int)cl.block_rank();
@@ -289,7 +286,7 @@ __global__ void __launch_bounds__(kMaxN, 1) green_cluster_kernel(GreenArgs a, in
       const bool own = rank == owner;
       // ---- phase 1: the owner factorises the panel (slots 8 lp .. 8 lp + 7) ---------------
       if (own) {
-        factor_panel(st, blk, kPB * (P / cs), colbuf, prow1, Fb, INV + buf * kPB, R + buf * kPB, nb, a.status, pg);
+        factor_panel(st, blk, kPB * (P / cs), candrow, Fb, INV + buf * kPB, R + buf * kPB, nb, a.status, pg);
         __threadfence();
       }
       cl.sync();
@@ -362,7 +359,7 @@ __global__ void __launch_bounds__(kMaxN, 1) green_cluster_kernel(GreenArgs a, in
       const int col = piv[j];
       for (int r = t; r < n; r += blockDim.x) out[(int64_t)col * n + r] = blk[(size_t)ls * n + r];
     }
-    // the next point rewrites the block, colbuf and piv: this CTA is done with them
+    // the next point rewrites the block and piv: this CTA is done with them
     __syncthreads();
   }
 }
