@@ -385,7 +385,8 @@ def test_jij_two_sites_tilted_moments(gpu):
 
 def test_spectral_expectation_on_request(gpu, fe_deck):
     """TG_GREEN_SPECTRAL: occupations and moments from one eigendecomposition per k (the energy
-    sum folded per eigenvalue) equal the Gauss-Jordan ones to 1e-11 on the Fe golden state."""
+    sum folded per eigenvalue, eigenvectors re-orthonormalised, Rayleigh-quotient eigenvalues)
+    equal the Gauss-Jordan ones to 1e-12 on the Fe golden state (5.2e-13 measured)."""
     s = fe_deck.system
     st = fe_deck.state
     gpu.setup(fe_deck, s.h0(st))
@@ -395,8 +396,8 @@ def test_spectral_expectation_on_request(gpu, fe_deck):
         sp = gpu.expectation(st.Ef, s.eta)
     finally:
         gpu.set_green_method("auto")
-    for a, b in zip(sp, gj):
-        assert np.max(np.abs(a - b)) < 1e-11
+    dev = max(np.max(np.abs(a - b)) for a, b in zip(sp, gj))
+    assert dev < 1e-12, dev
 
 
 def test_gs_orbital_matches_oracle_and_fe_golden(gpu, fe_deck):
