@@ -97,23 +97,47 @@ class NewtonResult:
     converged: bool
 
 
-def newton(gpu, system, state0, fixEf=False, tol=1e-12, maxit=40):
+def newton(gpu, system, state0, fixEf=False, tol=1e-12, maxit=40, max_step=None, ftol=None):
     """Newton iteration x <- x - J(x)^-1 f(x) with the analytic GPU Jacobian.
 
     The mesh must already be on the context (tg_set_imag_mesh, and
     tg_set_real_mesh for the E_F column).  Converged when the step is below
-    tol * max(1, |x|) (the reference's mag_tol = 1e-12, :10).
+    tol * max(1, |x|) (the reference's mag_tol = 1e-12, :10), or, when ftol is given,
+    when max |f| <= ftol.
+
+    max_step globalises the iteration far from the fixed point, where the reference
+    relies on the trust region of SLATEC dnsqe (mod_dnsqe.F90): the Newton step is
+    scaled so that no unknown moves by more than max_step, then halved until
+    |f| decreases (|f(x + t dx)| <= (1 - 1e-4 t) |f(x)|, t >= 1/1024).  Near the
+    fixed point the full step is taken and this is the plain iteration.
     """
     x = unknowns_from_state(system, state0, fixEf)
     converged = False
     it = 0
+    f, _ = residual(gpu, system, x, state0, fixEf)   # leaves h0(x) on the context
     for it in range(1, maxit + 1):
-        f, _ = residual(gpu, system, x, state0, fixEf)   # leaves h0(x) on the context
+        if ftol is not None and np.max(np.abs(f)) <= ftol:
+            converged = True
+            it -= 1
+            break
         Ef = float(x[-1]) if not fixEf else state0.Ef
         J = gpu.jacobian(Ef, system.eta, fixEf)
         dx = np.linalg.solve(J, -f)
-        x = x + dx
-        if np.max(np.abs(dx)) <= tol * max(1.0, np.max(np.abs(x))):
+        t = 1.0
+        if max_step is not None:
+            t = min(1.0, max_step / max(np.max(np.abs(dx)), 1e-300))
+            n0 = np.linalg.norm(f)
+            while True:
+                fn, _ = residual(gpu, system, x + t * dx, state0, fixEf)
+                if np.linalg.norm(fn) <= (1.0 - 1e-4 * t) * n0 or t < 1.0 / 1024:
+                    break
+                t *= 0.5
+            x = x + t * dx
+            f = fn
+        else:
+            x = x + dx
+            f, _ = residual(gpu, system, x, state0, fixEf)
+        if np.max(np.abs(t * dx)) <= tol * max(1.0, np.max(np.abs(x))):
             converged = True
             break
     f, out = residual(gpu, system, x, state0, fixEf)
