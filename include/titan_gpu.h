@@ -91,6 +91,18 @@ int tg_chi0_batch(tg_ctx* ctx, const double* q, int n_omega, const double* e, do
  * 1 .. 16384; 0 restores the default (1024).  No counterpart in the reference. */
 int tg_set_split_chunk(tg_ctx* ctx, int points);
 
+/* chi0 for n_q wave vectors q(3, n_q) and n_omega frequencies (the loops of calculate_chi
+ * over q and e, calculate_chi.F90:61-73, around eintshechi):
+ *   chiorb_hf(dimens, dimens, n_omega, n_q), x2 / p2 as in tg_chi0_batch.
+ * G2 = G(k, z) does not depend on q: when the imaginary axis is not a tabulated uniform
+ * mesh (adaptive meshes, or H(k) tables above 8 GiB) every pass inverts and quantises it
+ * once and contracts it with G1(k + q, z + e) of every (q, e) (on the real axis once per
+ * frequency, since x2 depends on e); on tabulated meshes the q run one after another, each
+ * sharing G2 over its frequencies.  No counterpart in the reference. */
+int tg_chi0_qbatch(tg_ctx* ctx, int n_q, const double* q, int n_omega, const double* e, double Ef,
+                   double eta, double etap, int n_real, const double* x2, const double* p2,
+                   int precision, int dimens, double* chiorb_hf);
+
 /* Restricts chi0 (tg_chi0, tg_chi0_batch) to a subset of each site's orbitals:
  * mask(norb_max, n_atoms) flags the orbitals mu (both spins) that enter chi; null
  * restores every orbital (the reference's dimens = 4 sum_i nOrb_i^2).  With a mask,

@@ -423,3 +423,28 @@ def test_gs_orbital_multi_site(gpu):
     P = gpu.gs_orbital(s.Ef, s.eta)
     ref = O.gs_orbital(O.Model(s, h0), deck.ek, s.Ef, s.eta)
     assert np.max(np.abs(P - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_chi0_qbatch_on_an_adaptive_mesh(gpu, precision):
+    """tg_chi0_qbatch over three q (q = 0 among them) and two frequencies on a non-uniform
+    (E, k) list, where one G2 per pass serves every (q, e): equal to one tg_chi0 call per
+    (q, e) and to the oracle."""
+    from titan_b200.host.deck import Deck
+    base = synthetic.make_deck("bcc1", nk=(4, 4, 4), n1gl=6, parts=1, n3gl=4, mesh=False)
+    p = dict(base.params)
+    p["nk_per_energy"] = [64, 64, 27, 27, 8, 8]
+    deck = Deck.from_system(base.system, p, True)
+    s, h0 = _setup(gpu, deck)
+    qs = np.array([[0.0, 0.0, 0.0], [0.1, 0.0, 0.0], [0.05, 0.1, 0.2]])
+    es = [0.0, 0.04]
+    xs = [deck.real_points(e, s.Ef) for e in es]
+    got = gpu.chi0_qbatch(qs, es, s.Ef, s.eta, s.etap, [x[0] for x in xs], [x[1] for x in xs], precision)
+    m = O.Model(s, h0)
+    for iq, q in enumerate(qs):
+        for w, e in enumerate(es):
+            single = gpu.chi0(q, e, s.Ef, s.eta, s.etap, xs[w][0], xs[w][1], precision)
+            ref = O.eintshechi(m, deck.ek, (deck.real_kp, deck.real_w), q, e, s.Ef, s.eta, s.etap, xs[w][0],
+                               xs[w][1])
+            assert rel(got[iq, w], single) < (1e-12 if precision == "fp64" else 1e-9)
+            assert rel(got[iq, w], ref) < (1e-10 if precision == "fp64" else 1e-9)

@@ -1225,6 +1225,223 @@ int tg_chi0(tg_ctx* c, const double* q, double e, double Ef, double eta, double 
   return tg_chi0_batch(c, q, 1, &e, Ef, eta, etap, n_real, x2, p2, precision, dimens, chiorb_hf);
 }
 
+}  // extern "C"
+
+namespace {
+
+// chi0 for n_q wave vectors and n_omega frequencies with G2 shared by all of them: on meshes
+// without H(k) tables (adaptive imaginary axes, large real-axis BZs) G2 = G(k, z) does not
+// depend on q, so every pass inverts and quantises it once and contracts it with G1(k + q, z + e)
+// of every (q, e); on the real axis G2(k, x2 + i eta') depends on e (through x2) but not on q.
+// Accumulators: n_q x n_omega x nsplit chi-sized partials for each axis.
+int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double* e, double Ef, double eta,
+                 double etap, int n_real, bool split, double* chiorb_hf) {
+  cudaStream_t s = c->stream;
+  const ChiView v = chi_view(c);
+  const int n = c->dimH;
+  const int64_t nn = (int64_t)n * n;
+  const int64_t cstride = (int64_t)v.dimens * v.dimens;
+  const int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, (int64_t)n_real * c->n_realk), (int64_t)6 << 30);
+  const int nsplit = split ? split_nsplit((int)v.split->tiles.size(), c->num_sms, P / kSplitK) : nsplit_view(c, v);
+  const int64_t nacc = (int64_t)n_q * n_omega * nsplit * cstride;
+  int rc = TG_OK;
+  if (split) {
+    TG_CHECK(c, c->d_split_err.ensure(1), "alloc");
+    TG_CHECK(c, cudaMemsetAsync(c->d_split_err.p, 0, sizeof(int), s), "memset");
+  }
+  TG_CHECK(c, c->d_A.ensure((size_t)P * v.ld), "alloc A");
+  TG_CHECK(c, c->d_B.ensure((size_t)P * v.ld), "alloc B");
+  if (v.gather) TG_CHECK(c, c->d_graw.ensure((size_t)P * nn), "alloc G");
+  TG_CHECK(c, c->d_C.ensure((size_t)nacc), "alloc C");
+  TG_CHECK(c, c->d_D.ensure((size_t)nacc), "alloc D");
+  TG_CHECK(c, c->d_chi.ensure((size_t)cstride), "alloc chi");
+  TG_CHECK(c, cudaMemsetAsync(c->d_C.p, 0, sizeof(double2) * nacc, s), "memset");
+  TG_CHECK(c, cudaMemsetAsync(c->d_D.p, 0, sizeof(double2) * nacc, s), "memset");
+  auto acc_at = [&](double2* base, int iq, int w) { return base + ((size_t)iq * n_omega + w) * nsplit * cstride; };
+  if ((rc = reset_status(c))) return rc;
+  profile_begin(c);
+  cudaEvent_t* ev = c->ev;
+  TG_CHECK(c, cudaEventRecord(ev[0], s), "event");
+  auto contract_into = [&](const SplitPassDev& pd, int64_t np, double2* Cw) -> int {
+    if (split) {
+      KindTimer kt(c, 1);
+      return split_contract_pass(c, v, pd, Cw, nsplit, cstride);
+    }
+    KindTimer kt(c, 1);
+    return contract(c, v, c->d_A.p, c->d_B.p, np, Cw, nsplit, cstride);
+  };
+  // ---------------- imaginary axis: G2 once per pass ----------------
+  for (int64_t p0 = 0; p0 < c->n_imag; p0 += P) {
+    const int64_t np = std::min<int64_t>(P, c->n_imag - p0);
+    GreenArgs g2 = base_args(c);
+    g2.pts.kind = 0;
+    g2.pts.y = c->d_y.p;
+    g2.pts.kp = c->d_kp.p;
+    g2.pts.w = c->d_w.p;
+    g2.p0 = p0;
+    g2.np = np;
+    g2.zr = Ef;
+    g2.zi = etap;
+    g2.mode = MODE_B_IMAG;
+    g2.out = c->d_B.p;
+    {
+      KindTimer kt(c, 0);
+      if ((rc = chi_green(c, v, g2, "green (imag, G2)"))) return rc;
+    }
+    SplitPassDev pd;
+    if (split) {
+      KindTimer kq(c, 3);
+      const double* yv = c->h_y.data() + p0;
+      const SplitChunks ch = make_chunks(np, c->split_chunk, [&](int64_t i) { return yv[i]; });
+      if ((rc = split_prepare(c, v, ch, pd))) return rc;
+      if ((rc = split_quantize_operand(c, v, 1, c->d_B.p, pd, nullptr))) return rc;
+    }
+    for (int iq = 0; iq < n_q; ++iq)
+      for (int w = 0; w < n_omega; ++w) {
+        GreenArgs g1 = g2;
+        g1.zr = Ef + e[w];
+        g1.zi = eta;
+        g1.q[0] = qs[3 * iq]; g1.q[1] = qs[3 * iq + 1]; g1.q[2] = qs[3 * iq + 2];
+        g1.mode = MODE_A_IMAG;
+        g1.out = c->d_A.p;
+        {
+          KindTimer kt(c, 0);
+          if ((rc = chi_green(c, v, g1, "green (imag, G1)"))) return rc;
+        }
+        if (split) {
+          KindTimer kq(c, 3);
+          if ((rc = split_quantize_operand(c, v, 0, c->d_A.p, pd, nullptr))) return rc;
+        }
+        if ((rc = contract_into(pd, np, acc_at(c->d_C.p, iq, w)))) return rc;
+      }
+  }
+  // ---------------- real axis: G2 once per pass and frequency ----------------
+  for (int w = 0; w < n_omega; ++w) {
+    if (std::fabs(e[w]) < 1e-15) continue;
+    const int64_t ntot = (int64_t)n_real * c->n_realk;
+    for (int64_t p0 = 0; p0 < ntot; p0 += P) {
+      const int64_t np = std::min<int64_t>(P, ntot - p0);
+      GreenArgs gr = base_args(c);
+      gr.pts.kind = 1;
+      gr.pts.kp = c->d_rkp.p;
+      gr.pts.w = c->d_rw.p;
+      gr.pts.x2 = c->d_x2.p + (size_t)w * n_real;
+      gr.pts.p2 = c->d_p2.p + (size_t)w * n_real;
+      gr.pts.nk = c->n_realk;
+      gr.p0 = p0;
+      gr.np = np;
+      gr.zr = 0.0;
+      gr.zi = etap;
+      gr.mode = MODE_B_REAL;
+      gr.out = c->d_B.p;
+      {
+        KindTimer kt(c, 0);
+        if ((rc = chi_green(c, v, gr, "green (real, G2)"))) return rc;
+      }
+      SplitPassDev pr;
+      const int64_t nrk = c->n_realk, pbase = p0;
+      if (split) {
+        KindTimer kq(c, 3);
+        const SplitChunks ch = make_chunks(np, c->split_chunk, [&](int64_t i) { return (pbase + i) / nrk; });
+        if ((rc = split_prepare(c, v, ch, pr))) return rc;
+        if ((rc = split_quantize_operand(c, v, 1, c->d_B.p, pr, nullptr))) return rc;
+      }
+      for (int iq = 0; iq < n_q; ++iq) {
+        GreenArgs g1 = gr;
+        g1.zr = e[w];
+        g1.zi = eta;
+        g1.q[0] = qs[3 * iq]; g1.q[1] = qs[3 * iq + 1]; g1.q[2] = qs[3 * iq + 2];
+        g1.mode = MODE_A_REAL;
+        g1.out = c->d_A.p;
+        {
+          KindTimer kt(c, 0);
+          if ((rc = chi_green(c, v, g1, "green (real, G1)"))) return rc;
+        }
+        if (split) {
+          KindTimer kq(c, 3);
+          if ((rc = split_quantize_operand(c, v, 0, c->d_A.p, pr, nullptr))) return rc;
+        }
+        if ((rc = contract_into(pr, np, acc_at(c->d_D.p, iq, w)))) return rc;
+      }
+    }
+  }
+  TG_CHECK(c, cudaEventRecord(ev[5], s), "event");
+  // ---------------- epilogue per (q, frequency) ----------------
+  for (int iq = 0; iq < n_q; ++iq)
+    for (int w = 0; w < n_omega; ++w) {
+      KindTimer kt(c, 2);
+      TG_CHECK(c, launch_chi_epilogue(acc_at(c->d_C.p, iq, w), acc_at(c->d_D.p, iq, w), nsplit, cstride, v.dimens,
+                                      v.decode, v.norb, v.pair_coff, c->n_atoms, 1.0 / (2.0 * kPi), c->d_chi.p, s),
+               "epilogue");
+      TG_CHECK(c, cudaMemcpyAsync(chiorb_hf + 2 * ((size_t)iq * n_omega + w) * cstride, c->d_chi.p,
+                                  sizeof(double2) * cstride, cudaMemcpyDeviceToHost, s),
+               "copy chi");
+    }
+  TG_CHECK(c, cudaEventRecord(ev[6], s), "event");
+  TG_CHECK(c, cudaEventSynchronize(ev[6]), "sync");
+  float ms_tot = 0, ms_epi = 0;
+  cudaEventElapsedTime(&ms_tot, ev[0], ev[6]);
+  cudaEventElapsedTime(&ms_epi, ev[5], ev[6]);
+  c->last_ms[0] = 0.0;
+  c->last_ms[1] = ms_tot - ms_epi;
+  c->last_ms[2] = ms_epi;
+  c->last_ms[3] = ms_tot;
+  profile_end(c);
+  if ((rc = read_status(c))) return rc;
+  if (split) {
+    int err = 0;
+    TG_CHECK(c, cudaMemcpy(&err, c->d_split_err.p, sizeof(int), cudaMemcpyDeviceToHost), "split status");
+    if (err) {
+      char b[128];
+      snprintf(b, sizeof b, "split contraction: a bounded wait expired (site %d)", err);
+      return set_err(c, TG_ERR_TIMEOUT, b);
+    }
+  }
+  return TG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tg_chi0_qbatch(tg_ctx* c, int n_q, const double* q, int n_omega, const double* e, double Ef, double eta,
+                   double etap, int n_real, const double* x2, const double* p2, int precision, int dimens,
+                   double* chiorb_hf) {
+  int rc = check_ready(c, true, false);
+  if (rc) return rc;
+  if (n_q <= 0 || !q || !e || n_omega <= 0 || !chiorb_hf) return set_err(c, TG_ERR_ARG, "tg_chi0_qbatch: bad args");
+  const ChiView v = chi_view(c);
+  if (dimens != v.dimens) return set_err(c, TG_ERR_ARG, "tg_chi0_qbatch: dimens mismatch (see tg_set_chi_orbitals)");
+  if (precision != TG_PREC_FP64 && precision != TG_PREC_SPLIT)
+    return set_err(c, TG_ERR_ARG, "tg_chi0_qbatch: precision");
+  bool any_real = false;
+  for (int w = 0; w < n_omega; ++w) any_real |= std::fabs(e[w]) >= 1e-15;
+  if (any_real && (n_real <= 0 || !x2 || !p2)) return set_err(c, TG_ERR_ARG, "tg_chi0_qbatch: real-axis points missing");
+  if (any_real && !c->real_set) return set_err(c, TG_ERR_STATE, "tg_set_real_mesh has not been called");
+  const int64_t cstride = (int64_t)dimens * dimens;
+  // tabulated imaginary axes: H(k + q) tables and their eigendecompositions are per q, so
+  // the frequencies of one q share G2 and the q run one after another; otherwise one G2 per
+  // pass serves every q (both axes then sum H(k) inside the inversion kernels)
+  const bool tab_imag = c->imag_uniform && (int64_t)c->nk_u * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
+  if (n_q == 1 || tab_imag) {
+    double tot[4] = {0, 0, 0, 0};
+    for (int iq = 0; iq < n_q; ++iq) {
+      rc = tg_chi0_batch(c, q + 3 * iq, n_omega, e, Ef, eta, etap, n_real, x2, p2, precision, dimens,
+                         chiorb_hf + 2 * (size_t)iq * n_omega * cstride);
+      if (rc) return rc;
+      for (int k = 0; k < 4; ++k) tot[k] += c->last_ms[k];
+    }
+    for (int k = 0; k < 4; ++k) c->last_ms[k] = tot[k];
+    return TG_OK;
+  }
+  cudaSetDevice(c->device);
+  if (any_real) {
+    TG_CHECK(c, c->d_x2.upload(x2, (size_t)n_omega * n_real, c->stream), "upload x2");
+    TG_CHECK(c, c->d_p2.upload(p2, (size_t)n_omega * n_real, c->stream), "upload p2");
+  }
+  return chi0_qshared(c, n_q, q, n_omega, e, Ef, eta, etap, n_real, precision == TG_PREC_SPLIT, chiorb_hf);
+}
+
 int tg_last_timing(const tg_ctx* c, double* ms) {
   if (!c || !ms) return TG_ERR_ARG;
   for (int i = 0; i < 4; ++i) ms[i] = c->last_ms[i];

@@ -75,6 +75,8 @@ SIGNATURES = {
     "tg_set_chi_orbitals": (C.c_int, [C.c_void_p, _ip]),
     "tg_set_split_chunk": (C.c_int, [C.c_void_p, C.c_int]),
     "tg_gs_orbital": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _dp]),
+    "tg_chi0_qbatch": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_double, C.c_double, C.c_double, C.c_int,
+                                 _dp, _dp, C.c_int, C.c_int, _dp]),
     "tg_fp64_peak": (C.c_int, [C.c_void_p, _dp, _dp]),
     "tg_rcp_check": (C.c_int, [C.c_int64, _dp, _dp]),
     "tg_adjoint_vb_orbitals": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _ip, _dp]),
@@ -281,6 +283,25 @@ class GreenGPU:
                                     _PREC[precision], D, _p(buf.view(np.float64)))
         self._check(rc)
         return np.swapaxes(buf, 1, 2)      # Fortran (row, col) -> numpy [row, col]
+
+    def chi0_qbatch(self, qs, es, Ef, eta, etap, x2s=None, p2s=None, precision="fp64", out=None):
+        """chiorb_hf for every (q, e): [n_q, n_omega, dimens, dimens] (tg_chi0_qbatch)."""
+        qa = np.ascontiguousarray(np.asarray(qs, np.float64).reshape(-1, 3))
+        es = np.ascontiguousarray(es, np.float64)
+        nq, nw = qa.shape[0], es.shape[0]
+        nreal = max((len(x) for x in x2s), default=0) if x2s is not None else 0
+        X2 = np.zeros((nw, max(nreal, 1)))
+        P2 = np.zeros((nw, max(nreal, 1)))
+        if nreal:
+            for w in range(nw):
+                X2[w, :len(x2s[w])] = x2s[w]
+                P2[w, :len(p2s[w])] = p2s[w]
+        D = self.chi_dimens
+        buf = out if out is not None else np.empty((nq, nw, D, D), np.complex128)
+        rc = self.lib.tg_chi0_qbatch(self.h, nq, _p(qa), nw, _p(es), Ef, eta, etap, nreal, _p(X2), _p(P2),
+                                     _PREC[precision], D, _p(buf.view(np.float64)))
+        self._check(rc)
+        return np.swapaxes(buf, 2, 3)
 
     def she(self, q, e, Ef, eta, etap, x2, p2, efield, prefactor=None):
         """tchiorbiikl(q, e) as a [dimens, 4] numpy array (eintshe): prefactor . (1/2 pi) sum w df1iikl;
