@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--config", default="sq2")
     ap.add_argument("--omegas-per-step", type=int, default=0,
                     help="frequencies per step (0: 4, or 1 for slab16 whose frequency costs minutes)")
+    ap.add_argument("--qs-per-step", type=int, default=0,
+                    help="wave vectors per step along Gamma-X (tg_chi0_qbatch; 0: 2 for slab5, else 1 at q = 0)")
     ap.add_argument("--chi-orbitals", default="auto", choices=["auto", "all", "d"],
                     help="orbitals that enter chi (auto: d for slab16, the d-only chi of dimension 1600, else all)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -138,20 +140,28 @@ def units_of(deck, omegas_idx, reals):
     return sum(nimag + len(reals[i][0]) * nk for i in omegas_idx)
 
 
-def inversions_of(deck, per, reals, first):
+def inversions_of(deck, per, reals, first, nq=1, shared=False):
     """Matrix inversions in one step: G2 once per imaginary point (shared by the step's
-    frequencies), G1 per imaginary point and frequency (G1 = G2 at e = 0, q = 0), and
-    two per real-axis point."""
+    frequencies, and by its wave vectors when shared), G1 per imaginary point, frequency and
+    wave vector (G1 = G2 at e = 0, q = 0 on a single-q call), two per real-axis point (G2 of a
+    real-axis point shared by the wave vectors when shared)."""
     n_om = len(reals)
     idx = [(first + j) % n_om for j in range(per)]
     nimag = deck.ek.n_points
     nk = deck.real_kp.shape[0]
+    if shared:
+        inv = nimag
+        for i in idx:
+            inv += nq * nimag
+            if len(reals[i][0]):
+                inv += (1 + nq) * len(reals[i][0]) * nk
+        return inv
     inv = nimag
     for i in idx:
         if len(reals[i][0]) == 0 and i == idx[0]:
             continue
         inv += nimag + 2 * len(reals[i][0]) * nk
-    return inv
+    return nq * inv
 
 
 def peaks():
@@ -221,10 +231,31 @@ def chi0_workload_desc(args, deck, omegas, reals):
             f"energies, {len(omegas)} omega in [0,{max(omegas):.2g}], q=0")
 
 
+def qs_per_step(args):
+    if args.qs_per_step > 0:
+        return args.qs_per_step
+    return 2 if args.config == "slab5" else 1
+
+
+def q_grid(system, nq=16):
+    """nq wave vectors uniform along Gamma-X (X = b1 / 2): q_i = (i / nq) b1 / 2, i = 0 .. nq - 1."""
+    b1 = np.asarray(system.reciprocal()[0], float)
+    return [0.5 * i / nq * b1 for i in range(nq)]
+
+
+def step_qs(args, system, step):
+    """The wave vectors of one step: [0] when a step has one, else consecutive Gamma-X points."""
+    nq = qs_per_step(args)
+    if nq == 1 and args.config != "slab5":
+        return [np.zeros(3)]
+    grid = q_grid(system)
+    return [grid[(step * nq + j) % len(grid)] for j in range(nq)]
+
+
 def omegas_per_step(args):
     if args.omegas_per_step > 0:
         return args.omegas_per_step
-    return 1 if args.config == "slab16" else 4
+    return 1 if args.config in ("slab16", "slab5") else 4
 
 
 def run_reference(args, rank, world):
@@ -256,20 +287,26 @@ def run_reference(args, rank, world):
 
 
 # --------------------------------------------------------------------------- our arm
-def timed_steps(gpu, deck, h0, omegas, reals, steps, start, per, precision, prof=True):
-    """Run `steps` chi0_batch calls; returns (device ms list, units, launches)."""
+def timed_steps(gpu, deck, h0, omegas, reals, steps, start, per, precision, prof=True, args=None, step0=0):
+    """Run `steps` chi0 calls (tg_chi0_batch at q = 0, or tg_chi0_qbatch over the step's wave
+    vectors); returns (device ms list, units, launches, last timing)."""
     s = deck.system
     n_om = len(omegas)
     ms, units, launches = [], 0, 0
     for st in range(steps):
         idx = [(start + st * per + j) % n_om for j in range(per)]
         es = [float(omegas[i]) for i in idx]
-        gpu.chi0_batch(np.zeros(3), es, s.Ef, s.eta, s.etap, [reals[i][0] for i in idx],
-                       [reals[i][1] for i in idx], precision)
+        qs = step_qs(args, s, step0 + st) if args is not None else [np.zeros(3)]
+        if len(qs) == 1 and not np.any(qs[0]):
+            gpu.chi0_batch(np.zeros(3), es, s.Ef, s.eta, s.etap, [reals[i][0] for i in idx],
+                           [reals[i][1] for i in idx], precision)
+        else:
+            gpu.chi0_qbatch(np.array(qs), es, s.Ef, s.eta, s.etap, [reals[i][0] for i in idx],
+                            [reals[i][1] for i in idx], precision)
         t = gpu.last_timing()
         ms.append(t[3])
         launches += int(t[10])
-        units += units_of(deck, idx, reals)
+        units += len(qs) * units_of(deck, idx, reals)
     return ms, units, launches, t
 
 
@@ -311,13 +348,13 @@ def run_ours(args, rank, world, local_rank):
     per = omegas_per_step(args)
     start = rank * per * (args.steps + args.warmup)     # ranks take different frequencies
     # warm-up (untimed)
-    timed_steps(gpu, deck, h0, omegas, reals, args.warmup, start, per, args.precision)
+    timed_steps(gpu, deck, h0, omegas, reals, args.warmup, start, per, args.precision, args=args, step0=0)
     barrier(world)
     torch.cuda.synchronize()
     clk = ClockSampler(local_rank)
     clk.start()
     ms, units, launches, last = timed_steps(gpu, deck, h0, omegas, reals, args.steps, start + args.warmup * per, per,
-                                            args.precision)
+                                            args.precision, args=args, step0=args.warmup)
     torch.cuda.synchronize()
     clocks = clk.stop()
     barrier(world)
@@ -330,8 +367,9 @@ def run_ours(args, rank, world, local_rank):
     con_ms, con_n = last[6], last[7]
     grn_ms, grn_n = last[4], last[5]
     q_ms, q_n = last[11], last[12]
-    last_units = units_of(deck, [(start + args.warmup * per + (args.steps - 1) * per + j) % len(omegas)
-                                 for j in range(per)], reals)
+    nq = len(step_qs(args, s, args.warmup + args.steps - 1))
+    last_units = nq * units_of(deck, [(start + args.warmup * per + (args.steps - 1) * per + j) % len(omegas)
+                                      for j in range(per)], reals)
     pk, pk_kind = peaks()
     flops_con = 8.0 * D ** 2 * last_units
     achieved = flops_con / (con_ms / 1e3) / 1e12 if con_ms > 0 else None
@@ -364,16 +402,24 @@ def run_ours(args, rank, world, local_rank):
                                           "nominal dense int8 rate is twice the bf16 rate; int8 itself is not "
                                           "measured, so this is an estimate; ncu's tensor-pipe activity of the "
                                           "same kernel is in profiles/split_contract_sq2_small.md)"}
-    fp64_nominal = 37.0
-    roof_inv = {"bound": "fp64", "achieved": (8.0 * s.dimH ** 3 * inversions_of(deck, per, reals, start + args.warmup
-                                                                               * per + (args.steps - 1) * per))
-                / (grn_ms / 1e3) / 1e12 if grn_ms else None,
-                "peak": fp64_nominal, "unit": "TFLOP/s", "peak_source": "nominal B200 FP64 (not measured)",
-                "kernel": ("eig_jacobi_kernel + spec_green_kernel (spectral G, FP64 DMMA)" if args.green != "gauss-jordan"
-                           else "green_w1_kernel / green_team_kernel (fused H(k) + Gauss-Jordan)"),
-                "flops_per_inversion": 8.0 * s.dimH ** 3,
+    from titan_b200.native import fp64_peak
+    dfma, dmma = fp64_peak()
+    native_n = s.dimH in (4, 8, 16, 18, 20, 36, 40, 54, 72, 90)
+    tabulated = len(set(np.bincount(deck.ek.energy_index).tolist())) == 1   # every energy on the same k list
+    spectral = args.green != "gauss-jordan" and native_n and s.dimH <= 72 and tabulated
+    shared = nq > 1 and not tabulated
+    n_inv = inversions_of(deck, per, reals, start + args.warmup * per + (args.steps - 1) * per, nq, shared)
+    kname = ("eig_jacobi_kernel + spec_green_kernel (spectral G, FP64 DMMA)" if spectral else
+             "green_w1_kernel / green_team_kernel (fused H(k) + Gauss-Jordan)" if native_n else
+             "green_cluster_kernel (thread-block-cluster Gauss-Jordan) + gather_kernel")
+    peak64 = dmma if spectral else dfma
+    roof_inv = {"bound": "fp64", "achieved": (8.0 * s.dimH ** 3 * n_inv) / (grn_ms / 1e3) / 1e12 if grn_ms else None,
+                "peak": peak64, "unit": "TFLOP/s",
+                "peak_source": ("of measured FP64 DMMA (tg_fp64_peak, this run)" if spectral
+                                else "of measured FP64 DFMA (tg_fp64_peak, this run)"),
+                "kernel": kname, "flops_per_inversion": 8.0 * s.dimH ** 3, "inversions_last_step": n_inv,
                 "ms_last_step": grn_ms, "launches_in_last_step": int(grn_n)}
-    roof_inv["frac"] = roof_inv["achieved"] / fp64_nominal if roof_inv["achieved"] else None
+    roof_inv["frac"] = roof_inv["achieved"] / peak64 if roof_inv["achieved"] else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
@@ -382,14 +428,18 @@ def run_ours(args, rank, world, local_rank):
             "config": {"workload": chi0_workload_desc(args, deck, omegas, reals),
                        "omegas_per_step": per, "precision": args.precision, "green": args.green,
                        "l2": "inputs larger than L2 (mesh 200+ MB, operands GBs per pass)"},
-            "roofline": roof, "roofline_inversion": roof_inv, "gpu_launches": launches, "clocks": clocks}
+            "roofline": roof, "roofline_inversion": roof_inv, "gpu_launches": launches, "clocks": clocks,
+            "schedule": {"nsplit_autotuned": gpu.tuning()[1 if args.precision == "split" else 0],
+                         "split_chunk_points": 1024, "wave_vectors_per_step": nq,
+                         "g2_shared_across_q": bool(shared)}}
     if not args.no_compare_fp64 and args.precision != "fp64":
         # the FP64 arm of the metric: the same step (same frequencies as the last timed step) on the
         # plain FP64 path, device-timed the same way
         f0 = start + args.warmup * per + (args.steps - 1) * per
-        ms64, u64, _, _ = timed_steps(gpu, deck, h0, omegas, reals, 1, f0, per, "fp64")
+        ms64, u64, _, _ = timed_steps(gpu, deck, h0, omegas, reals, 1, f0, per, "fp64", args=args,
+                                      step0=args.warmup + args.steps - 1)
         line["fp64_path"] = {"value": u64 / (sum(ms64) / 1e3), "unit": UNIT, "ms_per_step": sum(ms64),
-                             "step": "one tg_chi0_batch call over the frequencies of the last timed step, "
+                             "step": "one chi0 call over the frequencies and wave vectors of the last timed step, "
                                      "TG_PREC_FP64 (FP64 SIMT contraction), same Green functions"}
         line["split_over_fp64"] = (value / world) / line["fp64_path"]["value"]
     if args.precision == "split" and not args.no_check:

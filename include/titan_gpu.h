@@ -84,6 +84,15 @@ int tg_chi0_batch(tg_ctx* ctx, const double* q, int n_omega, const double* e, do
                   double eta, double etap, int n_real, const double* x2, const double* p2,
                   int precision, int dimens, double* chiorb_hf);
 
+/* Autotuning of the chi0 contraction schedule (on by default): the first call for each
+ * contraction layout (precision, site-pair tiles, points per pass, chi dimension) times the
+ * K-range split counts 1, 2, 4, ..., 64 of its contraction kernel on one pass with CUDA
+ * events and keeps the fastest for the context's later calls; off uses the cost model
+ * alone (and forgets the measured choices).  tg_tuning reports the split counts of the
+ * last FP64 and split-precision calls.  No counterpart in the reference. */
+int tg_set_autotune(tg_ctx* ctx, int enable);
+int tg_tuning(const tg_ctx* ctx, int* nsplit_fp64, int* nsplit_split);
+
 /* Points per chunk of the split-precision contraction (TG_PREC_SPLIT): each energy's
  * points are cut into chunks of at most this many, and every operand element gets one
  * power-of-two scale per chunk, so shorter chunks follow the magnitude of G along the k

@@ -166,6 +166,11 @@ struct tg_ctx {
   // disturbance response (eintshe)
   DevArray<int> d_she_tab, d_ia, d_she_ztiles, d_she_rowoff;
   DevArray<double2> d_she_part, d_she_sum, d_she_pref, d_she_out;
+  // autotuned K-range split counts per contraction layout (precision, tiles, pass K-steps)
+  bool autotune = true;
+  std::vector<std::pair<std::vector<int64_t>, int>> tuned;
+  int last_nsplit[2] = {0, 0};   // FP64, split
+  DevArray<double2> d_tune;
   // split precision: points per chunk (one scale per operand element and chunk); 1024
   // keeps every 4 x 4 spin block holding >= 1e-8 of the largest within 1e-9 on the sq2
   // workload (6e-10 measured)
@@ -611,6 +616,72 @@ int split_contract_pass(tg_ctx* c, const ChiView& v, const SplitPassDev& pd, dou
   return TG_OK;
 }
 
+// K-range split count of the contraction of a pass of P points: the cost-model choice, or
+// with autotuning on, the fastest of 1, 2, 4, ..., 64 measured once per layout (precision,
+// tiles, K-steps of a pass) on zero operands (the kernels' time does not depend on the
+// values) with CUDA events, into scratch accumulators, and cached in the context
+int choose_nsplit(tg_ctx* c, const ChiView& v, bool split, int64_t P, int* out) {
+  const int model = split ? split_nsplit((int)v.split->tiles.size(), c->num_sms, P / kSplitK) : nsplit_view(c, v);
+  *out = model;
+  if (!c->autotune || P <= 0) {
+    c->last_nsplit[split ? 1 : 0] = model;
+    return TG_OK;
+  }
+  const std::vector<int64_t> key = {split ? 1 : 0, v.ntiles, (int64_t)(split ? v.split->tiles.size() : 0), P,
+                                    (int64_t)v.dimens, (int64_t)c->split_chunk};
+  for (auto& kv : c->tuned)
+    if (kv.first == key) {
+      *out = kv.second;
+      c->last_nsplit[split ? 1 : 0] = kv.second;
+      return TG_OK;
+    }
+  cudaStream_t s = c->stream;
+  const int64_t cstride = (int64_t)v.dimens * v.dimens;
+  SplitPassDev pd;
+  if (split) {
+    const int64_t chunk = c->split_chunk;
+    const SplitChunks ch = make_chunks(P, c->split_chunk, [&](int64_t i) { return i / chunk; });
+    int rc = split_prepare(c, v, ch, pd);
+    if (rc) return rc;
+    TG_CHECK(c, cudaMemsetAsync(c->d_digA.p, 0, c->d_digA.n, s), "memset");
+    TG_CHECK(c, cudaMemsetAsync(c->d_digB.p, 0, c->d_digB.n, s), "memset");
+    TG_CHECK(c, cudaMemsetAsync(c->d_EA.p, 0, sizeof(int) * c->d_EA.n, s), "memset");
+    TG_CHECK(c, cudaMemsetAsync(c->d_EB.p, 0, sizeof(int) * c->d_EB.n, s), "memset");
+    TG_CHECK(c, c->d_split_err.ensure(1), "alloc");
+    TG_CHECK(c, cudaMemsetAsync(c->d_split_err.p, 0, sizeof(int), s), "memset");
+  } else {
+    TG_CHECK(c, c->d_A.ensure((size_t)P * v.ld), "alloc A");
+    TG_CHECK(c, c->d_B.ensure((size_t)P * v.ld), "alloc B");
+    TG_CHECK(c, cudaMemsetAsync(c->d_A.p, 0, sizeof(double2) * P * v.ld, s), "memset");
+    TG_CHECK(c, cudaMemsetAsync(c->d_B.p, 0, sizeof(double2) * P * v.ld, s), "memset");
+  }
+  float best_ms = 0.f;
+  int best = model;
+  for (int ns = 1; ns <= 64; ns *= 2) {
+    if ((int64_t)ns * v.ntiles > (int64_t)64 * c->num_sms * 64) break;
+    TG_CHECK(c, c->d_tune.ensure((size_t)ns * cstride), "alloc tuning accumulators");
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {   // the first launch warms up
+      TG_CHECK(c, cudaMemsetAsync(c->d_tune.p, 0, sizeof(double2) * ns * cstride, s), "memset");
+      TG_CHECK(c, cudaEventRecord(c->ev[6], s), "event");
+      int rc = split ? split_contract_pass(c, v, pd, c->d_tune.p, ns, cstride)
+                     : contract(c, v, c->d_A.p, c->d_B.p, P, c->d_tune.p, ns, cstride);
+      if (rc) return rc;
+      TG_CHECK(c, cudaEventRecord(c->ev[7], s), "event");
+      TG_CHECK(c, cudaEventSynchronize(c->ev[7]), "sync");
+      TG_CHECK(c, cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]), "timing");
+    }
+    if (ns == 1 || ms < best_ms) {
+      best_ms = ms;
+      best = ns;
+    }
+  }
+  c->tuned.push_back({key, best});
+  c->last_nsplit[split ? 1 : 0] = best;
+  *out = best;
+  return TG_OK;
+}
+
 // Green functions of a chi0 pass into the operand buffers: fused (the kernel writes the
 // operand layouts), or gathered (column-major G into d_graw, then the view's slots)
 int chi_green(tg_ctx* c, const ChiView& v, const GreenArgs& g, const char* what) {
@@ -898,6 +969,20 @@ int tg_set_real_mesh(tg_ctx* c, int64_t n_k, const double* kp, const double* w) 
   return TG_OK;
 }
 
+int tg_set_autotune(tg_ctx* c, int enable) {
+  if (!c) return TG_ERR_ARG;
+  c->autotune = enable != 0;
+  if (!c->autotune) c->tuned.clear();
+  return TG_OK;
+}
+
+int tg_tuning(const tg_ctx* c, int* nsplit_fp64, int* nsplit_split) {
+  if (!c || !nsplit_fp64 || !nsplit_split) return TG_ERR_ARG;
+  *nsplit_fp64 = c->last_nsplit[0];
+  *nsplit_split = c->last_nsplit[1];
+  return TG_OK;
+}
+
 int tg_set_split_chunk(tg_ctx* c, int points) {
   if (!c) return TG_ERR_ARG;
   if (points < 0 || points > kSplitMaxChunk)
@@ -953,7 +1038,8 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   // pass over a tabulated mesh then holds ~2400 points per energy, so the split
   // contraction's chunk ends (one per energy and pass) cost little
   const int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, (int64_t)n_real * c->n_realk), (int64_t)6 << 30);
-  const int nsplit = split ? split_nsplit((int)v.split->tiles.size(), c->num_sms, P / kSplitK) : nsplit_view(c, v);
+  int nsplit = 1;
+  if ((rc = choose_nsplit(c, v, split, P, &nsplit))) return rc;
   if (split) {
     TG_CHECK(c, c->d_split_err.ensure(1), "alloc");
     TG_CHECK(c, c->d_e16A.ensure((size_t)P * nn), "alloc exponents A");
@@ -1242,9 +1328,10 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
   const int64_t nn = (int64_t)n * n;
   const int64_t cstride = (int64_t)v.dimens * v.dimens;
   const int64_t P = pass_size(c, std::max<int64_t>(c->n_imag, (int64_t)n_real * c->n_realk), (int64_t)6 << 30);
-  const int nsplit = split ? split_nsplit((int)v.split->tiles.size(), c->num_sms, P / kSplitK) : nsplit_view(c, v);
+  int nsplit = 1;
+  int rc = choose_nsplit(c, v, split, P, &nsplit);
+  if (rc) return rc;
   const int64_t nacc = (int64_t)n_q * n_omega * nsplit * cstride;
-  int rc = TG_OK;
   if (split) {
     TG_CHECK(c, c->d_split_err.ensure(1), "alloc");
     TG_CHECK(c, cudaMemsetAsync(c->d_split_err.p, 0, sizeof(int), s), "memset");

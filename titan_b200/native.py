@@ -78,6 +78,8 @@ SIGNATURES = {
     "tg_chi0_qbatch": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_double, C.c_double, C.c_double, C.c_int,
                                  _dp, _dp, C.c_int, C.c_int, _dp]),
     "tg_fp64_peak": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "tg_set_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "tg_tuning": (C.c_int, [C.c_void_p, _ip, _ip]),
     "tg_rcp_check": (C.c_int, [C.c_int64, _dp, _dp]),
     "tg_adjoint_vb_orbitals": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _ip, _dp]),
 }
@@ -215,6 +217,15 @@ class GreenGPU:
         self.dimens = system.dimens
         self.chi_dimens = system.dimens
         self.nmax = nmax
+
+    def set_autotune(self, enable=True):
+        self._check(self.lib.tg_set_autotune(self.h, 1 if enable else 0))
+
+    def tuning(self):
+        """(K-range splits of the last FP64 call, of the last split-precision call) (tg_tuning)."""
+        a, b = C.c_int(), C.c_int()
+        self._check(self.lib.tg_tuning(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def set_split_chunk(self, points=0):
         """Points per split-precision chunk (tg_set_split_chunk; 0 = default)."""
