@@ -314,7 +314,7 @@ def split_accuracy(gpu, deck, omegas, reals, per):
     """Split chi0 against the FP64 path on the full workload, untimed: the frequencies of one
     step (the largest ones, which carry the real-axis part too), worst one.  Normwise per 4 x 4
     spin block, max over blocks, and over the whole matrix."""
-    from titan_b200.host.accuracy import spin_block_errors
+    from titan_b200.host.accuracy import spin_block_errors, spin_block_table
     s = deck.system
     idx = list(range(len(omegas) - per, len(omegas)))
     es = [float(omegas[i]) for i in idx]
@@ -322,13 +322,17 @@ def split_accuracy(gpu, deck, omegas, reals, per):
     sp = gpu.chi0_batch(np.zeros(3), es, s.Ef, s.eta, s.etap, x2s, p2s, "split").copy()
     fp = gpu.chi0_batch(np.zeros(3), es, s.Ef, s.eta, s.etap, x2s, p2s, "fp64")
     per_w = [spin_block_errors(sp[w], fp[w], significant=1e-8) for w in range(len(idx))]
+    tables = [spin_block_table(sp[w], fp[w]) for w in range(len(idx))]
+    by_threshold = {t: [tables[0][t][0], max(tb[t][1] for tb in tables)] for t in tables[0]}
     return {"max": max(e[1] for e in per_w),
+            "max_by_block_size": by_threshold,
             "frobenius": max(e[2] for e in per_w),
             "max_incl_roundoff_zero_blocks": max(e[0] for e in per_w),
             "per_omega_max": [e[1] for e in per_w], "omegas": es, "nonzero_blocks": per_w[0][3],
             "measure": "max over 4x4 spin blocks b holding >= 1e-8 of the largest block norm of "
                        "||chi_split_b - chi_fp64_b||_F / ||chi_fp64_b||_F (the smaller blocks are zero by "
                        "symmetry up to FP64 roundoff; max_incl_roundoff_zero_blocks includes them); "
+                       "max_by_block_size: {threshold: [blocks holding >= threshold of the largest, max error]}; "
                        "frobenius: whole matrix; same calls, full mesh"}
 
 

@@ -25,3 +25,19 @@ def spin_block_errors(chi, ref, significant=1e-6):
     big = fn >= significant * fn.max()
     return (float(rel[nz].max()), float(rel[big].max()),
             float(np.linalg.norm(chi - ref) / np.linalg.norm(ref)), int(nz.sum()))
+
+
+def spin_block_table(chi, ref, thresholds=(1e-2, 1e-3, 1e-4, 1e-5, 1e-6, 1e-7, 1e-8)):
+    """{threshold: (blocks holding >= threshold of the largest block norm, max normwise error
+    over them)} for the 4 x 4 spin blocks of chi against ref."""
+    D = ref.shape[0]
+    nb = D // 4
+    f = np.asarray(ref).reshape(nb, 4, nb, 4)
+    d = (np.asarray(chi) - np.asarray(ref)).reshape(nb, 4, nb, 4)
+    fn = np.sqrt(np.einsum("iajb,iajb->ij", np.abs(f), np.abs(f)))
+    dn = np.sqrt(np.einsum("iajb,iajb->ij", np.abs(d), np.abs(d)))
+    out = {}
+    for t in thresholds:
+        sel = fn >= t * fn.max()
+        out[f"{t:.0e}"] = (int(sel.sum()), float(np.max(dn[sel] / fn[sel])))
+    return out
