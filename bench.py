@@ -49,6 +49,8 @@ def parse():
                     help="frequencies per step (0: 4, or 1 for slab16 whose frequency costs minutes)")
     ap.add_argument("--qs-per-step", type=int, default=0,
                     help="wave vectors per step along Gamma-X (tg_chi0_qbatch; 0: 2 for slab5, else 1 at q = 0)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="cost-model split counts only (no trial launches; for profiler launch lists)")
     ap.add_argument("--chi-orbitals", default="auto", choices=["auto", "all", "d"],
                     help="orbitals that enter chi (auto: d for slab16, the d-only chi of dimension 1600, else all)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -348,6 +350,7 @@ def run_ours(args, rank, world, local_rank):
     gpu.set_chi_orbitals(sel)
     D = chi_dim(s, sel)
     gpu.set_green_method(args.green)
+    gpu.set_autotune(not args.no_autotune)
     gpu.profile(True)
     per = omegas_per_step(args)
     start = rank * per * (args.steps + args.warmup)     # ranks take different frequencies

@@ -52,13 +52,17 @@ def split_product(a, b, max_level=5, chunk=None):
                    for s in range(0, a.shape[0], chunk))
     da, Ea, _ = quantise(a)
     db, Eb, _ = quantise(b)
+    # the digit products summed over the points stay below 2^14 npts < 2^53: float64 matrix
+    # products are exact here and run on BLAS
+    da = [x.astype(np.float64) for x in da]
+    db = [x.astype(np.float64) for x in db]
     out = np.zeros((a.shape[1], b.shape[1]))
     for lvl in range(max_level + 1):
         S = np.zeros_like(out)
         for i in range(NDIG):
             j = lvl - i
             if 0 <= j < NDIG:
-                S += (da[i].T @ db[j]).astype(np.float64)   # exact: |S| < 2^53 here
+                S += da[i].T @ db[j]
         out += np.ldexp(S, -12 - 8 * lvl)
     return np.ldexp(out, Ea[:, None] + Eb[None, :])
 

@@ -63,3 +63,27 @@ def test_noalloc_ignores_the_spectral_method():
                 assert np.max(np.abs(a - b)) < 1e-12
     finally:
         gpu.close()
+
+
+def test_noalloc_refuses_what_its_fixed_array_cannot_hold():
+    """The 16-layer slab (dimH 288) needs the cluster Gauss-Jordan kernel, which keeps its
+    Green functions in allocated memory: TG_ERR_ARG with a message, before any work, and
+    the context stays usable."""
+    from titan_b200.native import GreenGPU, TG_ERR_ARG
+    deck = synthetic.make_deck("slab16", nk=(2, 2, 1), n1gl=4, parts=1, n3gl=4)
+    s = deck.system
+    gpu = GreenGPU(0)
+    try:
+        gpu.setup(deck, s.h0(initial_state(s)))
+        nat, nmax = s.n_atoms, gpu.nmax
+        out = [np.zeros((nat, nmax)) for _ in range(4)]
+        mp = np.zeros((nat, nmax), np.complex128)
+        dp = C.POINTER(C.c_double)
+        rc = gpu.lib.tg_expectation_noalloc(gpu.h, s.Ef, s.eta, *[o.ctypes.data_as(dp) for o in out],
+                                            mp.view(np.float64).ctypes.data_as(dp))
+        assert rc == TG_ERR_ARG
+        assert b"dimension" in gpu.lib.tg_last_error(gpu.h)
+        green = gpu.green_batch(np.array([s.Ef + 0.1j]), np.zeros((1, 3)))
+        assert np.all(np.isfinite(green))
+    finally:
+        gpu.close()
