@@ -322,6 +322,7 @@ def split_accuracy(gpu, deck, omegas, reals, per):
     es = [float(omegas[i]) for i in idx]
     x2s, p2s = [reals[i][0] for i in idx], [reals[i][1] for i in idx]
     sp = gpu.chi0_batch(np.zeros(3), es, s.Ef, s.eta, s.etap, x2s, p2s, "split").copy()
+    bound = gpu.error_bound(len(es))
     fp = gpu.chi0_batch(np.zeros(3), es, s.Ef, s.eta, s.etap, x2s, p2s, "fp64")
     per_w = [spin_block_errors(sp[w], fp[w], significant=1e-8) for w in range(len(idx))]
     tables = [spin_block_table(sp[w], fp[w]) for w in range(len(idx))]
@@ -331,6 +332,10 @@ def split_accuracy(gpu, deck, omegas, reals, per):
             "frobenius": max(e[2] for e in per_w),
             "max_incl_roundoff_zero_blocks": max(e[0] for e in per_w),
             "per_omega_max": [e[1] for e in per_w], "omegas": es, "nonzero_blocks": per_w[0][3],
+            "error_bound": {"per_omega": [float(b) for b in bound],
+                            "basis": "tg_chi0_error_bound: worst-case normwise bound of the split format "
+                                     "(46-bit rounding per chunk scale + dropped digit products), relative "
+                                     "to ||chi||_F; compare with frobenius"},
             "measure": "max over 4x4 spin blocks b holding >= 1e-8 of the largest block norm of "
                        "||chi_split_b - chi_fp64_b||_F / ||chi_fp64_b||_F (the smaller blocks are zero by "
                        "symmetry up to FP64 roundoff; max_incl_roundoff_zero_blocks includes them); "

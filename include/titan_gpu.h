@@ -93,6 +93,17 @@ int tg_chi0_batch(tg_ctx* ctx, const double* q, int n_omega, const double* e, do
 int tg_set_autotune(tg_ctx* ctx, int enable);
 int tg_tuning(const tg_ctx* ctx, int* nsplit_fp64, int* nsplit_split);
 
+/* Error bound of the last tg_chi0 / tg_chi0_batch / tg_chi0_qbatch call (the err_est output
+ * of the chi0 boundary): bound[r] for each of its n results (n = n_omega, or n_omega * n_q,
+ * in the order of chiorb_hf) bounds ||chi_split - chi||_F / ||chi_split||_F, chi being the same
+ * sums in exact arithmetic, from the split format alone: each operand element rounded to
+ * 46 bits of its chunk's power-of-two scale, and the digit products the format drops.  A
+ * worst-case bound, accumulated per chunk and site pair on the device.  0 for TG_PREC_FP64
+ * results (the FP64 rounding that both paths share is not part of it); NaN after a call that
+ * failed.  n other than the last call's result count is TG_ERR_ARG.  No counterpart in the
+ * reference. */
+int tg_chi0_error_bound(tg_ctx* ctx, int n, double* bound);
+
 /* Points per chunk of the split-precision contraction (TG_PREC_SPLIT): each energy's
  * points are cut into chunks of at most this many, and every operand element gets one
  * power-of-two scale per chunk, so shorter chunks follow the magnitude of G along the k
@@ -105,9 +116,11 @@ int tg_set_split_chunk(tg_ctx* ctx, int points);
  *   chiorb_hf(dimens, dimens, n_omega, n_q), x2 / p2 as in tg_chi0_batch.
  * G2 = G(k, z) does not depend on q: when the imaginary axis is not a tabulated uniform
  * mesh (adaptive meshes, or H(k) tables above 8 GiB) every pass inverts and quantises it
- * once and contracts it with G1(k + q, z + e) of every (q, e) (on the real axis once per
- * frequency, since x2 depends on e); on tabulated meshes the q run one after another, each
- * sharing G2 over its frequencies.  No counterpart in the reference. */
+ * once and contracts it with G1(k + q, z + e) of every (q, e).  The real axis then uses
+ * spectral Green functions where the method and dimension allow (eigendecompositions of
+ * H(k) once and of H(k + q) once per q, for every frequency), else one inversion of G2 per
+ * pass and frequency shared by the q.  On tabulated meshes the q run one after another,
+ * each sharing G2 over its frequencies.  No counterpart in the reference. */
 int tg_chi0_qbatch(tg_ctx* ctx, int n_q, const double* q, int n_omega, const double* e, double Ef,
                    double eta, double etap, int n_real, const double* x2, const double* p2,
                    int precision, int dimens, double* chiorb_hf);
@@ -294,8 +307,8 @@ int tg_ldos(tg_ctx* ctx, int n_e, const double* e, double eta, double* ldosu, do
  *   TG_GREEN_GAUSS_JORDAN    Gauss-Jordan everywhere
  *   TG_GREEN_SPECTRAL        spectral wherever the mesh allows (tg_she ~4x faster,
  *                            tg_expectation one eigendecomposition per k for all energies)
- * Other meshes and dimensions always use Gauss-Jordan.  No counterpart in the
- * reference. */
+ * The eigendecomposition handles even dimH up to 96; other meshes and dimensions always
+ * use Gauss-Jordan.  No counterpart in the reference. */
 #define TG_GREEN_AUTO          0
 #define TG_GREEN_GAUSS_JORDAN  1
 #define TG_GREEN_SPECTRAL      2

@@ -184,14 +184,18 @@ def test_chi0_adaptive_mesh_matches_oracle(gpu):
     ("sq2", (5, 5, 1), 0.1, (0.05, 0.02, 0.0)),
 ])
 def test_chi0_split_matches_fp64_and_oracle(gpu, shape, nk, e, q):
-    """int8-sliced tensor-core contraction: normwise relative error <= 1e-9."""
+    """int8-sliced tensor-core contraction: normwise relative error <= 1e-9, and within the
+    format's error bound (tg_chi0_error_bound; FP64 rounding of either path on top)."""
     deck = synthetic.make_deck(shape, nk=nk, n1gl=8, parts=1, n3gl=6)
     s, h0 = _setup(gpu, deck)
     x2, p2 = deck.real_points(e, s.Ef)
     qv = np.array(q, float)
     sp = gpu.chi0(qv, e, s.Ef, s.eta, s.etap, x2, p2, precision="split")
+    bound = gpu.error_bound(1)[0]
     fp = gpu.chi0(qv, e, s.Ef, s.eta, s.etap, x2, p2, precision="fp64")
+    assert gpu.error_bound(1)[0] == 0.0
     assert rel(sp, fp) < 1e-9
+    assert 0.0 < bound < 1e-6 and rel(sp, fp) <= bound + 1e-13, (bound, rel(sp, fp))
     ref = O.eintshechi(O.Model(s, h0), deck.ek, (deck.real_kp, deck.real_w), qv, e, s.Ef, s.eta, s.etap, x2, p2)
     assert rel(sp, ref) < 1e-9
 
@@ -268,9 +272,10 @@ def test_nanoribbon_golden_through_gpu(gpu, precision):
                         assert abs(a - b) <= 1e-8 * abs(b), (kind, i, j, a, b)
 
 
-@pytest.mark.parametrize("shape", ["bcc1", "sq2", "bcc4"])
+@pytest.mark.parametrize("shape", ["bcc1", "sq2", "bcc4", "slab5"])
 def test_eig_batch_matches_eigh(gpu, shape):
-    """Jacobi eigendecomposition of H(k) behind the spectral Green functions."""
+    """Jacobi eigendecomposition of H(k) behind the spectral Green functions (at dimH 90 on
+    the packed upper triangle of the rotated matrix)."""
     deck = synthetic.make_deck(shape, mesh=False)
     s = deck.system
     h0 = s.h0(initial_state(s))
@@ -294,6 +299,8 @@ def test_eig_batch_matches_eigh(gpu, shape):
     ("sq2", (5, 5, 1), 0.1, (0.05, 0.02, 0.0), "fp64"),
     ("sq2", (5, 5, 1), 0.1, (0.0, 0.0, 0.0), "split"),
     ("bcc4", (2, 2, 2), 0.05, (0.0, 0.1, 0.0), "fp64"),
+    ("slab5", (3, 3, 1), 0.05, (0.1, 0.0, 0.0), "fp64"),
+    ("slab5", (3, 3, 1), 0.05, (0.0, 0.0, 0.0), "split"),
 ])
 def test_spectral_green_equals_gauss_jordan(gpu, shape, nk, e, q, precision):
     """chi0 with G from the eigendecomposition (default on uniform meshes) and from
@@ -440,6 +447,8 @@ def test_chi0_qbatch_on_an_adaptive_mesh(gpu, precision):
     es = [0.0, 0.04]
     xs = [deck.real_points(e, s.Ef) for e in es]
     got = gpu.chi0_qbatch(qs, es, s.Ef, s.eta, s.etap, [x[0] for x in xs], [x[1] for x in xs], precision)
+    bounds = gpu.error_bound(len(qs) * len(es)).reshape(len(qs), len(es))
+    assert np.all(bounds == 0.0) if precision == "fp64" else np.all((bounds > 0.0) & (bounds < 1e-6))
     m = O.Model(s, h0)
     for iq, q in enumerate(qs):
         for w, e in enumerate(es):
@@ -448,3 +457,33 @@ def test_chi0_qbatch_on_an_adaptive_mesh(gpu, precision):
                                xs[w][1])
             assert rel(got[iq, w], single) < (1e-12 if precision == "fp64" else 1e-9)
             assert rel(got[iq, w], ref) < (1e-10 if precision == "fp64" else 1e-9)
+            if precision == "split":   # the bound plus FP64 rounding of the sums
+                assert rel(got[iq, w], ref) <= bounds[iq, w] + 1e-11
+
+
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_chi0_qbatch_adaptive_slab5_spectral_real_axis(gpu, precision):
+    """dimH 90 on an adaptive imaginary axis: tg_chi0_qbatch inverts G2 once per pass for both
+    q and takes the real axis from eigendecompositions of H(k) and H(k + q); equal to the
+    same call with Gauss-Jordan everywhere and to the oracle."""
+    from titan_b200.host.deck import Deck
+    base = synthetic.make_deck("slab5", nk=(3, 3, 1), n1gl=4, parts=1, n3gl=4, mesh=False)
+    p = dict(base.params)
+    p["nk_per_energy"] = [9, 9, 4, 4]
+    deck = Deck.from_system(base.system, p, True)
+    s, h0 = _setup(gpu, deck)
+    qs = np.array([[0.0, 0.0, 0.0], [0.1, 0.05, 0.0]])
+    es = [0.03]
+    xs = [deck.real_points(e, s.Ef) for e in es]
+    x2, p2 = [x[0] for x in xs], [x[1] for x in xs]
+    got = gpu.chi0_qbatch(qs, es, s.Ef, s.eta, s.etap, x2, p2, precision)
+    try:
+        gpu.set_green_method("gauss-jordan")
+        gj = gpu.chi0_qbatch(qs, es, s.Ef, s.eta, s.etap, x2, p2, precision)
+    finally:
+        gpu.set_green_method("auto")
+    m = O.Model(s, h0)
+    for iq, q in enumerate(qs):
+        ref = O.eintshechi(m, deck.ek, (deck.real_kp, deck.real_w), q, es[0], s.Ef, s.eta, s.etap, x2[0], p2[0])
+        assert rel(got[iq, 0], gj[iq, 0]) < (1e-12 if precision == "fp64" else 1e-9)
+        assert rel(got[iq, 0], ref) < (1e-10 if precision == "fp64" else 1e-9)

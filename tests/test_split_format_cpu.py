@@ -151,3 +151,25 @@ def test_exponent_sidecar_gives_the_quantiser_the_same_scale():
             continue
         stored = np.ldexp(1.0, int(E) - 1)
         assert np.frexp(stored)[1] == np.frexp(m[chunk].max())[1]
+
+
+def test_error_bound_covers_every_entry():
+    """The per-point bound behind tg_chi0_error_bound: rounding to 46 bits of the chunk scale
+    plus the dropped digit products of levels i + j >= 6 stay within 6.02 2^(E_A + E_B - 46)
+    per point and real product, so every entry of a chunked product lies within the sum of
+    the bounds of its chunks (here with margin for the float64 reference's own rounding)."""
+    A, B = operands(npts=512)
+    chunk = 128
+    for a, b in ((A.real, B.real), (A.imag, B.real), (A.real, B.imag), (A.imag, B.imag)):
+        got = split_product(a, b, chunk=chunk)
+        ref = a.T @ b
+        bound = np.zeros_like(ref)
+        for s0 in range(0, a.shape[0], chunk):
+            _, Ea, _ = quantise(a[s0:s0 + chunk])
+            _, Eb, _ = quantise(b[s0:s0 + chunk])
+            live = np.outer(np.max(np.abs(a[s0:s0 + chunk]), axis=0) > 0, np.max(np.abs(b[s0:s0 + chunk]), axis=0) > 0)
+            bound += np.where(live, chunk * 6.02 * np.ldexp(1.0, Ea[:, None] + Eb[None, :] - 46), 0.0)
+        slack = 4e-16 * (np.abs(a).T @ np.abs(b))
+        assert np.all(np.abs(got - ref) <= bound + slack)
+        # and the bound is not vacuous: within three orders of the largest error
+        assert np.max(np.abs(got - ref)) > 1e-3 * np.max(bound)

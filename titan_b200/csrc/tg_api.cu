@@ -156,6 +156,7 @@ struct tg_ctx {
   int green_method = 0;   // TG_GREEN_AUTO / TG_GREEN_GAUSS_JORDAN / TG_GREEN_SPECTRAL
   DevArray<double2> d_eigU[4];
   DevArray<double> d_eigL[4];
+  DevArray<double2> d_hchunk;   // bounded H(k) scratch of eigendecompositions built chunk by chunk
   DevArray<int> d_outinv, d_eig_status;
   DevArray<double> d_ldos_e, d_ldos;
   // linear SOC: V, G V G of both Green functions, four operands, chi_lsoc partials
@@ -171,6 +172,10 @@ struct tg_ctx {
   std::vector<std::pair<std::vector<int64_t>, int>> tuned;
   int last_nsplit[2] = {0, 0};   // FP64, split
   DevArray<double2> d_tune;
+  // split-format error bound of the last chi0 call: per result [imaginary, real] x site pair
+  // sums, and the relative normwise bounds (0 for FP64 results)
+  DevArray<double> d_bound;
+  std::vector<double> err_bound;
   // split precision: points per chunk (one scale per operand element and chunk); 1024
   // keeps every 4 x 4 spin block holding >= 1e-8 of the largest within 1e-9 on the sq2
   // workload (6e-10 measured)
@@ -362,6 +367,49 @@ int build_eig(tg_ctx* c, int slot, int64_t nk) {
                          c->num_sms, c->stream),
            "eigendecomposition");
   return TG_OK;
+}
+
+// U and lambda of H(k + q) for a k list whose H table is not kept (too long to be resident):
+// the table is built and diagonalised in chunks of at most 2 GiB in a scratch buffer, and only
+// the eigendecompositions stay, in eigenvector slot `slot`
+int build_eig_chunked(tg_ctx* c, int slot, const double* d_k, int64_t nk, const double* q) {
+  const int64_t n = c->dimH, nn = n * n;
+  const int64_t kc = std::max<int64_t>(1, std::min<int64_t>(nk, ((int64_t)2 << 30) / (nn * 16)));
+  TG_CHECK(c, c->d_eigU[slot].ensure((size_t)nk * nn), "alloc eigenvectors");
+  TG_CHECK(c, c->d_eigL[slot].ensure((size_t)nk * n), "alloc eigenvalues");
+  TG_CHECK(c, c->d_hchunk.ensure((size_t)kc * nn), "alloc H chunk");
+  TG_CHECK(c, c->d_hphase.ensure((size_t)kc * std::max(c->n_neigh, 1)), "alloc phases");
+  TG_CHECK(c, c->d_qvec.upload(q, 3, c->stream), "upload q");
+  const GreenArgs a = base_args(c);
+  KindTimer kt(c, 0);
+  for (int64_t k0 = 0; k0 < nk; k0 += kc) {
+    const int64_t m = std::min(kc, nk - k0);
+    TG_CHECK(c, launch_hk_table(a, d_k + 3 * k0, m, c->d_qvec.p, c->d_hphase.p, c->d_hchunk.p, c->stream),
+             "H table");
+    TG_CHECK(c, launch_eig(c->d_hchunk.p, m, (int)n, c->d_eigU[slot].p + k0 * nn, c->d_eigL[slot].p + k0 * n,
+                           c->d_eig_status.p, c->num_sms, c->stream),
+             "eigendecomposition");
+    c->launches += 3;
+  }
+  return TG_OK;
+}
+
+// whether eigendecompositions of nk points in the eigenvector slots s0 and s1 (-1: none)
+// leave room: what they add to the current allocations within half the free device memory
+bool eig_room(tg_ctx* c, int64_t nk, int s0, int s1) {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
+  const size_t nn = (size_t)c->dimH * c->dimH;
+  double need = 0.0;
+  for (int sl : {s0, s1}) {
+    if (sl < 0) continue;
+    const size_t want = (size_t)nk * nn;
+    if (c->d_eigU[sl].n < want) need += (double)(want - c->d_eigU[sl].n) * sizeof(double2);
+    need += (double)nk * c->dimH * sizeof(double);
+  }
+  const size_t kc = std::min<size_t>((size_t)nk, std::max<size_t>(1, ((size_t)2 << 30) / (nn * 16)));
+  if (c->d_hchunk.n < kc * nn) need += (double)(kc * nn - c->d_hchunk.n) * sizeof(double2);
+  return need <= 0.5 * (double)fr;
 }
 
 int reset_eig_status(tg_ctx* c) {
@@ -590,8 +638,15 @@ int split_quantize_operand(tg_ctx* c, const ChiView& v, int which, const double2
   return TG_OK;
 }
 
+// bnd (null: none): the pass's quantisation bound per site pair, added into bnd[n_pairs]
 int split_contract_pass(tg_ctx* c, const ChiView& v, const SplitPassDev& pd, double2* Cpart, int nsplit,
-                        int64_t cstride) {
+                        int64_t cstride, double* bnd = nullptr) {
+  if (bnd) {
+    TG_CHECK(c, split_bound(c->d_m64A.p, c->d_m64B.p, v.ld, pd, v.pair_M, v.pair_aoff, c->n_atoms * c->n_atoms, bnd,
+                            c->stream),
+             "split bound");
+    c->launches += 1;
+  }
   SplitContractArgs sa;
   sa.A = c->d_digA.p;
   sa.B = c->d_digB.p;
@@ -613,6 +668,51 @@ int split_contract_pass(tg_ctx* c, const ChiView& v, const SplitPassDev& pd, dou
   sa.num_ctas = c->num_sms;
   c->launches += 1;
   TG_CHECK(c, split_contract(sa, c->stream), "contraction (split)");
+  return TG_OK;
+}
+
+// per-result accumulators of the split bound (results x [imaginary, real] x site pairs)
+int bound_begin(tg_ctx* c, bool split, int n_res) {
+  c->err_bound.assign((size_t)n_res, std::nan(""));   // until the call completes
+  if (!split) return TG_OK;
+  const size_t len = (size_t)n_res * 2 * c->n_atoms * c->n_atoms;
+  TG_CHECK(c, c->d_bound.ensure(len), "alloc bound");
+  TG_CHECK(c, cudaMemsetAsync(c->d_bound.p, 0, sizeof(double) * len, c->stream), "memset");
+  return TG_OK;
+}
+
+double* bound_at(tg_ctx* c, bool split, int res, int axis) {
+  return split ? c->d_bound.p + ((size_t)res * 2 + axis) * c->n_atoms * c->n_atoms : nullptr;
+}
+
+// after the results are on the host (stream synchronised): chi = (C_ij + conj C_ji - i D_ij) / 2 pi
+// entry by entry, so ||E_chi||_F <= (2 ||E_C||_F + ||E_D||_F) / 2 pi, and per site pair
+// ||E_C,t||_F <= 2 sqrt(2) 6.02 2^-46 sum_c count_c ||2^E_A|| ||2^E_B|| (a complex product is four
+// real products, each within 6.02 2^(E_A + E_B - 46) per point); relative to ||chi||_F of the
+// result as returned (FP64 accumulation rounding, which the FP64 path shares, not included)
+int bound_finish(tg_ctx* c, bool split, int n_res, int64_t cstride, const double* chiorb) {
+  if (!split) {
+    c->err_bound.assign((size_t)n_res, 0.0);
+    return TG_OK;
+  }
+  const int np2 = c->n_atoms * c->n_atoms;
+  std::vector<double> h((size_t)n_res * 2 * np2);
+  TG_CHECK(c, cudaMemcpy(h.data(), c->d_bound.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost), "copy bound");
+  const double kappa = 2.0 * std::sqrt(2.0) * 6.02 * std::ldexp(1.0, -46) / (2.0 * kPi);
+  for (int r = 0; r < n_res; ++r) {
+    double sc = 0.0, sd = 0.0;
+    for (int t = 0; t < np2; ++t) {
+      const double bc = h[((size_t)r * 2) * np2 + t], bd = h[((size_t)r * 2 + 1) * np2 + t];
+      sc += bc * bc;
+      sd += bd * bd;
+    }
+    const double err = kappa * (2.0 * std::sqrt(sc) + std::sqrt(sd));
+    double nrm = 0.0;
+    const double* x = chiorb + 2 * (size_t)r * cstride;
+    for (int64_t i = 0; i < 2 * cstride; ++i) nrm += x[i] * x[i];
+    nrm = std::sqrt(nrm);
+    c->err_bound[r] = err == 0.0 ? 0.0 : (nrm > 0.0 ? err / nrm : HUGE_VAL);
+  }
   return TG_OK;
 }
 
@@ -743,6 +843,7 @@ int tg_destroy(tg_ctx* c) {
   c->d_dy.free_(); c->d_piv.free_();
   c->d_ylist.free_(); c->d_klist_u.free_(); c->d_qvec.free_(); c->d_hphase.free_();
   for (int t = 0; t < 4; ++t) c->d_htab[t].free_();
+  c->d_hchunk.free_();
   for (int i = 0; i < 8; ++i)
     if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
@@ -983,6 +1084,14 @@ int tg_tuning(const tg_ctx* c, int* nsplit_fp64, int* nsplit_split) {
   return TG_OK;
 }
 
+int tg_chi0_error_bound(tg_ctx* c, int n, double* bound) {
+  if (!c) return TG_ERR_ARG;
+  if (!bound || n != (int)c->err_bound.size())
+    return set_err(c, TG_ERR_ARG, "tg_chi0_error_bound: n must be the number of results of the last chi0 call");
+  for (int i = 0; i < n; ++i) bound[i] = c->err_bound[i];
+  return TG_OK;
+}
+
 int tg_set_split_chunk(tg_ctx* c, int points) {
   if (!c) return TG_ERR_ARG;
   if (points < 0 || points > kSplitMaxChunk)
@@ -1046,6 +1155,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     TG_CHECK(c, c->d_e16B.ensure((size_t)P * nn), "alloc exponents B");
     TG_CHECK(c, cudaMemsetAsync(c->d_split_err.p, 0, sizeof(int), s), "memset");
   }
+  if ((rc = bound_begin(c, split, n_omega))) return rc;
   TG_CHECK(c, c->d_A.ensure((size_t)P * v.ld), "alloc A");
   TG_CHECK(c, c->d_B.ensure((size_t)P * v.ld), "alloc B");
   if (v.gather) TG_CHECK(c, c->d_graw.ensure((size_t)P * nn), "alloc G");
@@ -1080,18 +1190,26 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   // real-axis slots 2 / 3 alias the imaginary-axis slots 0 / 1 when the k lists coincide
   const bool alias_real = tab_imag && tab_real && real_k_is_imag_k(c);
   const int rslot0 = alias_real ? 0 : 2, rslot1 = alias_real ? 1 : 3;
-  if (tab_real && !alias_real) {
+  // a real-axis BZ of its own: spectral Green functions from eigendecompositions built out of
+  // bounded H chunks (only U and lambda are kept, so long BZs qualify too) when they fit in
+  // memory, else Gauss-Jordan on resident H tables when those fit
+  const bool eig_real = any_real && !alias_real && spec && eig_room(c, c->n_realk, 2, q_zero ? -1 : 3);
+  const bool tab_real_gj = tab_real && !alias_real && !eig_real;
+  const bool kmajor_real = alias_real || tab_real_gj || eig_real;
+  if (tab_real_gj) {
     if ((rc = build_htab(c, 2, c->d_rkp.p, c->n_realk, zero3))) return rc;
-    if (spec && (rc = build_eig(c, 2, c->n_realk))) return rc;
     if (!q_zero && (rc = build_htab(c, 3, c->d_rkp.p, c->n_realk, q))) return rc;
-    if (!q_zero && spec && (rc = build_eig(c, 3, c->n_realk))) return rc;
+  }
+  if (eig_real) {
+    if ((rc = build_eig_chunked(c, 2, c->d_rkp.p, c->n_realk, zero3))) return rc;
+    if (!q_zero && (rc = build_eig_chunked(c, 3, c->d_rkp.p, c->n_realk, q))) return rc;
   }
   auto use_table = [&](GreenArgs& g, int slot, int64_t n_e, int64_t nk, const double* ylist) {
-    g.htab = c->d_htab[slot].p;
+    g.htab = eig_real && slot >= 2 ? nullptr : c->d_htab[slot].p;
     g.n_e = n_e;
     g.nk_tab = nk;
     g.ylist = ylist;
-    if (spec) {
+    if (spec && (slot < 2 || eig_real)) {
       g.eigU = c->d_eigU[slot].p;
       g.eigL = c->d_eigL[slot].p;
       g.outinv = c->d_outinv.p;
@@ -1148,7 +1266,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
           if ((rc = split_quantize_operand(c, v, 0, c->d_A.p, pd, e16_g2 ? c->d_e16A.p : nullptr))) return rc;
         }
         KindTimer kt(c, 1);
-        rc = split_contract_pass(c, v, pd, c->d_C.p, nsplit, cstride);
+        rc = split_contract_pass(c, v, pd, c->d_C.p, nsplit, cstride, bound_at(c, split, 0, 0));
       } else {
         KindTimer kt(c, 1);
         rc = contract(c, v, c->d_A.p, c->d_B.p, np, c->d_C.p, nsplit, cstride);
@@ -1182,7 +1300,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
             rc = split_quantize_operand(c, v, 0, c->d_A.p, pd, e16_g1 ? c->d_e16A.p : nullptr);
           }
           KindTimer kt(c, 1);
-          if (!rc) rc = split_contract_pass(c, v, pd, Cw, nsplit, cstride);
+          if (!rc) rc = split_contract_pass(c, v, pd, Cw, nsplit, cstride, bound_at(c, split, w, 0));
         } else {
           KindTimer kt(c, 1);
           rc = contract(c, v, c->d_A.p, c->d_B.p, np, Cw, nsplit, cstride);
@@ -1220,7 +1338,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       gr.zi = etap;
       gr.mode = MODE_B_REAL;
       gr.out = c->d_B.p;
-      if (tab_real) use_table(gr, rslot0, n_real, c->n_realk, nullptr);
+      if (kmajor_real) use_table(gr, rslot0, n_real, c->n_realk, nullptr);
       const bool e16_rb = split && !v.gather && green_is_spectral(gr);
       gr.eout = e16_rb ? c->d_e16B.p : nullptr;
       {
@@ -1233,7 +1351,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       gr.q[0] = q[0]; gr.q[1] = q[1]; gr.q[2] = q[2];
       gr.mode = MODE_A_REAL;
       gr.out = c->d_A.p;
-      if (tab_real) {
+      if (kmajor_real) {
         use_table(gr, q_zero ? rslot0 : rslot1, n_real, c->n_realk, nullptr);
         gr.q[0] = gr.q[1] = gr.q[2] = 0.0;
       }
@@ -1250,7 +1368,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
           const int64_t nrk = c->n_realk, pbase = p0;
           {
             KindTimer kq(c, 3);
-            const SplitChunks ch = tab_real ? make_chunks_kmajor(pbase, np, n_real, c->split_chunk)
+            const SplitChunks ch = kmajor_real ? make_chunks_kmajor(pbase, np, n_real, c->split_chunk)
                                             : make_chunks(np, c->split_chunk,
                                                           [&](int64_t i) { return (pbase + i) / nrk; });
             rc = split_prepare(c, v, ch, pr);
@@ -1258,7 +1376,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
             if (!rc) rc = split_quantize_operand(c, v, 0, c->d_A.p, pr, e16_ra ? c->d_e16A.p : nullptr);
           }
           KindTimer kt(c, 1);
-          if (!rc) rc = split_contract_pass(c, v, pr, Dw, nsplit, cstride);
+          if (!rc) rc = split_contract_pass(c, v, pr, Dw, nsplit, cstride, bound_at(c, split, w, 1));
         } else {
           KindTimer kt(c, 1);
           rc = contract(c, v, c->d_A.p, c->d_B.p, np, Dw, nsplit, cstride);
@@ -1303,7 +1421,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       return set_err(c, TG_ERR_TIMEOUT, b);
     }
   }
-  return TG_OK;
+  return bound_finish(c, split, n_omega, cstride, chiorb_hf);
 }
 
 int tg_chi0(tg_ctx* c, const double* q, double e, double Ef, double eta, double etap, int n_real, const double* x2,
@@ -1318,7 +1436,8 @@ namespace {
 // chi0 for n_q wave vectors and n_omega frequencies with G2 shared by all of them: on meshes
 // without H(k) tables (adaptive imaginary axes, large real-axis BZs) G2 = G(k, z) does not
 // depend on q, so every pass inverts and quantises it once and contracts it with G1(k + q, z + e)
-// of every (q, e); on the real axis G2(k, x2 + i eta') depends on e (through x2) but not on q.
+// of every (q, e); on the real axis G2(k, x2 + i eta') depends on e (through x2) but not on q,
+// and with spectral Green functions every (q, e) forms it again from U(k) instead.
 // Accumulators: n_q x n_omega x nsplit chi-sized partials for each axis.
 int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double* e, double Ef, double eta,
                  double etap, int n_real, bool split, double* chiorb_hf) {
@@ -1344,15 +1463,16 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
   TG_CHECK(c, c->d_chi.ensure((size_t)cstride), "alloc chi");
   TG_CHECK(c, cudaMemsetAsync(c->d_C.p, 0, sizeof(double2) * nacc, s), "memset");
   TG_CHECK(c, cudaMemsetAsync(c->d_D.p, 0, sizeof(double2) * nacc, s), "memset");
+  if ((rc = bound_begin(c, split, n_q * n_omega))) return rc;
   auto acc_at = [&](double2* base, int iq, int w) { return base + ((size_t)iq * n_omega + w) * nsplit * cstride; };
   if ((rc = reset_status(c))) return rc;
   profile_begin(c);
   cudaEvent_t* ev = c->ev;
   TG_CHECK(c, cudaEventRecord(ev[0], s), "event");
-  auto contract_into = [&](const SplitPassDev& pd, int64_t np, double2* Cw) -> int {
+  auto contract_into = [&](const SplitPassDev& pd, int64_t np, double2* Cw, double* bnd) -> int {
     if (split) {
       KindTimer kt(c, 1);
-      return split_contract_pass(c, v, pd, Cw, nsplit, cstride);
+      return split_contract_pass(c, v, pd, Cw, nsplit, cstride, bnd);
     }
     KindTimer kt(c, 1);
     return contract(c, v, c->d_A.p, c->d_B.p, np, Cw, nsplit, cstride);
@@ -1399,11 +1519,90 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
           KindTimer kq(c, 3);
           if ((rc = split_quantize_operand(c, v, 0, c->d_A.p, pd, nullptr))) return rc;
         }
-        if ((rc = contract_into(pd, np, acc_at(c->d_C.p, iq, w)))) return rc;
+        if ((rc = contract_into(pd, np, acc_at(c->d_C.p, iq, w), bound_at(c, split, iq * n_omega + w, 0)))) return rc;
       }
   }
+  // ---------------- real axis, spectral ----------------
+  // the real-axis BZ is one k list for every energy: with its eigendecompositions (H(k) once,
+  // H(k + q) once per q, from bounded H chunks) G2 and G1 of every frequency are GEMMs per
+  // block of energies; G2 is formed again for each q, which costs far less than sharing an
+  // inversion per point
+  bool any_real = false;
+  for (int w = 0; w < n_omega; ++w) any_real |= std::fabs(e[w]) >= 1e-15;
+  const bool eig_real = any_real && spectral_on(c) && eig_room(c, c->n_realk, 2, 3);
+  if (eig_real) {
+    const double zero3[3] = {0.0, 0.0, 0.0};
+    const bool e16 = split && !v.gather;
+    if (e16) {
+      TG_CHECK(c, c->d_e16A.ensure((size_t)P * nn), "alloc exponents A");
+      TG_CHECK(c, c->d_e16B.ensure((size_t)P * nn), "alloc exponents B");
+    }
+    if ((rc = reset_eig_status(c))) return rc;
+    if ((rc = build_eig_chunked(c, 2, c->d_rkp.p, c->n_realk, zero3))) return rc;
+    auto use_eig = [&](GreenArgs& g, int slot) {
+      g.htab = nullptr;
+      g.n_e = n_real;
+      g.nk_tab = c->n_realk;
+      g.ylist = nullptr;
+      g.eigU = c->d_eigU[slot].p;
+      g.eigL = c->d_eigL[slot].p;
+      g.outinv = c->d_outinv.p;
+    };
+    const int64_t ntot = (int64_t)n_real * c->n_realk;
+    for (int iq = 0; iq < n_q; ++iq) {
+      const double* qi = qs + 3 * iq;
+      const bool qz = qi[0] == 0.0 && qi[1] == 0.0 && qi[2] == 0.0;
+      if (!qz && (rc = build_eig_chunked(c, 3, c->d_rkp.p, c->n_realk, qi))) return rc;
+      for (int w = 0; w < n_omega; ++w) {
+        if (std::fabs(e[w]) < 1e-15) continue;
+        for (int64_t p0 = 0; p0 < ntot; p0 += P) {
+          const int64_t np = std::min<int64_t>(P, ntot - p0);
+          GreenArgs gr = base_args(c);
+          gr.pts.kind = 1;
+          gr.pts.kp = c->d_rkp.p;
+          gr.pts.w = c->d_rw.p;
+          gr.pts.x2 = c->d_x2.p + (size_t)w * n_real;
+          gr.pts.p2 = c->d_p2.p + (size_t)w * n_real;
+          gr.pts.nk = c->n_realk;
+          gr.p0 = p0;
+          gr.np = np;
+          gr.zr = 0.0;
+          gr.zi = etap;
+          gr.mode = MODE_B_REAL;
+          gr.out = c->d_B.p;
+          gr.eout = e16 ? c->d_e16B.p : nullptr;
+          use_eig(gr, 2);
+          {
+            KindTimer kt(c, 0);
+            if ((rc = chi_green(c, v, gr, "green (real, G2)"))) return rc;
+          }
+          GreenArgs g1 = gr;
+          g1.zr = e[w];
+          g1.zi = eta;
+          g1.mode = MODE_A_REAL;
+          g1.out = c->d_A.p;
+          g1.eout = e16 ? c->d_e16A.p : nullptr;
+          use_eig(g1, qz ? 2 : 3);
+          {
+            KindTimer kt(c, 0);
+            if ((rc = chi_green(c, v, g1, "green (real, G1)"))) return rc;
+          }
+          SplitPassDev pr;
+          if (split) {
+            KindTimer kq(c, 3);
+            const SplitChunks ch = make_chunks_kmajor(p0, np, n_real, c->split_chunk);
+            if ((rc = split_prepare(c, v, ch, pr))) return rc;
+            if ((rc = split_quantize_operand(c, v, 1, c->d_B.p, pr, e16 ? c->d_e16B.p : nullptr))) return rc;
+            if ((rc = split_quantize_operand(c, v, 0, c->d_A.p, pr, e16 ? c->d_e16A.p : nullptr))) return rc;
+          }
+          if ((rc = contract_into(pr, np, acc_at(c->d_D.p, iq, w), bound_at(c, split, iq * n_omega + w, 1))))
+            return rc;
+        }
+      }
+    }
+  }
   // ---------------- real axis: G2 once per pass and frequency ----------------
-  for (int w = 0; w < n_omega; ++w) {
+  for (int w = 0; w < n_omega && !eig_real; ++w) {
     if (std::fabs(e[w]) < 1e-15) continue;
     const int64_t ntot = (int64_t)n_real * c->n_realk;
     for (int64_t p0 = 0; p0 < ntot; p0 += P) {
@@ -1448,7 +1647,8 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
           KindTimer kq(c, 3);
           if ((rc = split_quantize_operand(c, v, 0, c->d_A.p, pr, nullptr))) return rc;
         }
-        if ((rc = contract_into(pr, np, acc_at(c->d_D.p, iq, w)))) return rc;
+        if ((rc = contract_into(pr, np, acc_at(c->d_D.p, iq, w), bound_at(c, split, iq * n_omega + w, 1))))
+          return rc;
       }
     }
   }
@@ -1475,6 +1675,7 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
   c->last_ms[3] = ms_tot;
   profile_end(c);
   if ((rc = read_status(c))) return rc;
+  if (eig_real && (rc = read_eig_status(c))) return rc;
   if (split) {
     int err = 0;
     TG_CHECK(c, cudaMemcpy(&err, c->d_split_err.p, sizeof(int), cudaMemcpyDeviceToHost), "split status");
@@ -1484,7 +1685,7 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
       return set_err(c, TG_ERR_TIMEOUT, b);
     }
   }
-  return TG_OK;
+  return bound_finish(c, split, n_q * n_omega, cstride, chiorb_hf);
 }
 
 }  // namespace
@@ -1512,13 +1713,16 @@ int tg_chi0_qbatch(tg_ctx* c, int n_q, const double* q, int n_omega, const doubl
   const bool tab_imag = c->imag_uniform && (int64_t)c->nk_u * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
   if (n_q == 1 || tab_imag) {
     double tot[4] = {0, 0, 0, 0};
+    std::vector<double> bounds;
     for (int iq = 0; iq < n_q; ++iq) {
       rc = tg_chi0_batch(c, q + 3 * iq, n_omega, e, Ef, eta, etap, n_real, x2, p2, precision, dimens,
                          chiorb_hf + 2 * (size_t)iq * n_omega * cstride);
       if (rc) return rc;
       for (int k = 0; k < 4; ++k) tot[k] += c->last_ms[k];
+      bounds.insert(bounds.end(), c->err_bound.begin(), c->err_bound.end());
     }
     for (int k = 0; k < 4; ++k) c->last_ms[k] = tot[k];
+    c->err_bound = bounds;
     return TG_OK;
   }
   cudaSetDevice(c->device);

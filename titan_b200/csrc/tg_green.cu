@@ -506,7 +506,7 @@ int green_acc_ctas(int n, int64_t np, int num_sms) {
 }
 
 bool green_is_spectral(const GreenArgs& a) {
-  return a.eigU && a.eigL && a.htab && spectral_supported(a.mode, a.mode2, a.out2 != nullptr);
+  return a.eigU && a.eigL && a.n_e > 0 && spectral_supported(a.mode, a.mode2, a.out2 != nullptr);
 }
 
 cudaError_t launch_green(const GreenArgs& a, int num_sms, cudaStream_t s, int* grid_used) {
@@ -515,6 +515,9 @@ cudaError_t launch_green(const GreenArgs& a, int num_sms, cudaStream_t s, int* g
     return launch_green_spectral(a, a.eigU, a.eigL, a.outinv, num_sms, s);
   }
   if (a.eout || a.eout2) return cudaErrorInvalidValue;   // only the spectral kernel writes sidecars
+  // eigendecompositions without an H(k) table: the pass is k-major, which only the spectral
+  // kernel walks without a table
+  if (a.eigU && !a.htab) return cudaErrorInvalidValue;
   if (green_w1_supported(a.n, a.mode)) return launch_green_w1(a, num_sms, s, grid_used);
   if (green_warp_supported(a.n, a.mode)) return launch_green_warp(a, num_sms, s, grid_used);
   const Cfg* c = find_cfg(a.n);

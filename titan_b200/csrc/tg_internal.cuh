@@ -134,8 +134,9 @@ struct GreenArgs {
   int64_t n_e = 0;
   int64_t nk_tab = 0;
   const double* ylist = nullptr;     // imaginary parts of the energies (structured imaginary axis)
-  // optional eigendecomposition of every table row (spectral Green functions):
-  // eigU[k][r][a] row-major, eigL[k][a]; outinv[r*n + c] = pair-block slot of (r, c)
+  // optional eigendecomposition of every k of the k-major traversal (spectral Green
+  // functions; with or without htab): eigU[k][r][a] row-major, eigL[k][a];
+  // outinv[r*n + c] = pair-block slot of (r, c)
   const double2* eigU = nullptr;
   const double* eigL = nullptr;
   const int* outinv = nullptr;

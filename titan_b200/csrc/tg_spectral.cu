@@ -65,34 +65,82 @@ __device__ double block_sum(double v, double* red) {
   return t;
 }
 
+// The Hermitian working matrix A in shared memory: the full n x n array, or (PACKED, for n
+// whose A and U do not both fit) the upper triangle only, column by column:
+// A(i, j), i <= j, at j (j + 1) / 2 + i; A(j, i) = conj A(i, j).
+template <bool PACKED>
+struct HermA {
+  double2* a;
+  int n;
+  __device__ __forceinline__ double2 get(int i, int j) const {
+    if (!PACKED) return a[i * n + j];
+    return i <= j ? a[j * (j + 1) / 2 + i] : cconj(a[i * (i + 1) / 2 + j]);
+  }
+  // A(i, j) = v and A(j, i) = conj v
+  __device__ __forceinline__ void set(int i, int j, double2 v) const {
+    if (!PACKED) {
+      a[i * n + j] = v;
+      a[j * n + i] = cconj(v);
+    } else if (i <= j) {
+      a[j * (j + 1) / 2 + i] = v;
+    } else {
+      a[i * (i + 1) / 2 + j] = cconj(v);
+    }
+  }
+  __device__ __forceinline__ void set_diag(int i, double v) const {
+    a[PACKED ? i * (i + 1) / 2 + i : i * n + i] = make_double2(v, 0.0);
+  }
+  __device__ __forceinline__ static int64_t entries(int n) { return PACKED ? (int64_t)n * (n + 1) / 2 : (int64_t)n * n; }
+  // (i, j) of storage entry e (i <= j when PACKED)
+  __device__ __forceinline__ void ij(int e, int& i, int& j) const {
+    if (!PACKED) {
+      i = e / n;
+      j = e % n;
+      return;
+    }
+    j = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+    while (j * (j + 1) / 2 > e) --j;
+    while ((j + 1) * (j + 2) / 2 <= e) ++j;
+    i = e - j * (j + 1) / 2;
+  }
+};
+
+constexpr int kEigCols = 3;   // columns per lane of the post-pass row products: n <= 96
+
 // H: [nk][n][n] row-major (the H(k) table); U: [nk][n][n] row-major U[r][a]; lam: [nk][n]
+template <bool PACKED>
 __global__ void __launch_bounds__(kEigThreads) eig_jacobi_kernel(const double2* __restrict__ H, int64_t nk, int n,
                                                                  double2* __restrict__ Uout, double* __restrict__ lam,
                                                                  int* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int np = n / 2;
-  double2* A = reinterpret_cast<double2*>(smem);
-  double2* U = A + n * n;
+  const int64_t na = HermA<PACKED>::entries(n);
+  const HermA<PACKED> A{reinterpret_cast<double2*>(smem), n};
+  double2* U = A.a + na;
   Rot* rot = reinterpret_cast<Rot*>(U + n * n);
   double* red = reinterpret_cast<double*>(rot + np);
   for (int64_t k = blockIdx.x; k < nk; k += gridDim.x) {
     // A = (H + H^+) / 2: the table's H(k) is Hermitian up to rounding; the iteration keeps
     // A exactly Hermitian (upper blocks computed, lower blocks their conjugates)
     const double2* Hk = H + k * (int64_t)n * n;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-      const int r = e / n, c = e % n;
-      const double2 x = Hk[e], y = Hk[c * n + r];
-      A[e] = r == c ? make_double2(x.x, 0.0) : make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
-      U[e] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+    for (int e = threadIdx.x; e < na; e += blockDim.x) {
+      int r, c;
+      A.ij(e, r, c);
+      const double2 x = Hk[r * n + c], y = Hk[c * n + r];
+      A.a[e] = r == c ? make_double2(x.x, 0.0) : make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
     }
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) U[e] = make_double2(e / n == e % n ? 1.0 : 0.0, 0.0);
     __syncthreads();
     bool converged = false;
     for (int sweep = 0; sweep < kEigMaxSweeps; ++sweep) {
       double off = 0.0, tot = 0.0;
-      for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-        const double m2 = A[e].x * A[e].x + A[e].y * A[e].y;
+      for (int e = threadIdx.x; e < na; e += blockDim.x) {
+        int r, c;
+        A.ij(e, r, c);
+        // a stored off-diagonal entry of the packed form stands for two of the matrix
+        const double m2 = (A.a[e].x * A.a[e].x + A.a[e].y * A.a[e].y) * (PACKED && r != c ? 2.0 : 1.0);
         tot += m2;
-        if (e / n != e % n) off += m2;
+        if (r != c) off += m2;
       }
       off = block_sum(off, red);
       tot = block_sum(tot, red);
@@ -109,8 +157,8 @@ __global__ void __launch_bounds__(kEigThreads) eig_jacobi_kernel(const double2* 
         for (int kk = threadIdx.x; kk < np; kk += blockDim.x) {
           int p, q;
           rr_pair(s, kk, n, p, q);
-          const double a = A[p * n + p].x, d = A[q * n + q].x;
-          const double2 b = A[p * n + q];
+          const double a = A.get(p, p).x, d = A.get(q, q).x;
+          const double2 b = A.get(p, q);
           const double ab = hypot(b.x, b.y);
           Rot r;
           if (ab <= thr_b) {
@@ -138,17 +186,16 @@ __global__ void __launch_bounds__(kEigThreads) eig_jacobi_kernel(const double2* 
           rr_pair(s, k2, n, p2, q2);
           const Rot r1 = rot[k1], r2 = rot[k2];
           if (k1 == k2) {
-            const double a = A[p1 * n + p1].x, d = A[q1 * n + q1].x;
-            const double2 b = A[p1 * n + q1];
+            const double a = A.get(p1, p1).x, d = A.get(q1, q1).x;
+            const double2 b = A.get(p1, q1);
             const double ab = hypot(b.x, b.y);
             const double t = r1.s / r1.c;
-            A[p1 * n + p1] = make_double2(a - t * ab, 0.0);
-            A[q1 * n + q1] = make_double2(d + t * ab, 0.0);
-            A[p1 * n + q1] = make_double2(0.0, 0.0);
-            A[q1 * n + p1] = make_double2(0.0, 0.0);
+            A.set_diag(p1, a - t * ab);
+            A.set_diag(q1, d + t * ab);
+            A.set(p1, q1, make_double2(0.0, 0.0));
             continue;
           }
-          const double2 xpp = A[p1 * n + p2], xpq = A[p1 * n + q2], xqp = A[q1 * n + p2], xqq = A[q1 * n + q2];
+          const double2 xpp = A.get(p1, p2), xpq = A.get(p1, q2), xqp = A.get(q1, p2), xqq = A.get(q1, q2);
           const double2 e2c = cconj(r2.e);
           // X = A_blk J2
           const double2 ypq = cmul(e2c, xpq), yqq = cmul(e2c, xqq);
@@ -158,18 +205,10 @@ __global__ void __launch_bounds__(kEigThreads) eig_jacobi_kernel(const double2* 
           const double2 x11 = cadd(cscale(xqp, r2.s), cscale(yqq, r2.c));
           // J1^+ X: rows (c x0 - s e x1, s x0 + c e x1)
           const double2 z10 = cmul(r1.e, x10), z11 = cmul(r1.e, x11);
-          const double2 n00 = csub(cscale(x00, r1.c), cscale(z10, r1.s));
-          const double2 n01 = csub(cscale(x01, r1.c), cscale(z11, r1.s));
-          const double2 n10 = cadd(cscale(x00, r1.s), cscale(z10, r1.c));
-          const double2 n11 = cadd(cscale(x01, r1.s), cscale(z11, r1.c));
-          A[p1 * n + p2] = n00;
-          A[p1 * n + q2] = n01;
-          A[q1 * n + p2] = n10;
-          A[q1 * n + q2] = n11;
-          A[p2 * n + p1] = cconj(n00);
-          A[q2 * n + p1] = cconj(n01);
-          A[p2 * n + q1] = cconj(n10);
-          A[q2 * n + q1] = cconj(n11);
+          A.set(p1, p2, csub(cscale(x00, r1.c), cscale(z10, r1.s)));
+          A.set(p1, q2, csub(cscale(x01, r1.c), cscale(z11, r1.s)));
+          A.set(q1, p2, cadd(cscale(x00, r1.s), cscale(z10, r1.c)));
+          A.set(q1, q2, cadd(cscale(x01, r1.s), cscale(z11, r1.c)));
         }
         // U <- U J (columns p, q of every row)
         for (int e = threadIdx.x; e < n * np; e += blockDim.x) {
@@ -189,71 +228,88 @@ __global__ void __launch_bounds__(kEigThreads) eig_jacobi_kernel(const double2* 
     // the rotated A carries the rounding of every sweep; re-orthonormalised vectors and
     // Rayleigh-quotient eigenvalues together bring spectral occupations to the inversion's
     // accuracy (checked on a CPU emulation of this kernel: 1.3e-14 -> 4.4e-16 on Fe bcc).
-    //  (1) E = U^H U - 1 into A (the rotated matrix is no longer needed)
+    //  (1) E = U^H U - 1 into A (the rotated matrix is no longer needed; E is Hermitian)
     __syncthreads();
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-      const int i = e / n, j = e % n;
+    for (int e = threadIdx.x; e < na; e += blockDim.x) {
+      int i, j;
+      A.ij(e, i, j);
       double2 acc = make_double2(i == j ? -1.0 : 0.0, 0.0);
       for (int r = 0; r < n; ++r) acc = cfma(cconj(U[r * n + i]), U[r * n + j], acc);
-      A[e] = acc;
+      A.a[e] = acc;
     }
     __syncthreads();
     //  (2) one Newton-Schulz step U <- U (1 - E / 2): a warp per row, the row read before written
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    constexpr int kCols = 3;   // columns per lane (n <= 72 fits in shared memory)
     for (int r = warp; r < n; r += nwarps) {
-      double2 v[kCols];
+      double2 v[kEigCols];
 #pragma unroll
-      for (int m = 0; m < kCols; ++m) {
+      for (int m = 0; m < kEigCols; ++m) {
         v[m] = make_double2(0.0, 0.0);
         const int j = lane + 32 * m;
         if (j < n)
-          for (int i = 0; i < n; ++i) v[m] = cfma(U[r * n + i], A[i * n + j], v[m]);
+          for (int i = 0; i < n; ++i) v[m] = cfma(U[r * n + i], A.get(i, j), v[m]);
       }
       __syncwarp();
 #pragma unroll
-      for (int m = 0; m < kCols; ++m) {
+      for (int m = 0; m < kEigCols; ++m) {
         const int j = lane + 32 * m;
         if (j < n) U[r * n + j] = csub(U[r * n + j], cscale(v[m], 0.5));
       }
       __syncwarp();
     }
     __syncthreads();
-    //  (3) lambda_a = Re u_a^H Hs u_a with Hs = (H + H^H) / 2 from the table: W = Hs U row by
-    //      row into A (a warp per row, in place), then one thread per eigenvalue
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-      const int r = e / n, c = e % n;
-      const double2 x = Hk[e], y = Hk[c * n + r];
-      A[e] = r == c ? make_double2(x.x, 0.0) : make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
-    }
-    __syncthreads();
-    for (int r = warp; r < n; r += nwarps) {
-      double2 v[kCols];
-#pragma unroll
-      for (int m = 0; m < kCols; ++m) {
-        v[m] = make_double2(0.0, 0.0);
-        const int j = lane + 32 * m;
-        if (j < n)
-          for (int c = 0; c < n; ++c) v[m] = cfma(A[r * n + c], U[c * n + j], v[m]);
-      }
-      __syncwarp();
-#pragma unroll
-      for (int m = 0; m < kCols; ++m) {
-        const int j = lane + 32 * m;
-        if (j < n) A[r * n + j] = v[m];
-      }
-      __syncwarp();
+    //  (3) lambda_a = Re u_a^H Hs u_a with Hs = (H + H^H) / 2 from the table
+    for (int e = threadIdx.x; e < na; e += blockDim.x) {
+      int r, c;
+      A.ij(e, r, c);
+      const double2 x = Hk[r * n + c], y = Hk[c * n + r];
+      A.a[e] = r == c ? make_double2(x.x, 0.0) : make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
     }
     __syncthreads();
     double2* Uk = Uout + k * (int64_t)n * n;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) Uk[e] = U[e];
-    for (int a = threadIdx.x; a < n; a += blockDim.x) {
-      double l = 0.0;
-      for (int r = 0; r < n; ++r) {
-        const double2 u = U[r * n + a], w = A[r * n + a];
-        l = fma(u.x, w.x, fma(u.y, w.y, l));   // Re(conj(u) w)
+    if (!PACKED) {
+      // W = Hs U row by row into A (a warp per row, in place), then one thread per eigenvalue
+      for (int r = warp; r < n; r += nwarps) {
+        double2 v[kEigCols];
+#pragma unroll
+        for (int m = 0; m < kEigCols; ++m) {
+          v[m] = make_double2(0.0, 0.0);
+          const int j = lane + 32 * m;
+          if (j < n)
+            for (int c = 0; c < n; ++c) v[m] = cfma(A.a[r * n + c], U[c * n + j], v[m]);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < kEigCols; ++m) {
+          const int j = lane + 32 * m;
+          if (j < n) A.a[r * n + j] = v[m];
+        }
+        __syncwarp();
       }
-      lam[k * n + a] = l;
+      __syncthreads();
+      for (int e = threadIdx.x; e < n * n; e += blockDim.x) Uk[e] = U[e];
+      for (int a = threadIdx.x; a < n; a += blockDim.x) {
+        double l = 0.0;
+        for (int r = 0; r < n; ++r) {
+          const double2 u = U[r * n + a], w = A.a[r * n + a];
+          l = fma(u.x, w.x, fma(u.y, w.y, l));   // Re(conj(u) w)
+        }
+        lam[k * n + a] = l;
+      }
+    } else {
+      // no room for W: a warp per eigenvalue, lanes over the rows r of sum_r conj(u_r) (Hs u)_r
+      for (int e = threadIdx.x; e < n * n; e += blockDim.x) Uk[e] = U[e];
+      for (int a = warp; a < n; a += nwarps) {
+        double l = 0.0;
+        for (int r = lane; r < n; r += 32) {
+          double2 w = make_double2(0.0, 0.0);
+          for (int c = 0; c < n; ++c) w = cfma(A.get(r, c), U[c * n + a], w);
+          const double2 u = U[r * n + a];
+          l = fma(u.x, w.x, fma(u.y, w.y, l));
+        }
+        for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+        if (lane == 0) lam[k * n + a] = l;
+      }
     }
     __syncthreads();
   }
@@ -555,31 +611,44 @@ cudaError_t launch_spec_ldos(const double2* U, const double* lam, const double* 
   return cudaGetLastError();
 }
 
-size_t eig_smem_bytes(int n) {
-  return sizeof(double2) * 2 * (size_t)n * n + sizeof(Rot) * (size_t)(n / 2) + sizeof(double) * 32;
+size_t eig_smem_bytes_form(int n, bool packed) {
+  const size_t na = packed ? (size_t)n * (n + 1) / 2 : (size_t)n * n;
+  return sizeof(double2) * (na + (size_t)n * n) + sizeof(Rot) * (size_t)(n / 2) + sizeof(double) * 32;
 }
 
-int eig_supported(int n) {
-  if (n % 2 != 0 || n < 2) return 0;
+int eig_optin() {
   int dev = 0, optin = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
-  return eig_smem_bytes(n) <= (size_t)optin;
+  return optin;
+}
+
+// the full A when A and U both fit in shared memory, else the packed upper triangle
+bool eig_packed(int n, int optin) { return eig_smem_bytes_form(n, false) > (size_t)optin; }
+
+size_t eig_smem_bytes(int n) { return eig_smem_bytes_form(n, eig_packed(n, eig_optin())); }
+
+int eig_supported(int n) {
+  if (n % 2 != 0 || n < 2 || n > 32 * kEigCols) return 0;
+  const int optin = eig_optin();
+  return eig_smem_bytes_form(n, eig_packed(n, optin)) <= (size_t)optin;
 }
 
 cudaError_t launch_eig(const double2* H, int64_t nk, int n, double2* U, double* lam, int* status, int num_sms,
                        cudaStream_t s) {
   if (nk <= 0) return cudaSuccess;
-  if (n % 2 != 0 || n < 2) return cudaErrorInvalidValue;
-  const size_t smem = eig_smem_bytes(n);
-  cudaError_t e = cudaFuncSetAttribute(eig_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (!eig_supported(n)) return cudaErrorInvalidValue;
+  const bool packed = eig_packed(n, eig_optin());
+  const size_t smem = eig_smem_bytes_form(n, packed);
+  auto kernel = packed ? eig_jacobi_kernel<true> : eig_jacobi_kernel<false>;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eig_jacobi_kernel, kEigThreads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kEigThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm <= 0) return cudaErrorInvalidValue;
   const int64_t grid = std::min<int64_t>(nk, (int64_t)num_sms * per_sm);
-  eig_jacobi_kernel<<<(unsigned)grid, kEigThreads, smem, s>>>(H, nk, n, U, lam, status);
+  kernel<<<(unsigned)grid, kEigThreads, smem, s>>>(H, nk, n, U, lam, status);
   return cudaGetLastError();
 }
 
@@ -595,7 +664,7 @@ int spectral_supported(int mode, int mode2, bool has_out2) {
 cudaError_t launch_green_spectral(const GreenArgs& g, const double2* U, const double* lam, const int* outinv,
                                   int num_sms, cudaStream_t s) {
   if (g.np <= 0) return cudaSuccess;
-  if (!g.htab || g.n_e <= 0 || !U || !lam) return cudaErrorInvalidValue;
+  if (g.n_e <= 0 || !U || !lam) return cudaErrorInvalidValue;
   if (!spectral_supported(g.mode, g.mode2, g.out2 != nullptr)) return cudaErrorInvalidValue;
   if (g.out2 && !outinv) return cudaErrorInvalidValue;
   if ((g.eout || g.eout2) && g.n % 2) return cudaErrorInvalidValue;   // paired 4-byte exponent stores

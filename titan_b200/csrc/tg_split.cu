@@ -106,6 +106,41 @@ __device__ __forceinline__ void digits16(const long long (&x)[16], uint4 (&out)[
   for (int i = 2; i < kSplitSlices; ++i) out[i] = make_uint4(b[5 - i][0], b[5 - i][1], b[5 - i][2], b[5 - i][3]);
 }
 
+// Error bound of the format for one pass: for every site pair t (elements [aoff_t, aoff_t +
+// M_t) of both operands) bnd[t] += sum_c count[c] ||s_A(c, t)||_2 ||s_B(c, t)||_2, with
+// s_X(c, e) = 2^E the power of two above element e's maximum over chunk c (0 for a chunk of
+// zeros).  A warp per (chunk, pair).
+__device__ __forceinline__ double pow2_sq_above(unsigned long long bits) {
+  const double m = __longlong_as_double((long long)bits);
+  if (!(m > 0.0)) return 0.0;
+  int E = 0;
+  frexp(m, &E);
+  return ldexp(1.0, 2 * E);
+}
+
+__global__ void split_bound_kernel(const unsigned long long* __restrict__ m64A,
+                                   const unsigned long long* __restrict__ m64B, int64_t ld, int n_chunks,
+                                   const int* __restrict__ count, const int* __restrict__ pair_M,
+                                   const int* __restrict__ pair_aoff, int n_pairs, double* __restrict__ bnd) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int64_t items = (int64_t)n_chunks * n_pairs;
+  for (int64_t it = blockIdx.x * (int64_t)nw + warp; it < items; it += (int64_t)gridDim.x * nw) {
+    const int ch = (int)(it / n_pairs), t = (int)(it % n_pairs);
+    const int M = pair_M[t];
+    const int64_t base = (int64_t)ch * ld + pair_aoff[t];
+    double sa = 0.0, sb = 0.0;
+    for (int e = lane; e < M; e += 32) {
+      sa += pow2_sq_above(m64A[base + e]);
+      sb += pow2_sq_above(m64B[base + e]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      sa += __shfl_xor_sync(0xffffffffu, sa, o);
+      sb += __shfl_xor_sync(0xffffffffu, sb, o);
+    }
+    if (lane == 0 && sa > 0.0 && sb > 0.0) atomicAdd(bnd + t, (double)count[ch] * sqrt(sa) * sqrt(sb));
+  }
+}
+
 // one thread per (K-step t, k half kc, group g, row r < rows): 16 points of one
 // element, Re and Im parts
 __global__ void __launch_bounds__(256) split_quantize_kernel(
@@ -588,6 +623,16 @@ cudaError_t split_rowmax_e16(const int16_t* E16, int64_t ld, const SplitPassDev&
   if (ld % 2) return cudaErrorInvalidValue;
   const int gx = (kSplitMaxChunk + kRowmaxSlots - 1) / kRowmaxSlots;
   split_rowmax_e16_kernel<<<dim3(gx, p.n_chunks), 256, 0, s>>>(E16, ld, p.stride, p.slot0, p.count, M64);
+  return cudaGetLastError();
+}
+
+cudaError_t split_bound(const unsigned long long* m64A, const unsigned long long* m64B, int64_t ld,
+                        const SplitPassDev& p, const int* pair_M, const int* pair_aoff, int n_pairs, double* bnd,
+                        cudaStream_t s) {
+  if (p.n_chunks <= 0 || n_pairs <= 0) return cudaSuccess;
+  const int64_t warps = (int64_t)p.n_chunks * n_pairs;
+  const int blocks = (int)std::min<int64_t>((warps + 7) / 8, 148 * 8);
+  split_bound_kernel<<<blocks, 256, 0, s>>>(m64A, m64B, ld, p.n_chunks, p.count, pair_M, pair_aoff, n_pairs, bnd);
   return cudaGetLastError();
 }
 

@@ -89,6 +89,15 @@ cudaError_t split_rowmax(const double2* X, int64_t ld, const SplitPassDev& p, un
 cudaError_t split_rowmax_e16(const int16_t* E16, int64_t ld, const SplitPassDev& p, unsigned long long* M64,
                              cudaStream_t s);
 
+// Quantisation bound of a pass (the chunk maxima M64 of both operands, before the next pass
+// overwrites them): bnd[t] += sum_c count[c] ||2^E_A(c, t)|| ||2^E_B(c, t)|| per site pair t.
+// Per point and real product the format's error is below 6.02 2^(E_A + E_B - 46): rounding to
+// 46 bits, 2^(E_A + E_B - 46), plus the digit products of levels i + j >= 6 it drops,
+// (5 2^46 + 2^40 + 3 2^30 + 2^23 + 2^14) 2^(E_A + E_B - 92) with balanced digits |d| <= 128.
+cudaError_t split_bound(const unsigned long long* m64A, const unsigned long long* m64B, int64_t ld,
+                        const SplitPassDev& p, const int* pair_M, const int* pair_aoff, int n_pairs, double* bnd,
+                        cudaStream_t s);
+
 // digits of one operand for a pass; writes E[c * ld + e] for every valid element
 cudaError_t split_quantize(const double2* X, int64_t ld, const SplitPassDev& p, const SplitGroup* groups,
                            int n_groups, int rows, const unsigned long long* M64, int* E, int8_t* dig,

@@ -80,6 +80,7 @@ SIGNATURES = {
     "tg_fp64_peak": (C.c_int, [C.c_void_p, _dp, _dp]),
     "tg_set_autotune": (C.c_int, [C.c_void_p, C.c_int]),
     "tg_tuning": (C.c_int, [C.c_void_p, _ip, _ip]),
+    "tg_chi0_error_bound": (C.c_int, [C.c_void_p, C.c_int, _dp]),
     "tg_rcp_check": (C.c_int, [C.c_int64, _dp, _dp]),
     "tg_adjoint_vb_orbitals": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _ip, _dp]),
 }
@@ -226,6 +227,13 @@ class GreenGPU:
         a, b = C.c_int(), C.c_int()
         self._check(self.lib.tg_tuning(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def error_bound(self, n):
+        """Relative normwise bound of the split format for each of the n results of the last
+        chi0 call (0 for FP64 results; tg_chi0_error_bound)."""
+        out = np.zeros(int(n))
+        self._check(self.lib.tg_chi0_error_bound(self.h, int(n), out.ctypes.data_as(_dp)))
+        return out
 
     def set_split_chunk(self, points=0):
         """Points per split-precision chunk (tg_set_split_chunk; 0 = default)."""
