@@ -142,11 +142,12 @@ def units_of(deck, omegas_idx, reals):
     return sum(nimag + len(reals[i][0]) * nk for i in omegas_idx)
 
 
-def inversions_of(deck, per, reals, first, nq=1, shared=False):
-    """Matrix inversions in one step: G2 once per imaginary point (shared by the step's
+def inversions_of(deck, per, reals, first, nq=1, shared=False, real_per_q=False):
+    """Green functions formed in one step: G2 once per imaginary point (shared by the step's
     frequencies, and by its wave vectors when shared), G1 per imaginary point, frequency and
     wave vector (G1 = G2 at e = 0, q = 0 on a single-q call), two per real-axis point (G2 of a
-    real-axis point shared by the wave vectors when shared)."""
+    real-axis point shared by the wave vectors when shared, unless the real axis is spectral
+    (real_per_q), where every wave vector forms its own G2)."""
     n_om = len(reals)
     idx = [(first + j) % n_om for j in range(per)]
     nimag = deck.ek.n_points
@@ -156,7 +157,7 @@ def inversions_of(deck, per, reals, first, nq=1, shared=False):
         for i in idx:
             inv += nq * nimag
             if len(reals[i][0]):
-                inv += (1 + nq) * len(reals[i][0]) * nk
+                inv += (2 * nq if real_per_q else 1 + nq) * len(reals[i][0]) * nk
         return inv
     inv = nimag
     for i in idx:
@@ -408,26 +409,33 @@ def run_ours(args, rank, world, local_rank):
         tiles = sum(-(-4 * a * b // 64) * -(-4 * a * b // 40) for a in nc for b in nc)
         ops = tiles * (last_units / 32.0) / con_n * 21 * 2 * 128 * 80 * 32
         tops = ops / (con_ms / con_n / 1e3) / 1e12
-        roof["executed_int8"] = {"tops": tops, "peak_tops": 2.0 * peak, "frac": tops / (2.0 * peak),
+        roof["executed_int8"] = {"tops": tops, "nominal_dense_tops": 4500.0, "frac_of_nominal": tops / 4500.0,
+                                 "frac_of_2x_measured_bf16": tops / (2.0 * peak),
                                  "basis": "int8 MMA ops issued per launch (K-step padding not counted) / "
-                                          "launch time; peak = 2 x the measured sustained bf16 rate (the "
-                                          "nominal dense int8 rate is twice the bf16 rate; int8 itself is not "
-                                          "measured, so this is an estimate; ncu's tensor-pipe activity of the "
-                                          "same kernel is in profiles/split_contract_sq2_small.md)"}
+                                          "launch time, against the nominal dense int8 rate (4.5 POPS); that "
+                                          "fraction is the one to set beside ncu's sm__pipe_tensor_cycles_active "
+                                          "of the kernel (profiles/split_contract_sq2_small.md). Twice the "
+                                          "measured bf16 rate is below the nominal int8 rate because the bf16 "
+                                          "GEMM it comes from runs at the power cap"}
     from titan_b200.native import fp64_peak
     dfma, dmma = fp64_peak()
     native_n = s.dimH in (4, 8, 16, 18, 20, 36, 40, 54, 72, 90)
     tabulated = len(set(np.bincount(deck.ek.energy_index).tolist())) == 1   # every energy on the same k list
-    spectral = args.green != "gauss-jordan" and native_n and s.dimH <= 72 and tabulated
+    eig_ok = args.green != "gauss-jordan" and s.dimH % 2 == 0 and s.dimH <= 96   # the Jacobi kernel's range
+    spectral = eig_ok and tabulated
     shared = nq > 1 and not tabulated
-    n_inv = inversions_of(deck, per, reals, start + args.warmup * per + (args.steps - 1) * per, nq, shared)
+    spectral_real = eig_ok and (tabulated or shared)   # the real-axis BZ is one k list for every energy
+    n_inv = inversions_of(deck, per, reals, start + args.warmup * per + (args.steps - 1) * per, nq, shared,
+                          spectral_real and shared)
     kname = ("eig_jacobi_kernel + spec_green_kernel (spectral G, FP64 DMMA)" if spectral else
+             "green_w1_kernel / green_team_kernel (imaginary axis, Gauss-Jordan) + eig_jacobi_kernel + "
+             "spec_green_kernel (real axis, spectral)" if spectral_real else
              "green_w1_kernel / green_team_kernel (fused H(k) + Gauss-Jordan)" if native_n else
              "green_cluster_kernel (thread-block-cluster Gauss-Jordan) + gather_kernel")
-    peak64 = dmma if spectral else dfma
+    peak64 = dmma if spectral or spectral_real else dfma
     roof_inv = {"bound": "fp64", "achieved": (8.0 * s.dimH ** 3 * n_inv) / (grn_ms / 1e3) / 1e12 if grn_ms else None,
                 "peak": peak64, "unit": "TFLOP/s",
-                "peak_source": ("of measured FP64 DMMA (tg_fp64_peak, this run)" if spectral
+                "peak_source": ("of measured FP64 DMMA (tg_fp64_peak, this run)" if spectral or spectral_real
                                 else "of measured FP64 DFMA (tg_fp64_peak, this run)"),
                 "kernel": kname, "flops_per_inversion": 8.0 * s.dimH ** 3, "inversions_last_step": n_inv,
                 "ms_last_step": grn_ms, "launches_in_last_step": int(grn_n)}

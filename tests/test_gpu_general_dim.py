@@ -141,3 +141,25 @@ def test_dyson_at_the_d_only_dimension_of_the_16_layer_slab(gpu):
     got = gpu.dyson(chi, U)
     ref = O.dyson(chi, U)
     assert rel(got, ref) < 1e-10
+
+
+@pytest.mark.parametrize("shape,sel_d,precision", [("slab6", False, "fp64"), ("slab16", True, "fp64"),
+                                                   ("slab16", True, "split")])
+def test_tridiagonal_resolvents_equal_gauss_jordan(gpu, shape, sel_d, precision):
+    """Uniform meshes beyond the Jacobi kernel's dimensions: chi0 from G over the rows chi
+    needs, formed from a Householder tridiagonalisation per k (the default there), equals the
+    cluster Gauss-Jordan path, at q != 0 with the real axis."""
+    deck = synthetic.make_deck(shape, nk=(3, 3, 1), n1gl=4, parts=1, n3gl=3)
+    s = deck.system
+    gpu.setup(deck, s.h0(initial_state(s)))
+    gpu.set_chi_orbitals([list(d) for d in s.dorbs] if sel_d else None)
+    e, q = 0.05, np.array([0.1, 0.0, 0.0])
+    x2, p2 = deck.real_points(e, s.Ef)
+    try:
+        auto = gpu.chi0(q, e, s.Ef, s.eta, s.etap, x2, p2, precision=precision)
+        gpu.set_green_method("gauss-jordan")
+        gj = gpu.chi0(q, e, s.Ef, s.eta, s.etap, x2, p2, precision=precision)
+    finally:
+        gpu.set_green_method("auto")
+        gpu.set_chi_orbitals(None)
+    assert rel(auto, gj) < (1e-12 if precision == "fp64" else 1e-9)

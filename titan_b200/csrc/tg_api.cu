@@ -74,6 +74,7 @@ struct ChiLayout {
   std::vector<int64_t> pair_coff;
   std::vector<PairTile> tiles;
   SplitLayout split;
+  DevArray<int> d_rows;               // the nsel rows of G that enter chi, site by site
   DevArray<int> d_outmap, d_decode, d_norb, d_pair_M, d_pair_aoff;
   DevArray<int64_t> d_pair_coff;
   DevArray<PairTile> d_tiles;
@@ -94,6 +95,8 @@ struct ChiView {
   const SplitLayout* split = nullptr;
   const SplitGroup *sgA = nullptr, *sgB = nullptr;
   const SplitTile* stiles = nullptr;
+  const int* rows = nullptr;          // the rows of G that enter chi
+  int nrows = 0;
 };
 
 }  // namespace
@@ -184,6 +187,10 @@ struct tg_ctx {
   bool chi_sel_on = false;
   ChiLayout chi_sel;
   DevArray<double2> d_graw;   // column-major G of a pass (gathered chi0 operands)
+  DevArray<int> d_allrows;    // 0 .. dimH - 1
+  // Householder tridiagonalisations per k list (same slots as the H tables)
+  DevArray<double> d_triD[4], d_triE[4];
+  DevArray<double2> d_triQ[4];
   DevArray<unsigned char> d_clws;   // workspace of the thread-block-cluster Gauss-Jordan kernel
   // tg_expectation_noalloc: device address of the library's fixed scratch array on this
   // context's device (looked up by the context's first no-alloc call)
@@ -412,6 +419,49 @@ bool eig_room(tg_ctx* c, int64_t nk, int s0, int s1) {
   return need <= 0.5 * (double)fr;
 }
 
+// Householder tridiagonalisation of H(k + q) for a k list into slot `slot`: T and the rows
+// v.rows of Q, built chunk by chunk in the bounded H scratch (only T and Q_S are kept)
+int build_tri_chunked(tg_ctx* c, int slot, const double* d_k, int64_t nk, const double* q, const ChiView& v) {
+  const int64_t n = c->dimH, nn = n * n, ns = v.nrows;
+  const int64_t kc = std::max<int64_t>(1, std::min<int64_t>(nk, ((int64_t)2 << 30) / (nn * 16)));
+  TG_CHECK(c, c->d_triD[slot].ensure((size_t)nk * n), "alloc T");
+  TG_CHECK(c, c->d_triE[slot].ensure((size_t)nk * n), "alloc T");
+  TG_CHECK(c, c->d_triQ[slot].ensure((size_t)nk * ns * n), "alloc Q rows");
+  TG_CHECK(c, c->d_hchunk.ensure((size_t)kc * nn), "alloc H chunk");
+  TG_CHECK(c, c->d_hphase.ensure((size_t)kc * std::max(c->n_neigh, 1)), "alloc phases");
+  TG_CHECK(c, c->d_qvec.upload(q, 3, c->stream), "upload q");
+  const GreenArgs a = base_args(c);
+  KindTimer kt(c, 0);
+  for (int64_t k0 = 0; k0 < nk; k0 += kc) {
+    const int64_t m = std::min(kc, nk - k0);
+    TG_CHECK(c, launch_hk_table(a, d_k + 3 * k0, m, c->d_qvec.p, c->d_hphase.p, c->d_hchunk.p, c->stream),
+             "H table");
+    TG_CHECK(c, launch_tridiag(c->d_hchunk.p, m, (int)n, v.rows, (int)ns, c->d_triD[slot].p + k0 * n,
+                               c->d_triE[slot].p + k0 * n, c->d_triQ[slot].p + k0 * ns * n, c->num_sms, c->stream),
+             "tridiagonalisation");
+    c->launches += 3;
+  }
+  return TG_OK;
+}
+
+// whether tridiagonalisations of nk points in slots s0 and s1 (-1: none) fit: what they add to
+// the current allocations (and the H chunk) within half the free device memory
+bool tri_room(tg_ctx* c, int64_t nk, int64_t ns, int s0, int s1) {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
+  const size_t n = c->dimH, nn = n * n;
+  double need = 0.0;
+  for (int sl : {s0, s1}) {
+    if (sl < 0) continue;
+    const size_t want = (size_t)nk * ns * n;
+    if (c->d_triQ[sl].n < want) need += (double)(want - c->d_triQ[sl].n) * sizeof(double2);
+    need += 2.0 * nk * n * sizeof(double);
+  }
+  const size_t kc = std::min<size_t>((size_t)nk, std::max<size_t>(1, ((size_t)2 << 30) / (nn * 16)));
+  if (c->d_hchunk.n < kc * nn) need += (double)(kc * nn - c->d_hchunk.n) * sizeof(double2);
+  return need <= 0.5 * (double)fr;
+}
+
 int reset_eig_status(tg_ctx* c) {
   const int big = 0x7fffffff;
   TG_CHECK(c, c->d_eig_status.ensure(1), "alloc");
@@ -450,6 +500,7 @@ ChiView chi_view(tg_ctx* c) {
   v.pair_M = L.d_pair_M.p; v.pair_aoff = L.d_pair_aoff.p; v.pair_coff = L.d_pair_coff.p;
   v.tiles = L.d_tiles.p; v.ntiles = (int)L.tiles.size(); v.split = &L.split;
   v.sgA = L.d_sgA.p; v.sgB = L.d_sgB.p; v.stiles = L.d_stiles.p;
+  v.rows = L.d_rows.p; v.nrows = L.nsel;
   return v;
 }
 
@@ -499,6 +550,10 @@ int build_chi_layout(tg_ctx* c, const std::vector<std::vector<int>>& orbs, ChiLa
         for (int sg = 0; sg < 4; ++sg) decode[kount++] = sg | (i << 2) | (mu << 12) | (nu << 18);
   split_build_layout(np2, L.pair_M.data(), L.pair_aoff.data(), L.split);
   cudaStream_t s = c->stream;
+  std::vector<int> rows;
+  for (int i = 0; i < nat; ++i)
+    for (int x = 0; x < 2 * L.nc[i]; ++x) rows.push_back(row_of(i, x));
+  TG_CHECK(c, L.d_rows.upload(rows.data(), rows.size(), s), "upload");
   TG_CHECK(c, L.d_outmap.upload(outmap.data(), outmap.size(), s), "upload");
   TG_CHECK(c, L.d_decode.upload(decode.data(), decode.size(), s), "upload");
   TG_CHECK(c, L.d_norb.upload(L.nc.data(), nat, s), "upload");
@@ -523,6 +578,7 @@ ChiView full_view(tg_ctx* c) {
   v.pair_M = c->d_pair_M.p; v.pair_aoff = c->d_pair_aoff.p; v.pair_coff = c->d_pair_coff.p;
   v.tiles = c->d_tiles.p; v.ntiles = (int)c->tiles.size(); v.split = &c->split;
   v.sgA = c->d_sgA.p; v.sgB = c->d_sgB.p; v.stiles = c->d_stiles.p;
+  v.rows = c->d_allrows.p; v.nrows = c->dimH;
   return v;
 }
 
@@ -985,6 +1041,11 @@ int tg_set_system(tg_ctx* c, int n_atoms, const int* norb, int norb_max, int n_n
   TG_CHECK(c, c->d_row_spin.upload(rspin.data(), n, s), "upload");
   TG_CHECK(c, c->d_outmap.upload(outmap.data(), outmap.size(), s), "upload");
   {
+    std::vector<int> all(n);
+    for (int r = 0; r < n; ++r) all[r] = r;
+    TG_CHECK(c, c->d_allrows.upload(all.data(), all.size(), s), "upload");
+  }
+  {
     std::vector<int> outinv((size_t)n * n);
     for (size_t o = 0; o < outmap.size(); ++o) outinv[outmap[o]] = (int)o;
     TG_CHECK(c, c->d_outinv.upload(outinv.data(), outinv.size(), s), "upload");
@@ -1177,9 +1238,28 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   // ---------------- H(k) tables (k-major traversal) ----------------
   const bool q_zero = q[0] == 0.0 && q[1] == 0.0 && q[2] == 0.0;
   const double zero3[3] = {0.0, 0.0, 0.0};
-  const bool tab_imag = c->imag_uniform && (int64_t)c->nk_u * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
-  const bool tab_real = any_real && (int64_t)c->n_realk * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
   const bool spec = spectral_on(c);
+  // dimensions beyond the Jacobi kernel (gathered operands) on meshes whose energies share a k
+  // list: G over the rows chi needs from a Householder tridiagonalisation per k, kept as T and
+  // those rows of Q (built from bounded H chunks)
+  const bool tri_ok = !spec && c->green_method != TG_GREEN_GAUSS_JORDAN && v.gather && tri_supported(c->dimH);
+  const bool tri_imag = tri_ok && c->imag_uniform && c->nk_u > 0 &&
+                        tri_room(c, c->nk_u, v.nrows, 0, q_zero ? -1 : 1);
+  if (tri_imag) {
+    if ((rc = build_tri_chunked(c, 0, c->d_klist_u.p, c->nk_u, zero3, v))) return rc;
+    if (!q_zero && (rc = build_tri_chunked(c, 1, c->d_klist_u.p, c->nk_u, q, v))) return rc;
+  }
+  const bool alias_tri = tri_imag && any_real && real_k_is_imag_k(c);
+  const bool tri_real = tri_ok && any_real && !alias_tri && c->n_realk > 0 &&
+                        tri_room(c, c->n_realk, v.nrows, 2, q_zero ? -1 : 3);
+  if (tri_real) {
+    if ((rc = build_tri_chunked(c, 2, c->d_rkp.p, c->n_realk, zero3, v))) return rc;
+    if (!q_zero && (rc = build_tri_chunked(c, 3, c->d_rkp.p, c->n_realk, q, v))) return rc;
+  }
+  const bool tab_imag = !tri_imag && c->imag_uniform &&
+                        (int64_t)c->nk_u * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
+  const bool tab_real = !tri_real && !alias_tri && any_real &&
+                        (int64_t)c->n_realk * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
   if (spec && (rc = reset_eig_status(c))) return rc;
   if (tab_imag) {
     if ((rc = build_htab(c, 0, c->d_klist_u.p, c->nk_u, zero3))) return rc;
@@ -1188,14 +1268,14 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     if (!q_zero && spec && (rc = build_eig(c, 1, c->nk_u))) return rc;
   }
   // real-axis slots 2 / 3 alias the imaginary-axis slots 0 / 1 when the k lists coincide
-  const bool alias_real = tab_imag && tab_real && real_k_is_imag_k(c);
+  const bool alias_real = (tab_imag && tab_real && real_k_is_imag_k(c)) || alias_tri;
   const int rslot0 = alias_real ? 0 : 2, rslot1 = alias_real ? 1 : 3;
   // a real-axis BZ of its own: spectral Green functions from eigendecompositions built out of
   // bounded H chunks (only U and lambda are kept, so long BZs qualify too) when they fit in
   // memory, else Gauss-Jordan on resident H tables when those fit
   const bool eig_real = any_real && !alias_real && spec && eig_room(c, c->n_realk, 2, q_zero ? -1 : 3);
   const bool tab_real_gj = tab_real && !alias_real && !eig_real;
-  const bool kmajor_real = alias_real || tab_real_gj || eig_real;
+  const bool kmajor_real = alias_real || tab_real_gj || eig_real || tri_real;
   if (tab_real_gj) {
     if ((rc = build_htab(c, 2, c->d_rkp.p, c->n_realk, zero3))) return rc;
     if (!q_zero && (rc = build_htab(c, 3, c->d_rkp.p, c->n_realk, q))) return rc;
@@ -1205,10 +1285,19 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     if (!q_zero && (rc = build_eig_chunked(c, 3, c->d_rkp.p, c->n_realk, q))) return rc;
   }
   auto use_table = [&](GreenArgs& g, int slot, int64_t n_e, int64_t nk, const double* ylist) {
-    g.htab = eig_real && slot >= 2 ? nullptr : c->d_htab[slot].p;
     g.n_e = n_e;
     g.nk_tab = nk;
     g.ylist = ylist;
+    if (slot < 2 ? tri_imag : tri_real) {
+      g.htab = nullptr;
+      g.triD = c->d_triD[slot].p;
+      g.triE = c->d_triE[slot].p;
+      g.triQ = c->d_triQ[slot].p;
+      g.trirows = v.rows;
+      g.tri_ns = v.nrows;
+      return;
+    }
+    g.htab = eig_real && slot >= 2 ? nullptr : c->d_htab[slot].p;
     if (spec && (slot < 2 || eig_real)) {
       g.eigU = c->d_eigU[slot].p;
       g.eigL = c->d_eigL[slot].p;
@@ -1229,7 +1318,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     g2.zi = etap;
     g2.mode = MODE_B_IMAG;
     g2.out = c->d_B.p;
-    if (tab_imag) use_table(g2, 0, c->n_e_u, c->nk_u, c->d_ylist.p);
+    if (tab_imag || tri_imag) use_table(g2, 0, c->n_e_u, c->nk_u, c->d_ylist.p);
     // G1 = G2 when e = 0, q = 0 and eta = eta': one inversion feeds both operands
     int w_start = 0;
     if (e[0] == 0.0 && q_zero && eta == etap) {
@@ -1254,7 +1343,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
     if (split) {
       KindTimer kt(c, 3);
       const double* yv = c->h_y.data() + p0;
-      const SplitChunks ch = tab_imag ? make_chunks_kmajor(p0, np, c->n_e_u, c->split_chunk)
+      const SplitChunks ch = tab_imag || tri_imag ? make_chunks_kmajor(p0, np, c->n_e_u, c->split_chunk)
                                       : make_chunks(np, c->split_chunk, [&](int64_t i) { return yv[i]; });
       if ((rc = split_prepare(c, v, ch, pd))) return rc;
       if ((rc = split_quantize_operand(c, v, 1, c->d_B.p, pd, e16_g2 ? c->d_e16B.p : nullptr))) return rc;
@@ -1282,7 +1371,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       g1.q[0] = q[0]; g1.q[1] = q[1]; g1.q[2] = q[2];
       g1.mode = MODE_A_IMAG;
       g1.out = c->d_A.p;
-      if (tab_imag) {
+      if (tab_imag || tri_imag) {
         use_table(g1, q_zero ? 0 : 1, c->n_e_u, c->nk_u, c->d_ylist.p);
         g1.q[0] = g1.q[1] = g1.q[2] = 0.0;   // q is inside the table
       }
@@ -1711,7 +1800,10 @@ int tg_chi0_qbatch(tg_ctx* c, int n_q, const double* q, int n_omega, const doubl
   // the frequencies of one q share G2 and the q run one after another; otherwise one G2 per
   // pass serves every q (both axes then sum H(k) inside the inversion kernels)
   const bool tab_imag = c->imag_uniform && (int64_t)c->nk_u * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
-  if (n_q == 1 || tab_imag) {
+  // (likewise on uniform meshes whose dimension takes the tridiagonalised path of tg_chi0_batch)
+  const bool tri_imag = c->imag_uniform && !spectral_on(c) && c->green_method != TG_GREEN_GAUSS_JORDAN &&
+                        v.gather && tri_supported(c->dimH);
+  if (n_q == 1 || tab_imag || tri_imag) {
     double tot[4] = {0, 0, 0, 0};
     std::vector<double> bounds;
     for (int iq = 0; iq < n_q; ++iq) {

@@ -510,6 +510,10 @@ bool green_is_spectral(const GreenArgs& a) {
 }
 
 cudaError_t launch_green(const GreenArgs& a, int num_sms, cudaStream_t s, int* grid_used) {
+  if (a.triQ) {
+    if (grid_used) *grid_used = 0;
+    return launch_green_tri(a, num_sms, s);
+  }
   if (green_is_spectral(a)) {
     if (grid_used) *grid_used = 0;
     return launch_green_spectral(a, a.eigU, a.eigL, a.outinv, num_sms, s);

@@ -139,6 +139,14 @@ struct GreenArgs {
   // outinv[r*n + c] = pair-block slot of (r, c)
   const double2* eigU = nullptr;
   const double* eigL = nullptr;
+  // optional Householder tridiagonalisation of every k of the k-major traversal (dimensions
+  // beyond the Jacobi kernel): T's diagonal triD[k][n] and off-diagonal triE[k][n], the rows
+  // trirows[tri_ns] of Q as triQ[k][s][c]; the output is G over those rows and columns
+  const double* triD = nullptr;
+  const double* triE = nullptr;
+  const double2* triQ = nullptr;
+  const int* trirows = nullptr;
+  int tri_ns = 0;
   const int* outinv = nullptr;
   // optional exponent sidecars of out / out2 (spectral G only): per stored value the
   // frexp exponent of max(|Re|, |Im|), -32768 for zero or subnormal
@@ -197,6 +205,12 @@ int eig_supported(int n);
 cudaError_t launch_eig(const double2* H, int64_t nk, int n, double2* U, double* lam, int* status, int num_sms,
                        cudaStream_t s);
 int spectral_supported(int mode, int mode2, bool has_out2);
+// Resolvents from a Householder tridiagonalisation per k: H (an H(k) table, overwritten) ->
+// T (D, E) and the rows `rows` of Q; G over those rows per point of a k-major pass (MODE_RAW)
+int tri_supported(int n);
+cudaError_t launch_tridiag(double2* H, int64_t nk, int n, const int* rows, int ns, double* D, double* E,
+                           double2* Q, int num_sms, cudaStream_t s);
+cudaError_t launch_green_tri(const GreenArgs& g, int num_sms, cudaStream_t s);
 // per-CTA slices [grid][2 n] of the energy-summed diagonal spin blocks (uu, dd, ud, du per orbital)
 cudaError_t launch_spec_expect(const double2* U, const double* lam, int64_t nk, int n, const double* ylist, int64_t n_e,
                                const double* w, double zr, double zi, const int* rows, double2* partial, int grid,

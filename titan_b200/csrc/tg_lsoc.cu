@@ -108,7 +108,7 @@ __global__ void gather_kernel(GreenArgs g, const double2* __restrict__ G, int mo
     const double2* gp = G + pl * nn;
     const int64_t wi = g.p0 + pl;
     double w;
-    if (g.htab || g.eigU) {   // k-major: an H(k) table or its eigendecompositions
+    if (g.htab || g.eigU || g.triQ) {   // k-major: an H(k) table, or its decompositions
       const int64_t ik = wi / g.n_e, ie = wi % g.n_e;
       w = g.pts.kind == 0 ? g.pts.w[ie * g.nk_tab + ik] : g.pts.p2[ie] * g.pts.w[ik];
     } else if (g.pts.kind == 0) {
