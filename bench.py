@@ -427,17 +427,24 @@ def run_ours(args, rank, world, local_rank):
     spectral_real = eig_ok and (tabulated or shared)   # the real-axis BZ is one k list for every energy
     n_inv = inversions_of(deck, per, reals, start + args.warmup * per + (args.steps - 1) * per, nq, shared,
                           spectral_real and shared)
+    # beyond the Jacobi kernel, uniform meshes take G over the rows chi needs from a Householder
+    # tridiagonalisation per k: 8 |S|^2 n flops per point (|S| = rows of chi), a DMMA GEMM
+    tri = args.green != "gauss-jordan" and not eig_ok and tabulated and (sel is not None or not native_n)
+    ns = (sum(2 * len(o) for o in sel) if sel is not None else s.dimH) if tri else s.dimH
     kname = ("eig_jacobi_kernel + spec_green_kernel (spectral G, FP64 DMMA)" if spectral else
              "green_w1_kernel / green_team_kernel (imaginary axis, Gauss-Jordan) + eig_jacobi_kernel + "
              "spec_green_kernel (real axis, spectral)" if spectral_real else
+             "hh_tridiag_kernel + tri_green_kernel (Householder tridiagonalisation per k, G over the %d rows "
+             "of chi per point: tridiagonal solves + FP64 DMMA GEMM) + gather_kernel" % ns if tri else
              "green_w1_kernel / green_team_kernel (fused H(k) + Gauss-Jordan)" if native_n else
              "green_cluster_kernel (thread-block-cluster Gauss-Jordan) + gather_kernel")
-    peak64 = dmma if spectral or spectral_real else dfma
-    roof_inv = {"bound": "fp64", "achieved": (8.0 * s.dimH ** 3 * n_inv) / (grn_ms / 1e3) / 1e12 if grn_ms else None,
+    peak64 = dmma if spectral or spectral_real or tri else dfma
+    flops_g = 8.0 * ns * ns * s.dimH if tri else 8.0 * s.dimH ** 3
+    roof_inv = {"bound": "fp64", "achieved": (flops_g * n_inv) / (grn_ms / 1e3) / 1e12 if grn_ms else None,
                 "peak": peak64, "unit": "TFLOP/s",
-                "peak_source": ("of measured FP64 DMMA (tg_fp64_peak, this run)" if spectral or spectral_real
+                "peak_source": ("of measured FP64 DMMA (tg_fp64_peak, this run)" if spectral or spectral_real or tri
                                 else "of measured FP64 DFMA (tg_fp64_peak, this run)"),
-                "kernel": kname, "flops_per_inversion": 8.0 * s.dimH ** 3, "inversions_last_step": n_inv,
+                "kernel": kname, "flops_per_inversion": flops_g, "inversions_last_step": n_inv,
                 "ms_last_step": grn_ms, "launches_in_last_step": int(grn_n)}
     roof_inv["frac"] = roof_inv["achieved"] / peak64 if roof_inv["achieved"] else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

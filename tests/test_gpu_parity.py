@@ -303,8 +303,9 @@ def test_eig_batch_matches_eigh(gpu, shape):
     ("slab5", (3, 3, 1), 0.05, (0.0, 0.0, 0.0), "split"),
 ])
 def test_spectral_green_equals_gauss_jordan(gpu, shape, nk, e, q, precision):
-    """chi0 with G from the eigendecomposition (default on uniform meshes) and from
-    Gauss-Jordan per point agree to roundoff; both match the oracle."""
+    """chi0 with G from the eigendecomposition (default on uniform meshes up to dimH 72; at
+    dimH 90 the default is the tridiagonalised path and the packed eigendecomposition runs on
+    request) and from Gauss-Jordan per point agree to roundoff; both match the oracle."""
     deck = synthetic.make_deck(shape, nk=nk, n1gl=8, parts=1, n3gl=6)
     s, h0 = _setup(gpu, deck)
     x2, p2 = deck.real_points(e, s.Ef)
@@ -312,10 +313,13 @@ def test_spectral_green_equals_gauss_jordan(gpu, shape, nk, e, q, precision):
     try:
         gpu.set_green_method("gauss-jordan")
         gj = gpu.chi0(q, e, s.Ef, s.eta, s.etap, x2, p2, precision=precision)
+        gpu.set_green_method("spectral")
+        forced = gpu.chi0(q, e, s.Ef, s.eta, s.etap, x2, p2, precision=precision)
     finally:
         gpu.set_green_method("auto")
     sp = gpu.chi0(q, e, s.Ef, s.eta, s.etap, x2, p2, precision=precision)
     assert rel(sp, gj) < (1e-12 if precision == "fp64" else 1e-10)
+    assert rel(forced, gj) < (1e-12 if precision == "fp64" else 1e-10)
     ref = O.eintshechi(O.Model(s, h0), deck.ek, (deck.real_kp, deck.real_w), q, e, s.Ef, s.eta, s.etap, x2, p2)
     assert rel(sp, ref) < (1e-10 if precision == "fp64" else 1e-9)
 

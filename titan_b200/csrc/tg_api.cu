@@ -364,6 +364,16 @@ int build_htab(tg_ctx* c, int slot, const double* d_k, int64_t nk, const double*
 // tg_set_green_method)
 bool spectral_on(tg_ctx* c) { return c->green_method != TG_GREEN_GAUSS_JORDAN && eig_supported(c->dimH); }
 bool spectral_forced(tg_ctx* c) { return c->green_method == TG_GREEN_SPECTRAL && eig_supported(c->dimH); }
+// chi0 on meshes whose energies share a k list: spectral G where the Jacobi kernel holds A and
+// U in shared memory (or when asked for), else under TG_GREEN_AUTO G from a Householder
+// tridiagonalisation per k (cheaper per k than the packed Jacobi kernel, and as accurate as
+// Gauss-Jordan near the real axis)
+bool chi_spectral(tg_ctx* c) {
+  return spectral_on(c) && (eig_fast(c->dimH) || c->green_method == TG_GREEN_SPECTRAL);
+}
+bool chi_tridiag(tg_ctx* c) {
+  return !chi_spectral(c) && c->green_method == TG_GREEN_AUTO && tri_supported(c->dimH);
+}
 
 int build_eig(tg_ctx* c, int slot, int64_t nk) {
   const size_t nn = (size_t)c->dimH * c->dimH;
@@ -841,7 +851,8 @@ int choose_nsplit(tg_ctx* c, const ChiView& v, bool split, int64_t P, int* out) 
 // Green functions of a chi0 pass into the operand buffers: fused (the kernel writes the
 // operand layouts), or gathered (column-major G into d_graw, then the view's slots)
 int chi_green(tg_ctx* c, const ChiView& v, const GreenArgs& g, const char* what) {
-  if (!v.gather) {
+  // the tridiagonalised path writes G column-major only: its operands are always gathered
+  if (!v.gather && !g.triQ) {
     TG_CHECK(c, launch_green(g, c->num_sms, c->stream, nullptr), what);
     return TG_OK;
   }
@@ -1219,7 +1230,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   if ((rc = bound_begin(c, split, n_omega))) return rc;
   TG_CHECK(c, c->d_A.ensure((size_t)P * v.ld), "alloc A");
   TG_CHECK(c, c->d_B.ensure((size_t)P * v.ld), "alloc B");
-  if (v.gather) TG_CHECK(c, c->d_graw.ensure((size_t)P * nn), "alloc G");
+  if (v.gather || chi_tridiag(c)) TG_CHECK(c, c->d_graw.ensure((size_t)P * nn), "alloc G");
   TG_CHECK(c, c->d_C.ensure((size_t)n_omega * nsplit * cstride), "alloc C");
   TG_CHECK(c, c->d_D.ensure((size_t)n_omega * nsplit * cstride), "alloc D");
   TG_CHECK(c, c->d_chi.ensure((size_t)cstride), "alloc chi");
@@ -1238,11 +1249,11 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
   // ---------------- H(k) tables (k-major traversal) ----------------
   const bool q_zero = q[0] == 0.0 && q[1] == 0.0 && q[2] == 0.0;
   const double zero3[3] = {0.0, 0.0, 0.0};
-  const bool spec = spectral_on(c);
-  // dimensions beyond the Jacobi kernel (gathered operands) on meshes whose energies share a k
-  // list: G over the rows chi needs from a Householder tridiagonalisation per k, kept as T and
-  // those rows of Q (built from bounded H chunks)
-  const bool tri_ok = !spec && c->green_method != TG_GREEN_GAUSS_JORDAN && v.gather && tri_supported(c->dimH);
+  const bool spec = chi_spectral(c);
+  // otherwise, on meshes whose energies share a k list: G over the rows chi needs from a
+  // Householder tridiagonalisation per k, kept as T and those rows of Q (built from bounded H
+  // chunks); its operands are gathered
+  const bool tri_ok = chi_tridiag(c);
   const bool tri_imag = tri_ok && c->imag_uniform && c->nk_u > 0 &&
                         tri_room(c, c->nk_u, v.nrows, 0, q_zero ? -1 : 1);
   if (tri_imag) {
@@ -1546,7 +1557,7 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
   }
   TG_CHECK(c, c->d_A.ensure((size_t)P * v.ld), "alloc A");
   TG_CHECK(c, c->d_B.ensure((size_t)P * v.ld), "alloc B");
-  if (v.gather) TG_CHECK(c, c->d_graw.ensure((size_t)P * nn), "alloc G");
+  if (v.gather || chi_tridiag(c)) TG_CHECK(c, c->d_graw.ensure((size_t)P * nn), "alloc G");
   TG_CHECK(c, c->d_C.ensure((size_t)nacc), "alloc C");
   TG_CHECK(c, c->d_D.ensure((size_t)nacc), "alloc D");
   TG_CHECK(c, c->d_chi.ensure((size_t)cstride), "alloc chi");
@@ -1611,37 +1622,51 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
         if ((rc = contract_into(pd, np, acc_at(c->d_C.p, iq, w), bound_at(c, split, iq * n_omega + w, 0)))) return rc;
       }
   }
-  // ---------------- real axis, spectral ----------------
-  // the real-axis BZ is one k list for every energy: with its eigendecompositions (H(k) once,
-  // H(k + q) once per q, from bounded H chunks) G2 and G1 of every frequency are GEMMs per
-  // block of energies; G2 is formed again for each q, which costs far less than sharing an
-  // inversion per point
+  // ---------------- real axis, spectral or tridiagonalised ----------------
+  // the real-axis BZ is one k list for every energy: with its eigendecompositions, or its
+  // Householder tridiagonalisations (H(k) once, H(k + q) once per q, from bounded H chunks), G2
+  // and G1 of every frequency cost a GEMM per point (or block of energies); G2 is formed again
+  // for each q, which costs far less than sharing an inversion per point
   bool any_real = false;
   for (int w = 0; w < n_omega; ++w) any_real |= std::fabs(e[w]) >= 1e-15;
-  const bool eig_real = any_real && spectral_on(c) && eig_room(c, c->n_realk, 2, 3);
-  if (eig_real) {
+  const bool eig_real = any_real && chi_spectral(c) && eig_room(c, c->n_realk, 2, 3);
+  const bool tri_real = any_real && !eig_real && chi_tridiag(c) && tri_room(c, c->n_realk, v.nrows, 2, 3);
+  if (eig_real || tri_real) {
     const double zero3[3] = {0.0, 0.0, 0.0};
-    const bool e16 = split && !v.gather;
+    const bool e16 = split && !v.gather && eig_real;
     if (e16) {
       TG_CHECK(c, c->d_e16A.ensure((size_t)P * nn), "alloc exponents A");
       TG_CHECK(c, c->d_e16B.ensure((size_t)P * nn), "alloc exponents B");
     }
-    if ((rc = reset_eig_status(c))) return rc;
-    if ((rc = build_eig_chunked(c, 2, c->d_rkp.p, c->n_realk, zero3))) return rc;
+    if (eig_real) {
+      if ((rc = reset_eig_status(c))) return rc;
+      if ((rc = build_eig_chunked(c, 2, c->d_rkp.p, c->n_realk, zero3))) return rc;
+    } else if ((rc = build_tri_chunked(c, 2, c->d_rkp.p, c->n_realk, zero3, v))) {
+      return rc;
+    }
     auto use_eig = [&](GreenArgs& g, int slot) {
       g.htab = nullptr;
       g.n_e = n_real;
       g.nk_tab = c->n_realk;
       g.ylist = nullptr;
-      g.eigU = c->d_eigU[slot].p;
-      g.eigL = c->d_eigL[slot].p;
-      g.outinv = c->d_outinv.p;
+      if (eig_real) {
+        g.eigU = c->d_eigU[slot].p;
+        g.eigL = c->d_eigL[slot].p;
+        g.outinv = c->d_outinv.p;
+      } else {
+        g.triD = c->d_triD[slot].p;
+        g.triE = c->d_triE[slot].p;
+        g.triQ = c->d_triQ[slot].p;
+        g.trirows = v.rows;
+        g.tri_ns = v.nrows;
+      }
     };
     const int64_t ntot = (int64_t)n_real * c->n_realk;
     for (int iq = 0; iq < n_q; ++iq) {
       const double* qi = qs + 3 * iq;
       const bool qz = qi[0] == 0.0 && qi[1] == 0.0 && qi[2] == 0.0;
-      if (!qz && (rc = build_eig_chunked(c, 3, c->d_rkp.p, c->n_realk, qi))) return rc;
+      if (!qz && eig_real && (rc = build_eig_chunked(c, 3, c->d_rkp.p, c->n_realk, qi))) return rc;
+      if (!qz && tri_real && (rc = build_tri_chunked(c, 3, c->d_rkp.p, c->n_realk, qi, v))) return rc;
       for (int w = 0; w < n_omega; ++w) {
         if (std::fabs(e[w]) < 1e-15) continue;
         for (int64_t p0 = 0; p0 < ntot; p0 += P) {
@@ -1691,7 +1716,7 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
     }
   }
   // ---------------- real axis: G2 once per pass and frequency ----------------
-  for (int w = 0; w < n_omega && !eig_real; ++w) {
+  for (int w = 0; w < n_omega && !eig_real && !tri_real; ++w) {
     if (std::fabs(e[w]) < 1e-15) continue;
     const int64_t ntot = (int64_t)n_real * c->n_realk;
     for (int64_t p0 = 0; p0 < ntot; p0 += P) {
@@ -1801,8 +1826,7 @@ int tg_chi0_qbatch(tg_ctx* c, int n_q, const double* q, int n_omega, const doubl
   // pass serves every q (both axes then sum H(k) inside the inversion kernels)
   const bool tab_imag = c->imag_uniform && (int64_t)c->nk_u * c->dimH * c->dimH * 16 <= ((int64_t)8 << 30);
   // (likewise on uniform meshes whose dimension takes the tridiagonalised path of tg_chi0_batch)
-  const bool tri_imag = c->imag_uniform && !spectral_on(c) && c->green_method != TG_GREEN_GAUSS_JORDAN &&
-                        v.gather && tri_supported(c->dimH);
+  const bool tri_imag = c->imag_uniform && chi_tridiag(c);
   if (n_q == 1 || tab_imag || tri_imag) {
     double tot[4] = {0, 0, 0, 0};
     std::vector<double> bounds;

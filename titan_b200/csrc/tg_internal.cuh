@@ -202,6 +202,7 @@ cudaError_t launch_reduce_blocks(const double2* part, int nblocks, int len, doub
 // Spectral Green functions: Jacobi eigendecomposition of an H(k) table and G from (U, lambda)
 size_t eig_smem_bytes(int n);
 int eig_supported(int n);
+int eig_fast(int n);
 cudaError_t launch_eig(const double2* H, int64_t nk, int n, double2* U, double* lam, int* status, int num_sms,
                        cudaStream_t s);
 int spectral_supported(int mode, int mode2, bool has_out2);

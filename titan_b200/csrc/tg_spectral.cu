@@ -364,8 +364,10 @@ __device__ __forceinline__ int16_t exponent_code(double2 v) {
 // registers with a 4-byte spill, measured faster than 64 registers at four CTAs
 // ANTI (MODE_A_REAL, w (G - G^+)): the diagonal -2i y / |z - lambda|^2 is purely
 // imaginary, so two of the four DMMAs per step would multiply by zero and are skipped
-template <bool ANTI>
-__global__ void __launch_bounds__(kSpecThreads, 5) spec_green_kernel(SpecArgs sa) {
+// THREADS = 1024 (one CTA per SM) where the shared memory of U leaves room for one CTA only
+// (n > 72): 32 warps instead of 8 hide the DMMA and shared-memory latencies
+template <bool ANTI, int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == kSpecThreads ? 5 : 1) spec_green_kernel(SpecArgs sa) {
   extern __shared__ __align__(16) unsigned char smem[];
   const GreenArgs& a = sa.g;
   const int n = a.n, kp = sa.kp, nn = n * n;
@@ -628,6 +630,13 @@ bool eig_packed(int n, int optin) { return eig_smem_bytes_form(n, false) > (size
 
 size_t eig_smem_bytes(int n) { return eig_smem_bytes_form(n, eig_packed(n, eig_optin())); }
 
+// the unpacked kernel (A and U both in shared memory): fast enough to diagonalise per k even
+// where few energies share a k list
+int eig_fast(int n) {
+  if (n % 2 != 0 || n < 2 || n > 32 * kEigCols) return 0;
+  return !eig_packed(n, eig_optin());
+}
+
 int eig_supported(int n) {
   if (n % 2 != 0 || n < 2 || n > 32 * kEigCols) return 0;
   const int optin = eig_optin();
@@ -676,17 +685,27 @@ cudaError_t launch_green_spectral(const GreenArgs& g, const double2* U, const do
   sa.kp = (g.n + 3) / 4 * 4;
   const size_t smem = spec_smem(g.n, sa.kp);
   const bool anti = g.mode == MODE_A_REAL;
-  auto kernel = anti ? spec_green_kernel<true> : spec_green_kernel<false>;
+  auto kernel = anti ? spec_green_kernel<true, kSpecThreads> : spec_green_kernel<false, kSpecThreads>;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kSpecThreads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm <= 0) return cudaErrorInvalidValue;
+  int threads = kSpecThreads;
+  if (per_sm == 1) {
+    kernel = anti ? spec_green_kernel<true, 1024> : spec_green_kernel<false, 1024>;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 1024, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm <= 0) return cudaErrorInvalidValue;
+    threads = 1024;
+  }
   const int64_t ne = g.n_e;
   const int64_t ntask = ((g.p0 + g.np - 1) / ne - g.p0 / ne + 1) * ((ne + kSpecZ - 1) / kSpecZ);
   const int64_t grid = std::min<int64_t>(ntask, (int64_t)num_sms * per_sm);
-  kernel<<<(unsigned)grid, kSpecThreads, smem, s>>>(sa);
+  kernel<<<(unsigned)grid, threads, smem, s>>>(sa);
   return cudaGetLastError();
 }
 
