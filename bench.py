@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--precision", default="split", choices=["split", "fp64"])
     ap.add_argument("--config", default="sq2")
     ap.add_argument("--omegas-per-step", type=int, default=0,
-                    help="frequencies per step (0: 4, or 1 for slab16 whose frequency costs minutes)")
+                    help="frequencies per step (0: 4, or 1 for slab16 and slab5, whose frequency costs tens of seconds)")
     ap.add_argument("--qs-per-step", type=int, default=0,
                     help="wave vectors per step along Gamma-X (tg_chi0_qbatch; 0: 2 for slab5, else 1 at q = 0)")
     ap.add_argument("--no-autotune", action="store_true",
@@ -421,28 +421,37 @@ def run_ours(args, rank, world, local_rank):
     dfma, dmma = fp64_peak()
     native_n = s.dimH in (4, 8, 16, 18, 20, 36, 40, 54, 72, 90)
     tabulated = len(set(np.bincount(deck.ek.energy_index).tolist())) == 1   # every energy on the same k list
-    eig_ok = args.green != "gauss-jordan" and s.dimH % 2 == 0 and s.dimH <= 96   # the Jacobi kernel's range
-    spectral = eig_ok and tabulated
+    # chi0's Green functions on meshes whose energies share a k list: spectral from the unpacked
+    # Jacobi kernel (even dimH <= 72), else under AUTO from a Householder tridiagonalisation per k
+    # (G over the rows chi needs: 8 |S|^2 n flops per point, a DMMA GEMM); adaptive imaginary axes
+    # (shared G2 across q) keep Gauss-Jordan there and use these on the real axis only
+    eig_fast = args.green != "gauss-jordan" and s.dimH % 2 == 0 and s.dimH <= 72
+    tri_ok = args.green == "auto" and not eig_fast
     shared = nq > 1 and not tabulated
-    spectral_real = eig_ok and (tabulated or shared)   # the real-axis BZ is one k list for every energy
+    spectral = eig_fast and tabulated
+    spectral_real = eig_fast and shared
+    tri_all = tri_ok and tabulated
+    tri_real = tri_ok and shared
     n_inv = inversions_of(deck, per, reals, start + args.warmup * per + (args.steps - 1) * per, nq, shared,
-                          spectral_real and shared)
-    # beyond the Jacobi kernel, uniform meshes take G over the rows chi needs from a Householder
-    # tridiagonalisation per k: 8 |S|^2 n flops per point (|S| = rows of chi), a DMMA GEMM
-    tri = args.green != "gauss-jordan" and not eig_ok and tabulated and (sel is not None or not native_n)
-    ns = (sum(2 * len(o) for o in sel) if sel is not None else s.dimH) if tri else s.dimH
+                          (spectral_real or tri_real) and shared)
+    ns = sum(2 * len(o) for o in sel) if sel is not None else s.dimH
+    tri_name = ("hh_tridiag_kernel + tri_green_kernel (Householder tridiagonalisation per k, G over the %d rows "
+                "of chi per point: tridiagonal solves + FP64 DMMA GEMM) + gather_kernel" % ns)
+    gj_name = ("green_w1_kernel / green_team_kernel (fused H(k) + Gauss-Jordan)" if native_n else
+               "green_cluster_kernel (thread-block-cluster Gauss-Jordan) + gather_kernel")
     kname = ("eig_jacobi_kernel + spec_green_kernel (spectral G, FP64 DMMA)" if spectral else
-             "green_w1_kernel / green_team_kernel (imaginary axis, Gauss-Jordan) + eig_jacobi_kernel + "
-             "spec_green_kernel (real axis, spectral)" if spectral_real else
-             "hh_tridiag_kernel + tri_green_kernel (Householder tridiagonalisation per k, G over the %d rows "
-             "of chi per point: tridiagonal solves + FP64 DMMA GEMM) + gather_kernel" % ns if tri else
-             "green_w1_kernel / green_team_kernel (fused H(k) + Gauss-Jordan)" if native_n else
-             "green_cluster_kernel (thread-block-cluster Gauss-Jordan) + gather_kernel")
-    peak64 = dmma if spectral or spectral_real or tri else dfma
-    flops_g = 8.0 * ns * ns * s.dimH if tri else 8.0 * s.dimH ** 3
+             gj_name + " on the imaginary axis; eig_jacobi_kernel + spec_green_kernel (spectral) on the real axis"
+             if spectral_real else
+             tri_name if tri_all else
+             gj_name + " on the imaginary axis; " + tri_name + " on the real axis" if tri_real else gj_name)
+    dmma_path = spectral or spectral_real or tri_all or tri_real
+    peak64 = dmma if dmma_path else dfma
+    # algorithmic flops per Green function: 8 n^3 (an inversion or a full spectral G), 8 |S|^2 n where
+    # the tridiagonalised path forms G over the rows S only (mixed paths: the n^3 figure)
+    flops_g = 8.0 * ns * ns * s.dimH if tri_all else 8.0 * s.dimH ** 3
     roof_inv = {"bound": "fp64", "achieved": (flops_g * n_inv) / (grn_ms / 1e3) / 1e12 if grn_ms else None,
                 "peak": peak64, "unit": "TFLOP/s",
-                "peak_source": ("of measured FP64 DMMA (tg_fp64_peak, this run)" if spectral or spectral_real or tri
+                "peak_source": ("of measured FP64 DMMA (tg_fp64_peak, this run)" if dmma_path
                                 else "of measured FP64 DFMA (tg_fp64_peak, this run)"),
                 "kernel": kname, "flops_per_inversion": flops_g, "inversions_last_step": n_inv,
                 "ms_last_step": grn_ms, "launches_in_last_step": int(grn_n)}

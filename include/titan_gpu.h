@@ -300,15 +300,19 @@ int tg_ldos(tg_ctx* ctx, int n_e, const double* e, double eta, double* ldosu, do
  * error against the FP64 oracle as Gauss-Jordan), but the disturbance integral feeds
  * B_eff through an ill-conditioned site-reduced chi^-1, and the occupations feed a Newton
  * iteration whose step tolerance (mag_tol = 1e-12) the spectral noise exceeds, so:
- *   TG_GREEN_AUTO (default)  spectral for chi0 and tg_ldos; Gauss-Jordan for
+ *   TG_GREEN_AUTO (default)  spectral for chi0 (dimH <= 72) and tg_ldos; for chi0 beyond
+ *                            dimH 72, G over the rows chi needs from one Householder
+ *                            tridiagonalisation per k, H = Q T Q^H, and per energy
+ *                            Q_S (z - T)^-1 Q_S^H (LU-like accuracy); Gauss-Jordan for
  *                            tg_expectation; for tg_she spectral at Im z >= 10 eta and
  *                            Gauss-Jordan below and on the real axis (dimH 36; elsewhere
  *                            Gauss-Jordan)
  *   TG_GREEN_GAUSS_JORDAN    Gauss-Jordan everywhere
  *   TG_GREEN_SPECTRAL        spectral wherever the mesh allows (tg_she ~4x faster,
  *                            tg_expectation one eigendecomposition per k for all energies)
- * The eigendecomposition handles even dimH up to 96; other meshes and dimensions always
- * use Gauss-Jordan.  No counterpart in the reference. */
+ * The eigendecomposition handles even dimH up to 96 and the tridiagonalisation any dimH up
+ * to 288; meshes whose energies do not share a k list (adaptive imaginary axes) always use
+ * Gauss-Jordan there.  No counterpart in the reference. */
 #define TG_GREEN_AUTO          0
 #define TG_GREEN_GAUSS_JORDAN  1
 #define TG_GREEN_SPECTRAL      2
