@@ -316,8 +316,10 @@ __global__ void __launch_bounds__(kEigThreads) eig_jacobi_kernel(const double2* 
 }
 
 // --------------------------------------------------------------------------- G from (U, lambda)
+// not volatile: the scheduler may interleave the MMAs of independent accumulators (a chain on
+// one accumulator keeps its order through the data dependence, so results do not change)
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                : "+d"(c0), "+d"(c1)
                : "d"(a), "d"(b));
 }
