@@ -850,6 +850,10 @@ int choose_nsplit(tg_ctx* c, const ChiView& v, bool split, int64_t P, int* out) 
 
 // Green functions of a chi0 pass into the operand buffers: fused (the kernel writes the
 // operand layouts), or gathered (column-major G into d_graw, then the view's slots)
+// whether the launch of g (through chi_green) writes an exponent sidecar beside its operand:
+// the spectral kernel does, and so does the gather kernel for every gathered operand
+bool writes_sidecar(const ChiView& v, const GreenArgs& g) { return v.gather || g.triQ || green_is_spectral(g); }
+
 int chi_green(tg_ctx* c, const ChiView& v, const GreenArgs& g, const char* what) {
   // the tridiagonalised path writes G column-major only: its operands are always gathered
   if (!v.gather && !g.triQ) {
@@ -862,8 +866,10 @@ int chi_green(tg_ctx* c, const ChiView& v, const GreenArgs& g, const char* what)
   r.out2 = nullptr;
   r.eout = r.eout2 = nullptr;
   TG_CHECK(c, launch_green(r, c->num_sms, c->stream, nullptr), what);
-  TG_CHECK(c, launch_gather(g, c->d_graw.p, g.mode, v.outmap, v.ld, g.out, c->num_sms, c->stream), what);
-  if (g.out2) TG_CHECK(c, launch_gather(g, c->d_graw.p, g.mode2, v.outmap, v.ld, g.out2, c->num_sms, c->stream), what);
+  TG_CHECK(c, launch_gather(g, c->d_graw.p, g.mode, v.outmap, v.ld, g.out, g.eout, c->num_sms, c->stream), what);
+  if (g.out2)
+    TG_CHECK(c, launch_gather(g, c->d_graw.p, g.mode2, v.outmap, v.ld, g.out2, g.eout2, c->num_sms, c->stream),
+             what);
   c->launches += g.out2 ? 2 : 1;
   return TG_OK;
 }
@@ -1337,8 +1343,9 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       g2.mode2 = MODE_A_IMAG;
       w_start = 1;
     }
-    // the split row maxima read exponent sidecars when the spectral kernel writes G
-    const bool e16_g2 = split && !v.gather && green_is_spectral(g2);
+    // the split row maxima read exponent sidecars when the spectral kernel or the gather
+    // kernel writes the operand
+    const bool e16_g2 = split && writes_sidecar(v, g2);
     if (e16_g2) {
       g2.eout = c->d_e16B.p;
       if (g2.out2) g2.eout2 = c->d_e16A.p;
@@ -1386,7 +1393,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
         use_table(g1, q_zero ? 0 : 1, c->n_e_u, c->nk_u, c->d_ylist.p);
         g1.q[0] = g1.q[1] = g1.q[2] = 0.0;   // q is inside the table
       }
-      const bool e16_g1 = split && !v.gather && green_is_spectral(g1);
+      const bool e16_g1 = split && writes_sidecar(v, g1);
       if (e16_g1) g1.eout = c->d_e16A.p;
       {
         KindTimer kt(c, 0);
@@ -1439,7 +1446,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
       gr.mode = MODE_B_REAL;
       gr.out = c->d_B.p;
       if (kmajor_real) use_table(gr, rslot0, n_real, c->n_realk, nullptr);
-      const bool e16_rb = split && !v.gather && green_is_spectral(gr);
+      const bool e16_rb = split && writes_sidecar(v, gr);
       gr.eout = e16_rb ? c->d_e16B.p : nullptr;
       {
         KindTimer kt(c, 0);
@@ -1455,7 +1462,7 @@ int tg_chi0_batch(tg_ctx* c, const double* q, int n_omega, const double* e, doub
         use_table(gr, q_zero ? rslot0 : rslot1, n_real, c->n_realk, nullptr);
         gr.q[0] = gr.q[1] = gr.q[2] = 0.0;
       }
-      const bool e16_ra = split && !v.gather && green_is_spectral(gr);
+      const bool e16_ra = split && writes_sidecar(v, gr);
       gr.eout = e16_ra ? c->d_e16A.p : nullptr;
       {
         KindTimer kt(c, 0);
@@ -1633,7 +1640,7 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
   const bool tri_real = any_real && !eig_real && chi_tridiag(c) && tri_room(c, c->n_realk, v.nrows, 2, 3);
   if (eig_real || tri_real) {
     const double zero3[3] = {0.0, 0.0, 0.0};
-    const bool e16 = split && !v.gather && eig_real;
+    const bool e16 = split;   // the spectral kernel or the gather kernel writes every operand here
     if (e16) {
       TG_CHECK(c, c->d_e16A.ensure((size_t)P * nn), "alloc exponents A");
       TG_CHECK(c, c->d_e16B.ensure((size_t)P * nn), "alloc exponents B");

@@ -230,8 +230,18 @@ cudaError_t launch_operand(const double2* G, int n, int64_t np, int64_t p0, cons
                            const int* outmap, double2* out, int num_sms, cudaStream_t s);
 // operand of a Green-function launch g from its column-major G (MODE_RAW output of g):
 // ld slots per point, outmap[o] = r * n + c (an orbital subset in pair-block order)
+// eout (null: none): the operand's exponent sidecar (exponent_code16 of every value written)
 cudaError_t launch_gather(const GreenArgs& g, const double2* G, int mode, const int* outmap, int64_t ld, double2* out,
-                          int num_sms, cudaStream_t s);
+                          int16_t* eout, int num_sms, cudaStream_t s);
+
+// frexp exponent of max(|Re|, |Im|) from the bits (the exponent field - 1022 for a normal
+// number), -32768 for zero or a subnormal: the exponent sidecar the split quantiser's row
+// maxima read instead of the FP64 values
+__device__ __forceinline__ int16_t exponent_code16(double2 v) {
+  const double m = fmax(fabs(v.x), fabs(v.y));
+  const int f = (int)((__double_as_longlong(m) >> 52) & 0x7ff);
+  return f == 0 ? (int16_t)-32768 : (int16_t)(f - 1022);
+}
 
 // Exchange coupling: d-orbital GG tensors T(G(k), G(k - q)) and T(G(k - q), G(k)) per site pair
 cudaError_t launch_jij(const double2* Ga, const double2* Gb, int64_t p0, int64_t np, const double* w, int n,

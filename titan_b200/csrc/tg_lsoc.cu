@@ -95,7 +95,7 @@ __global__ void operand_kernel(const double2* __restrict__ G, int n, int64_t np,
 // the weights follow the point traversal of the Green-function launch g (tabulated k-major
 // or the flattened list), as the fused output stages do
 __global__ void gather_kernel(GreenArgs g, const double2* __restrict__ G, int mode, const int* __restrict__ outmap,
-                              int64_t ld, double2* __restrict__ out) {
+                              int64_t ld, double2* __restrict__ out, int16_t* __restrict__ eout) {
   const int n = g.n;
   const int64_t nn = (int64_t)n * n;
   const int64_t total = g.np * ld;
@@ -131,19 +131,20 @@ __global__ void gather_kernel(GreenArgs g, const double2* __restrict__ G, int mo
       v = cconj(grc);
     }
     out[idx] = v;
+    if (eout) eout[idx] = exponent_code16(v);
   }
 }
 
 }  // namespace
 
 cudaError_t launch_gather(const GreenArgs& g, const double2* G, int mode, const int* outmap, int64_t ld, double2* out,
-                          int num_sms, cudaStream_t s) {
+                          int16_t* eout, int num_sms, cudaStream_t s) {
   if (g.np <= 0) return cudaSuccess;
   if (mode != MODE_A_IMAG && mode != MODE_B_IMAG && mode != MODE_A_REAL && mode != MODE_B_REAL)
     return cudaErrorInvalidValue;
   const int64_t total = g.np * ld;
   const int64_t grid = std::min<int64_t>((total + 255) / 256, (int64_t)num_sms * 16);
-  gather_kernel<<<(unsigned)grid, 256, 0, s>>>(g, G, mode, outmap, ld, out);
+  gather_kernel<<<(unsigned)grid, 256, 0, s>>>(g, G, mode, outmap, ld, out, eout);
   return cudaGetLastError();
 }
 
