@@ -163,3 +163,30 @@ def test_tridiagonal_resolvents_equal_gauss_jordan(gpu, shape, sel_d, precision)
         gpu.set_green_method("auto")
         gpu.set_chi_orbitals(None)
     assert rel(auto, gj) < (1e-12 if precision == "fp64" else 1e-9)
+
+
+@pytest.mark.parametrize("sel_d", [False, True])
+def test_tridiagonal_real_axis_of_its_own(gpu, sel_d):
+    """A real-axis BZ that differs from the imaginary-axis k list gets tridiagonalisations of
+    its own (H(k) and H(k + q) slots apart from the imaginary axis'): equal to Gauss-Jordan
+    and to the oracle on the same meshes."""
+    deck = synthetic.make_deck("slab6", nk=(3, 3, 1), n1gl=4, parts=1, n3gl=3)
+    s = deck.system
+    h0 = s.h0(initial_state(s))
+    gpu.setup(deck, h0)
+    rkp = deck.real_kp + np.array([0.013, -0.021, 0.0])   # another k list than the imaginary axis'
+    gpu.set_real_mesh(rkp, deck.real_w)
+    sel = [list(d) for d in s.dorbs] if sel_d else None
+    gpu.set_chi_orbitals(sel)
+    e, q = 0.05, np.array([0.1, 0.0, 0.0])
+    x2, p2 = deck.real_points(e, s.Ef)
+    try:
+        auto = gpu.chi0(q, e, s.Ef, s.eta, s.etap, x2, p2, precision="fp64")
+        gpu.set_green_method("gauss-jordan")
+        gj = gpu.chi0(q, e, s.Ef, s.eta, s.etap, x2, p2, precision="fp64")
+    finally:
+        gpu.set_green_method("auto")
+        gpu.set_chi_orbitals(None)
+    assert rel(auto, gj) < 1e-12
+    ref = O.eintshechi(O.Model(s, h0), deck.ek, (rkp, deck.real_w), q, e, s.Ef, s.eta, s.etap, x2, p2, sel=sel)
+    assert rel(auto, ref) < 1e-10
