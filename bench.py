@@ -432,8 +432,9 @@ def run_ours(args, rank, world, local_rank):
     spectral_real = eig_fast and shared
     tri_all = tri_ok and tabulated
     tri_real = tri_ok and shared
+    # the spectral real axis forms G2 again per wave vector; the tridiagonalised one shares it
     n_inv = inversions_of(deck, per, reals, start + args.warmup * per + (args.steps - 1) * per, nq, shared,
-                          (spectral_real or tri_real) and shared)
+                          spectral_real and shared)
     ns = sum(2 * len(o) for o in sel) if sel is not None else s.dimH
     tri_name = ("hh_tridiag_kernel + tri_green_kernel (Householder tridiagonalisation per k, G over the %d rows "
                 "of chi per point: tridiagonal solves + FP64 DMMA GEMM) + gather_kernel" % ns)

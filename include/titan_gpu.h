@@ -118,8 +118,10 @@ int tg_set_split_chunk(tg_ctx* ctx, int points);
  * mesh (adaptive meshes, or H(k) tables above 8 GiB) every pass inverts and quantises it
  * once and contracts it with G1(k + q, z + e) of every (q, e).  The real axis then uses
  * spectral Green functions where the method and dimension allow (eigendecompositions of
- * H(k) once and of H(k + q) once per q, for every frequency), else one inversion of G2 per
- * pass and frequency shared by the q.  On tabulated meshes the q run one after another,
+ * H(k) once and of H(k + q) once per q, for every frequency; G2 formed again per q), or
+ * beyond dimH 72 Householder tridiagonalisations of H(k) and of every H(k + q) (up to 8
+ * nonzero q at once, memory permitting) with G2 formed once per pass and frequency for all
+ * q, else one inversion of G2 per pass and frequency shared by the q.  On tabulated meshes the q run one after another,
  * each sharing G2 over its frequencies.  No counterpart in the reference. */
 int tg_chi0_qbatch(tg_ctx* ctx, int n_q, const double* q, int n_omega, const double* e, double Ef,
                    double eta, double etap, int n_real, const double* x2, const double* p2,

@@ -30,6 +30,7 @@ int dyson_device(int n, const double2* chi_hf, const double2* U, double2* work, 
 namespace {
 
 constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr int kTriQSlots = 8;   // tridiagonalisations of H(k + q) kept at once by tg_chi0_qbatch
 
 template <class T>
 struct DevArray {
@@ -189,8 +190,9 @@ struct tg_ctx {
   DevArray<double2> d_graw;   // column-major G of a pass (gathered chi0 operands)
   DevArray<int> d_allrows;    // 0 .. dimH - 1
   // Householder tridiagonalisations per k list (same slots as the H tables)
-  DevArray<double> d_triD[4], d_triE[4];
-  DevArray<double2> d_triQ[4];
+  // (slots 4 .. 4 + kTriQSlots - 1: one per wave vector of a q-batched real axis)
+  DevArray<double> d_triD[4 + kTriQSlots], d_triE[4 + kTriQSlots];
+  DevArray<double2> d_triQ[4 + kTriQSlots];
   DevArray<unsigned char> d_clws;   // workspace of the thread-block-cluster Gauss-Jordan kernel
   // tg_expectation_noalloc: device address of the library's fixed scratch array on this
   // context's device (looked up by the context's first no-alloc call)
@@ -456,12 +458,12 @@ int build_tri_chunked(tg_ctx* c, int slot, const double* d_k, int64_t nk, const 
 
 // whether tridiagonalisations of nk points in slots s0 and s1 (-1: none) fit: what they add to
 // the current allocations (and the H chunk) within half the free device memory
-bool tri_room(tg_ctx* c, int64_t nk, int64_t ns, int s0, int s1) {
+bool tri_room_slots(tg_ctx* c, int64_t nk, int64_t ns, const std::vector<int>& slots) {
   size_t fr = 0, tot = 0;
   if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
   const size_t n = c->dimH, nn = n * n;
   double need = 0.0;
-  for (int sl : {s0, s1}) {
+  for (int sl : slots) {
     if (sl < 0) continue;
     const size_t want = (size_t)nk * ns * n;
     if (c->d_triQ[sl].n < want) need += (double)(want - c->d_triQ[sl].n) * sizeof(double2);
@@ -471,6 +473,8 @@ bool tri_room(tg_ctx* c, int64_t nk, int64_t ns, int s0, int s1) {
   if (c->d_hchunk.n < kc * nn) need += (double)(kc * nn - c->d_hchunk.n) * sizeof(double2);
   return need <= 0.5 * (double)fr;
 }
+
+bool tri_room(tg_ctx* c, int64_t nk, int64_t ns, int s0, int s1) { return tri_room_slots(c, nk, ns, {s0, s1}); }
 
 int reset_eig_status(tg_ctx* c) {
   const int big = 0x7fffffff;
@@ -1543,8 +1547,9 @@ namespace {
 // chi0 for n_q wave vectors and n_omega frequencies with G2 shared by all of them: on meshes
 // without H(k) tables (adaptive imaginary axes, large real-axis BZs) G2 = G(k, z) does not
 // depend on q, so every pass inverts and quantises it once and contracts it with G1(k + q, z + e)
-// of every (q, e); on the real axis G2(k, x2 + i eta') depends on e (through x2) but not on q,
-// and with spectral Green functions every (q, e) forms it again from U(k) instead.
+// of every (q, e); on the real axis G2(k, x2 + i eta') depends on e (through x2) but not on q:
+// with spectral Green functions every (q, e) forms it again from U(k) instead, with
+// tridiagonalised ones (every H(k + q) decomposed up front) it serves every q.
 // Accumulators: n_q x n_omega x nsplit chi-sized partials for each axis.
 int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double* e, double Ef, double eta,
                  double etap, int n_real, bool split, double* chiorb_hf) {
@@ -1669,11 +1674,14 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
       }
     };
     const int64_t ntot = (int64_t)n_real * c->n_realk;
+    // slot of each wave vector's H(k + q) decomposition (2: that of H(k), for q = 0)
+    std::vector<int> qslot(n_q, 2), nzq;
     for (int iq = 0; iq < n_q; ++iq) {
       const double* qi = qs + 3 * iq;
-      const bool qz = qi[0] == 0.0 && qi[1] == 0.0 && qi[2] == 0.0;
-      if (!qz && eig_real && (rc = build_eig_chunked(c, 3, c->d_rkp.p, c->n_realk, qi))) return rc;
-      if (!qz && tri_real && (rc = build_tri_chunked(c, 3, c->d_rkp.p, c->n_realk, qi, v))) return rc;
+      if (!(qi[0] == 0.0 && qi[1] == 0.0 && qi[2] == 0.0)) nzq.push_back(iq);
+    }
+    // every pass and frequency: G2 once (and quantised once), then G1 of each wave vector in iqs
+    auto real_passes = [&](const std::vector<int>& iqs) -> int {
       for (int w = 0; w < n_omega; ++w) {
         if (std::fabs(e[w]) < 1e-15) continue;
         for (int64_t p0 = 0; p0 < ntot; p0 += P) {
@@ -1693,32 +1701,65 @@ int chi0_qshared(tg_ctx* c, int n_q, const double* qs, int n_omega, const double
           gr.out = c->d_B.p;
           gr.eout = e16 ? c->d_e16B.p : nullptr;
           use_eig(gr, 2);
+          int rc2 = 0;
           {
             KindTimer kt(c, 0);
-            if ((rc = chi_green(c, v, gr, "green (real, G2)"))) return rc;
-          }
-          GreenArgs g1 = gr;
-          g1.zr = e[w];
-          g1.zi = eta;
-          g1.mode = MODE_A_REAL;
-          g1.out = c->d_A.p;
-          g1.eout = e16 ? c->d_e16A.p : nullptr;
-          use_eig(g1, qz ? 2 : 3);
-          {
-            KindTimer kt(c, 0);
-            if ((rc = chi_green(c, v, g1, "green (real, G1)"))) return rc;
+            if ((rc2 = chi_green(c, v, gr, "green (real, G2)"))) return rc2;
           }
           SplitPassDev pr;
           if (split) {
             KindTimer kq(c, 3);
             const SplitChunks ch = make_chunks_kmajor(p0, np, n_real, c->split_chunk);
-            if ((rc = split_prepare(c, v, ch, pr))) return rc;
-            if ((rc = split_quantize_operand(c, v, 1, c->d_B.p, pr, e16 ? c->d_e16B.p : nullptr))) return rc;
-            if ((rc = split_quantize_operand(c, v, 0, c->d_A.p, pr, e16 ? c->d_e16A.p : nullptr))) return rc;
+            if ((rc2 = split_prepare(c, v, ch, pr))) return rc2;
+            if ((rc2 = split_quantize_operand(c, v, 1, c->d_B.p, pr, e16 ? c->d_e16B.p : nullptr))) return rc2;
           }
-          if ((rc = contract_into(pr, np, acc_at(c->d_D.p, iq, w), bound_at(c, split, iq * n_omega + w, 1))))
-            return rc;
+          for (int iq : iqs) {
+            GreenArgs g1 = gr;
+            g1.zr = e[w];
+            g1.zi = eta;
+            g1.mode = MODE_A_REAL;
+            g1.out = c->d_A.p;
+            g1.eout = e16 ? c->d_e16A.p : nullptr;
+            use_eig(g1, qslot[iq]);
+            {
+              KindTimer kt(c, 0);
+              if ((rc2 = chi_green(c, v, g1, "green (real, G1)"))) return rc2;
+            }
+            if (split) {
+              KindTimer kq(c, 3);
+              if ((rc2 = split_quantize_operand(c, v, 0, c->d_A.p, pr, e16 ? c->d_e16A.p : nullptr))) return rc2;
+            }
+            if ((rc2 = contract_into(pr, np, acc_at(c->d_D.p, iq, w), bound_at(c, split, iq * n_omega + w, 1))))
+              return rc2;
+          }
         }
+      }
+      return TG_OK;
+    };
+    // tridiagonalisations of every H(k + q) at once, where they fit, let G2 serve every q
+    std::vector<int> qslots;
+    for (size_t j = 0; j < nzq.size(); ++j) qslots.push_back(4 + (int)j);
+    const bool share = tri_real && n_q > 1 && (int)nzq.size() <= kTriQSlots &&
+                       tri_room_slots(c, c->n_realk, v.nrows, qslots);
+    if (share) {
+      for (size_t j = 0; j < nzq.size(); ++j) {
+        const int iq = nzq[j];
+        qslot[iq] = qslots[j];
+        if ((rc = build_tri_chunked(c, qslot[iq], c->d_rkp.p, c->n_realk, qs + 3 * iq, v))) return rc;
+      }
+      std::vector<int> all(n_q);
+      for (int iq = 0; iq < n_q; ++iq) all[iq] = iq;
+      if ((rc = real_passes(all))) return rc;
+    } else {
+      for (int iq = 0; iq < n_q; ++iq) {
+        const double* qi = qs + 3 * iq;
+        const bool qz = qi[0] == 0.0 && qi[1] == 0.0 && qi[2] == 0.0;
+        if (!qz) {
+          qslot[iq] = 3;
+          if (eig_real && (rc = build_eig_chunked(c, 3, c->d_rkp.p, c->n_realk, qi))) return rc;
+          if (tri_real && (rc = build_tri_chunked(c, 3, c->d_rkp.p, c->n_realk, qi, v))) return rc;
+        }
+        if ((rc = real_passes({iq}))) return rc;
       }
     }
   }
